@@ -1,0 +1,139 @@
+/* gsj - B200-native (sm_100a) spatial-join engine: the C ABI.
+ *
+ * Drop-in for the engine entry points behind the gpujoind daemon of landstats-us/postgis-cuda (paths below are
+ * relative to that project). Plain pointers and sizes only; every call returns an int status (0 = GSJ_OK) and
+ * never exits the process (the reference's CK() aborts, engine/common.h:13-14); gsj_last_error() gives the
+ * message. Host inputs are copied at upload; result pointers handed to a sink are valid only during the call
+ * (as the reference's callback contract, engine/engine.cuh:1047-1055). One context per GPU; a context is used
+ * by one host thread at a time (the serving loop owns it).
+ */
+#ifndef GSJ_H
+#define GSJ_H
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GSJ_OK 0
+#define GSJ_ERR_ARG 1        /* invalid argument */
+#define GSJ_ERR_CUDA 2       /* CUDA runtime error (message in gsj_last_error) */
+#define GSJ_ERR_NOMEM 3      /* device or host allocation failed / admission refused */
+#define GSJ_ERR_CANCELLED 4  /* the cancel flag was raised between batches */
+#define GSJ_ERR_SINK 5       /* the sink returned non-zero */
+#define GSJ_ERR_TIMEOUT 6    /* a bounded device-side wait expired */
+
+typedef struct gsj_ctx gsj_ctx;
+typedef struct gsj_layer gsj_layer;
+
+/* Context on a CUDA device (replaces the daemon's process-global device state, daemon/gpujoind.cu:589-621). */
+int gsj_ctx_create(int device, gsj_ctx** out);
+void gsj_ctx_destroy(gsj_ctx* ctx);
+const char* gsj_last_error(const gsj_ctx* ctx);
+/* Free device memory and the number of SMs, for admission decisions (gpujoind.cu:133-137). */
+int gsj_ctx_mem_info(gsj_ctx* ctx, uint64_t* free_bytes, uint64_t* total_bytes, int* sm_count);
+
+/* Resident polygon layer + its LBVH: upload_set (engine/engine.cuh:42-89) followed by build_bvh (engine.cuh:197-228).
+ * gro[n+1], rvo[nr+1], xy[2nv] world coordinates (closed rings, shells CCW, holes CW: daemon/loader.h:100-102).
+ * parent[n] (piece -> geometry, non-decreasing) and syn[nv] (1: edge v->v+1 was created by subdivision) are
+ * optional (NULL), as upload_set's parent/syn arguments. */
+int gsj_layer_upload_polygons(gsj_ctx* ctx, uint64_t n, uint64_t nr, uint64_t nv, const uint64_t* gro, const uint64_t* rvo,
+                              const double* xy, const uint32_t* parent, const uint8_t* syn, gsj_layer** out);
+/* Resident point layer + LBVH over the points' degenerate boxes: upload_points (engine.cuh:1068-1076). */
+int gsj_layer_upload_points(gsj_ctx* ctx, uint64_t n, const double* xy, gsj_layer** out);
+/* free_set / free_points / free_bvh (engine.cuh:91-97, 1077, 230). */
+void gsj_layer_free(gsj_ctx* ctx, gsj_layer* layer);
+
+typedef struct gsj_layer_info {
+  uint64_t n, nr, nv;     /* geometries (pieces), rings, vertices (points: n = nv, nr = 0) */
+  uint32_t nparent;       /* parent geometries (== n when not subdivided) */
+  int is_points;
+  uint32_t max_geom_edges;
+  uint64_t device_bytes;  /* resident bytes incl. the LBVH (Layer::gpu_bytes, gpujoind.cu:145) */
+} gsj_layer_info;
+int gsj_layer_get_info(const gsj_layer* layer, gsj_layer_info* info);
+
+/* RefineParams (engine.cuh:517-518). Defaults: 1e-12, 1e-7, 1e-11, area on, relate off, snap off. */
+typedef struct gsj_refine_params {
+  double tol_rel, eps_par, tol_abs;
+  int want_area, want_relate, snap_half_ulp;
+} gsj_refine_params;
+void gsj_refine_params_default(gsj_refine_params* p);
+
+/* Refinement variants: GSJ_REFINE_PLAIN = FP64 everywhere (the reference's scheme); GSJ_REFINE_FILTERED = FP32
+ * certified filters in front of the FP64 predicates plus size-binned scheduling. Same results bit for bit. */
+#define GSJ_REFINE_PLAIN 0
+#define GSJ_REFINE_FILTERED 1
+
+/* JoinOpts (engine.cuh:799-813). */
+typedef struct gsj_join_opts {
+  uint32_t batch_q;          /* probe geometries per batch (0: whole probe layer) */
+  uint64_t max_pairs;        /* candidate pairs per refine launch (0: 128 Mi) */
+  int upper;                 /* self-join: each unordered pair once (b >= a) */
+  int no_agg;                /* report piece pairs instead of parent pairs */
+  int refine_mode;           /* GSJ_REFINE_PLAIN / GSJ_REFINE_FILTERED */
+  const volatile int* cancel;  /* checked between batches (Conn::broken, gpujoind.cu:225) */
+} gsj_join_opts;
+void gsj_join_opts_default(gsj_join_opts* o);
+
+/* JoinStats (engine.cuh:814) plus device-side timings of the phases. */
+typedef struct gsj_join_stats {
+  double traverse_ms, refine_ms, compact_ms, copy_ms;
+  uint64_t candidates, hits, heavy, batches;
+} gsj_join_stats;
+
+/* Sink for a finished batch (the host callback of join_stream): pairs[2n] = (P index, R index) in parent ids,
+ * area[n] (NULL without want_area), code[n] DE-9IM codes of relate(P, R) (NULL without want_relate; 2 bits per
+ * cell II IB IE BI BB BE EI EB EE, 0 = F, 1 = '0', 2 = '1', 3 = '2', engine.cuh:845-856). Return 0 to continue. */
+typedef int (*gsj_join_sink)(void* user, const uint32_t* pairs, const double* area, const uint32_t* code, uint64_t n);
+
+/* Intersects (+ area, + DE-9IM evidence) join of probe P against build R: join_stream (engine.cuh:895-1061).
+ * Behind gpu_join / gpu_intersects and gpu_relate (op_join / op_relate, daemon/gpujoind.cu:210-388). */
+int gsj_join(gsj_ctx* ctx, const gsj_layer* P, const gsj_layer* R, const gsj_refine_params* rp, const gsj_join_opts* o,
+             gsj_join_sink sink, void* user, gsj_join_stats* stats);
+
+/* Points in polygons: join_points_stream (engine.cuh:1112-1178). Sink gets (point, parent polygon) pairs and
+ * where[n] = 1 interior / 2 boundary (DE-9IM 0FFFFF212 / F0FFFF212, engine.cuh:337-338). */
+typedef int (*gsj_points_sink)(void* user, const uint32_t* pairs, const uint8_t* where, uint64_t n);
+int gsj_join_points(gsj_ctx* ctx, const gsj_layer* pts, const gsj_layer* R, const gsj_join_opts* o, gsj_points_sink sink,
+                    void* user, gsj_join_stats* stats);
+
+/* ST_ClusterIntersecting: cluster_intersecting (engine.cuh:1216-1234). root[nparent] = smallest parent index of each
+ * parent's connected component in the intersects graph. */
+int gsj_cluster(gsj_ctx* ctx, const gsj_layer* P, uint32_t nparent, const gsj_join_opts* o, uint32_t* root,
+                gsj_join_stats* stats);
+
+/* Pair sink for distance / buffer joins: (P parent, R parent) pairs. */
+typedef int (*gsj_pairs_sink)(void* user, const uint32_t* pairs, uint64_t n);
+/* ST_DWithin(a::geography, b::geography, d) polygon x polygon: dwithin_join_stream (engine/buffer.cuh:892-991).
+ * same: P and R are the same layer (pieces of one parent are within any distance; with upper). */
+int gsj_dwithin(gsj_ctx* ctx, const gsj_layer* P, const gsj_layer* R, double d_m, int same, const gsj_join_opts* o,
+                gsj_pairs_sink sink, void* user, gsj_join_stats* stats);
+/* ST_Intersects(ST_Buffer(a::geography, -ra), ST_Buffer(b::geography, -rb)): erode_join_stream (buffer.cuh:765-889).
+ * need_self[nparent] (host, optional): self pairs wanted for these parents (BufferQuery::need_self, buffer.cuh:694). */
+int gsj_erode(gsj_ctx* ctx, const gsj_layer* P, const gsj_layer* R, double ra_m, double rb_m, int same, const uint8_t* need_self,
+              const gsj_join_opts* o, gsj_pairs_sink sink, void* user, gsj_join_stats* stats);
+/* points x polygons: ST_DWithin (k_pt_dwithin) and point in ST_Buffer(polygon, -r) (k_pt_erode):
+ * points_buffer_join_stream (buffer.cuh:1137-1231). Sink gets (point, parent polygon) pairs. */
+int gsj_points_dwithin(gsj_ctx* ctx, const gsj_layer* pts, const gsj_layer* R, double d_m, const gsj_join_opts* o,
+                       gsj_pairs_sink sink, void* user, gsj_join_stats* stats);
+int gsj_points_erode(gsj_ctx* ctx, const gsj_layer* pts, const gsj_layer* R, double r_m, const gsj_join_opts* o,
+                     gsj_pairs_sink sink, void* user, gsj_join_stats* stats);
+
+/* Parity / diagnostics: candidate pairs of the LBVH traversal (k_traverse, engine.cuh:233-259) and the per-pair
+ * refinement outputs of k_refine (engine.cuh:530-636) for given piece pairs: flag 0/1/2, area, ev[4n]
+ * (inside / on lengths of A's then B's real boundary), evb bits. Output arrays are host memory, NULL to skip. */
+int gsj_candidates(gsj_ctx* ctx, const gsj_layer* P, const gsj_layer* R, int upper, gsj_pairs_sink sink, void* user);
+int gsj_refine_pairs(gsj_ctx* ctx, const gsj_layer* P, const gsj_layer* R, const uint32_t* pairs, uint64_t np,
+                     const gsj_refine_params* rp, int refine_mode, uint8_t* flag, double* area, double* ev, uint32_t* evb);
+
+/* DE-9IM helpers: de9im_str / de9im_transpose / de9im_match (engine.cuh:871-888). out gets 9 chars (no NUL). */
+void gsj_de9im_str(uint32_t code, char* out9);
+uint32_t gsj_de9im_transpose(uint32_t code);
+int gsj_de9im_match(uint32_t code, const char* pattern9);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,210 @@
+// The C ABI (include/gsj.h): status codes instead of exits, exceptions stop here.
+#include <cstring>
+#include "engine.h"
+
+namespace gsj {
+RefineArgs to_args(const gsj_refine_params* p);
+void join_host(gsj_ctx* c, const gsj_layer* P, const gsj_layer* R, const gsj_refine_params* rpp, const gsj_join_opts* op, gsj_join_sink sink,
+               void* user, gsj_join_stats* stp);
+void points_host(gsj_ctx* c, const gsj_layer* pts, const gsj_layer* R, const gsj_join_opts* op, gsj_points_sink sink, void* user,
+                 gsj_join_stats* stp);
+void cluster_host(gsj_ctx* c, const gsj_layer* P, uint32_t nparent, const gsj_join_opts* op, uint32_t* root, gsj_join_stats* stp);
+void candidates_host(gsj_ctx* c, const gsj_layer* P, const gsj_layer* R, int upper, gsj_pairs_sink sink, void* user);
+void refine_pairs_host(gsj_ctx* c, const gsj_layer* P, const gsj_layer* R, const uint32_t* pairs, uint64_t np, const gsj_refine_params* rpp,
+                       int mode, uint8_t* flag, double* area, double* ev, uint32_t* evb);
+void dwithin_host(gsj_ctx* c, const gsj_layer* P, const gsj_layer* R, double d, int same, const gsj_join_opts* op, gsj_pairs_sink sink, void* user,
+                  gsj_join_stats* stp);
+void erode_host(gsj_ctx* c, const gsj_layer* P, const gsj_layer* R, double ra, double rb, int same, const uint8_t* need_self, const gsj_join_opts* op,
+                gsj_pairs_sink sink, void* user, gsj_join_stats* stp);
+void points_buffer_host(gsj_ctx* c, const gsj_layer* pts, const gsj_layer* R, double d, int erode, const gsj_join_opts* op, gsj_pairs_sink sink,
+                        void* user, gsj_join_stats* stp);
+}  // namespace gsj
+
+using gsj::Error;
+
+template <class F> static int guard(gsj_ctx* c, F&& f) {
+  try {
+    if (c) GSJ_CK(cudaSetDevice(c->device));
+    f();
+    if (c) c->err.clear();
+    return GSJ_OK;
+  } catch (const Error& e) {
+    if (c) c->err = e.what();
+    if (e.code == GSJ_ERR_CUDA || e.code == GSJ_ERR_NOMEM) (void)cudaGetLastError();   // clear a sticky-free error state
+    return e.code;
+  } catch (const std::bad_alloc&) {
+    if (c) c->err = "host allocation failed";
+    return GSJ_ERR_NOMEM;
+  } catch (const std::exception& e) {
+    if (c) c->err = e.what();
+    return GSJ_ERR_ARG;
+  }
+}
+
+extern "C" {
+
+int gsj_ctx_create(int device, gsj_ctx** out) {
+  if (!out) return GSJ_ERR_ARG;
+  *out = nullptr;
+  gsj_ctx* c = new gsj_ctx();
+  c->device = device;
+  int rc = guard(c, [&] {
+    int nd = 0;
+    GSJ_CK(cudaGetDeviceCount(&nd));
+    if (device < 0 || device >= nd) throw Error(GSJ_ERR_ARG, "no such CUDA device");
+    GSJ_CK(cudaSetDevice(device));
+    GSJ_CK(cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, device));
+    GSJ_CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+  });
+  if (rc) { delete c; return rc; }
+  *out = c;
+  return GSJ_OK;
+}
+
+void gsj_ctx_destroy(gsj_ctx* c) {
+  if (!c) return;
+  cudaSetDevice(c->device);
+  if (c->stream) { cudaStreamSynchronize(c->stream); cudaStreamDestroy(c->stream); }
+  delete c;
+}
+
+const char* gsj_last_error(const gsj_ctx* c) { return c ? c->err.c_str() : "no context"; }
+
+int gsj_ctx_mem_info(gsj_ctx* c, uint64_t* fr, uint64_t* tot, int* sms) {
+  if (!c) return GSJ_ERR_ARG;
+  return guard(c, [&] {
+    size_t f = 0, t = 0;
+    GSJ_CK(cudaMemGetInfo(&f, &t));
+    if (fr) *fr = f;
+    if (tot) *tot = t;
+    if (sms) *sms = c->sm_count;
+  });
+}
+
+int gsj_layer_upload_polygons(gsj_ctx* c, uint64_t n, uint64_t nr, uint64_t nv, const uint64_t* gro, const uint64_t* rvo, const double* xy,
+                              const uint32_t* parent, const uint8_t* syn, gsj_layer** out) {
+  if (!c || !out) return GSJ_ERR_ARG;
+  *out = nullptr;
+  gsj_layer* L = new gsj_layer();
+  L->device = c->device;
+  int rc = guard(c, [&] { gsj::layer_upload_polygons(c, n, nr, nv, gro, rvo, xy, parent, syn, L); });
+  if (rc) { gsj::layer_free(L); delete L; return rc; }
+  *out = L;
+  return GSJ_OK;
+}
+
+int gsj_layer_upload_points(gsj_ctx* c, uint64_t n, const double* xy, gsj_layer** out) {
+  if (!c || !out) return GSJ_ERR_ARG;
+  *out = nullptr;
+  gsj_layer* L = new gsj_layer();
+  L->device = c->device;
+  int rc = guard(c, [&] { gsj::layer_upload_points(c, n, xy, L); });
+  if (rc) { gsj::layer_free(L); delete L; return rc; }
+  *out = L;
+  return GSJ_OK;
+}
+
+void gsj_layer_free(gsj_ctx* c, gsj_layer* L) {
+  if (!L) return;
+  if (c) { cudaSetDevice(c->device); if (c->stream) cudaStreamSynchronize(c->stream); }
+  gsj::layer_free(L);
+  delete L;
+}
+
+int gsj_layer_get_info(const gsj_layer* L, gsj_layer_info* info) {
+  if (!L || !info) return GSJ_ERR_ARG;
+  info->n = L->d.n; info->nr = L->d.nr; info->nv = L->d.nv; info->nparent = L->nparent; info->is_points = L->is_points;
+  info->max_geom_edges = L->max_geom_edges; info->device_bytes = L->bytes;
+  return GSJ_OK;
+}
+
+void gsj_refine_params_default(gsj_refine_params* p) {
+  if (!p) return;
+  p->tol_rel = 1e-12; p->eps_par = 1e-7; p->tol_abs = 1e-11;
+  p->want_area = 1; p->want_relate = 0; p->snap_half_ulp = 0;
+}
+
+void gsj_join_opts_default(gsj_join_opts* o) {
+  if (!o) return;
+  memset(o, 0, sizeof(*o));
+  o->batch_q = 0; o->max_pairs = 0; o->upper = 0; o->no_agg = 0; o->refine_mode = GSJ_REFINE_FILTERED; o->cancel = nullptr;
+}
+
+int gsj_join(gsj_ctx* c, const gsj_layer* P, const gsj_layer* R, const gsj_refine_params* rp, const gsj_join_opts* o, gsj_join_sink sink,
+             void* user, gsj_join_stats* st) {
+  if (!c || !P || !R) return GSJ_ERR_ARG;
+  return guard(c, [&] { gsj::join_host(c, P, R, rp, o, sink, user, st); });
+}
+
+int gsj_join_points(gsj_ctx* c, const gsj_layer* pts, const gsj_layer* R, const gsj_join_opts* o, gsj_points_sink sink, void* user,
+                    gsj_join_stats* st) {
+  if (!c || !pts || !R) return GSJ_ERR_ARG;
+  return guard(c, [&] { gsj::points_host(c, pts, R, o, sink, user, st); });
+}
+
+int gsj_cluster(gsj_ctx* c, const gsj_layer* P, uint32_t nparent, const gsj_join_opts* o, uint32_t* root, gsj_join_stats* st) {
+  if (!c || !P || !root) return GSJ_ERR_ARG;
+  return guard(c, [&] { gsj::cluster_host(c, P, nparent, o, root, st); });
+}
+
+int gsj_dwithin(gsj_ctx* c, const gsj_layer* P, const gsj_layer* R, double d, int same, const gsj_join_opts* o, gsj_pairs_sink sink, void* user,
+                gsj_join_stats* st) {
+  if (!c || !P || !R || !(d >= 0)) return GSJ_ERR_ARG;
+  return guard(c, [&] { gsj::dwithin_host(c, P, R, d, same, o, sink, user, st); });
+}
+
+int gsj_erode(gsj_ctx* c, const gsj_layer* P, const gsj_layer* R, double ra, double rb, int same, const uint8_t* need_self, const gsj_join_opts* o,
+              gsj_pairs_sink sink, void* user, gsj_join_stats* st) {
+  if (!c || !P || !R || !(ra >= 0) || !(rb >= 0)) return GSJ_ERR_ARG;
+  return guard(c, [&] { gsj::erode_host(c, P, R, ra, rb, same, need_self, o, sink, user, st); });
+}
+
+int gsj_points_dwithin(gsj_ctx* c, const gsj_layer* pts, const gsj_layer* R, double d, const gsj_join_opts* o, gsj_pairs_sink sink, void* user,
+                       gsj_join_stats* st) {
+  if (!c || !pts || !R || !(d >= 0)) return GSJ_ERR_ARG;
+  return guard(c, [&] { gsj::points_buffer_host(c, pts, R, d, 0, o, sink, user, st); });
+}
+
+int gsj_points_erode(gsj_ctx* c, const gsj_layer* pts, const gsj_layer* R, double r, const gsj_join_opts* o, gsj_pairs_sink sink, void* user,
+                     gsj_join_stats* st) {
+  if (!c || !pts || !R || !(r >= 0)) return GSJ_ERR_ARG;
+  return guard(c, [&] { gsj::points_buffer_host(c, pts, R, r, 1, o, sink, user, st); });
+}
+
+int gsj_candidates(gsj_ctx* c, const gsj_layer* P, const gsj_layer* R, int upper, gsj_pairs_sink sink, void* user) {
+  if (!c || !P || !R) return GSJ_ERR_ARG;
+  return guard(c, [&] { gsj::candidates_host(c, P, R, upper, sink, user); });
+}
+
+int gsj_refine_pairs(gsj_ctx* c, const gsj_layer* P, const gsj_layer* R, const uint32_t* pairs, uint64_t np, const gsj_refine_params* rp,
+                     int mode, uint8_t* flag, double* area, double* ev, uint32_t* evb) {
+  if (!c || !P || !R || (np && !pairs)) return GSJ_ERR_ARG;
+  return guard(c, [&] { gsj::refine_pairs_host(c, P, R, pairs, np, rp, mode, flag, area, ev, evb); });
+}
+
+void gsj_de9im_str(uint32_t code, char* out) {
+  for (int k = 0; k < 9; k++) out[k] = "F012"[(code >> (2 * k)) & 3];
+}
+
+uint32_t gsj_de9im_transpose(uint32_t c) {
+  uint32_t t = 0;
+  for (int r = 0; r < 3; r++)
+    for (int q = 0; q < 3; q++) t |= ((c >> (2 * (3 * r + q))) & 3) << (2 * (3 * q + r));
+  return t;
+}
+
+int gsj_de9im_match(uint32_t code, const char* pat) {
+  if (!pat) return 0;
+  for (int k = 0; k < 9; k++) {
+    const char p = pat[k];
+    const uint32_t v = (code >> (2 * k)) & 3;
+    if (p == '*') continue;
+    if (p == 'T' || p == 't') { if (v == 0) return 0; continue; }
+    if (p == 'F' || p == 'f') { if (v != 0) return 0; continue; }
+    if (p >= '0' && p <= '2') { if (v != (uint32_t)(p - '0') + 1) return 0; continue; }
+    return 0;
+  }
+  return 1;
+}
+
+}  // extern "C"

@@ -1,0 +1,121 @@
+// Host-side engine internals: context, resident layers, grow-only scratch pools, launch helpers.
+// Errors are thrown as gsj::Error inside the library and turned into status codes at the C ABI (capi.cu).
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <cstdio>
+#include <stdexcept>
+#include <string>
+#include <vector>
+#include "../../include/gsj.h"
+#include "geom.cuh"
+
+namespace gsj {
+
+struct Error : std::runtime_error {
+  int code;
+  Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+#define GSJ_CK(x)                                                                                                   \
+  do {                                                                                                              \
+    cudaError_t e_ = (x);                                                                                           \
+    if (e_ != cudaSuccess)                                                                                          \
+      throw ::gsj::Error(e_ == cudaErrorMemoryAllocation ? GSJ_ERR_NOMEM : GSJ_ERR_CUDA,                            \
+                         std::string(#x) + ": " + cudaGetErrorString(e_) + " (" __FILE__ ":" + std::to_string(__LINE__) + ")"); \
+  } while (0)
+
+// grow-only device scratch: the pools live in the context, so steady-state requests allocate nothing
+struct DevBuf {
+  void* p = nullptr; size_t cap = 0;
+  void* get(size_t n) {
+    if (n > cap) {
+      if (p) cudaFree(p);
+      p = nullptr; cap = 0;
+      size_t want = n + n / 4 + 256;
+      GSJ_CK(cudaMalloc(&p, want));
+      cap = want;
+    }
+    return p;
+  }
+  template <class T> T* as(size_t count) { return reinterpret_cast<T*>(get(count * sizeof(T) + 16)); }
+  void release() { if (p) cudaFree(p); p = nullptr; cap = 0; }
+  ~DevBuf() { release(); }
+};
+struct PinnedBuf {
+  void* p = nullptr; size_t cap = 0;
+  void* get(size_t n) {
+    if (n > cap) {
+      if (p) cudaFreeHost(p);
+      p = nullptr; cap = 0;
+      size_t want = n + n / 4 + 256;
+      GSJ_CK(cudaHostAlloc(&p, want, cudaHostAllocDefault));
+      cap = want;
+    }
+    return p;
+  }
+  template <class T> T* as(size_t count) { return reinterpret_cast<T*>(get(count * sizeof(T) + 16)); }
+  void release() { if (p) cudaFreeHost(p); p = nullptr; cap = 0; }
+  ~PinnedBuf() { release(); }
+};
+
+struct Timer {
+  cudaEvent_t a = nullptr, b = nullptr; cudaStream_t s = nullptr;
+  explicit Timer(cudaStream_t st) : s(st) { GSJ_CK(cudaEventCreate(&a)); GSJ_CK(cudaEventCreate(&b)); }
+  ~Timer() { if (a) cudaEventDestroy(a); if (b) cudaEventDestroy(b); }
+  void start() { GSJ_CK(cudaEventRecord(a, s)); }
+  float stop() { GSJ_CK(cudaEventRecord(b, s)); GSJ_CK(cudaEventSynchronize(b)); float ms = 0; GSJ_CK(cudaEventElapsedTime(&ms, a, b)); return ms; }
+};
+
+}  // namespace gsj
+
+struct gsj_layer {
+  gsj::DLayer d;
+  gsj::DBvh bvh;
+  int is_points = 0;
+  uint32_t nparent = 0;
+  uint32_t max_geom_edges = 0;
+  uint64_t bytes = 0;
+  std::vector<void*> allocs;           // owned device memory
+  std::vector<uint32_t> h_parent;      // host copy (batches keep the pieces of one parent together)
+  const double2* pts = nullptr;        // points layer: world coordinates
+  int device = 0;
+};
+
+struct gsj_ctx {
+  int device = 0;
+  int sm_count = 148;
+  cudaStream_t stream = nullptr;
+  std::string err;
+  int refine_attr = 0;
+  // scratch pools
+  gsj::DevBuf counters, cand, flag, area, ev, evb, heavy, scratch, keep, opairs, oarea, oev, oevb, ocode, tmp, keys, keys2, idx,
+      idx2, agg_area, agg_ev, agg_evb, agg_flag, qbb, uf, misc1, misc2, misc3;
+  gsj::PinnedBuf h_counters, h_pairs, h_area, h_code, h_where;
+};
+
+namespace gsj {
+
+inline int grid_for(uint64_t n, int block) { return (int)std::min<uint64_t>((n + block - 1) / block, (uint64_t)1 << 30); }
+
+// kernels / drivers implemented in the .cu files
+void layer_upload_polygons(gsj_ctx* c, uint64_t n, uint64_t nr, uint64_t nv, const uint64_t* gro, const uint64_t* rvo, const double* xy,
+                           const uint32_t* parent, const uint8_t* syn, gsj_layer* L);
+void layer_upload_points(gsj_ctx* c, uint64_t n, const double* xy, gsj_layer* L);
+void build_bvh(gsj_ctx* c, gsj_layer* L);
+void layer_free(gsj_layer* L);
+
+// candidate pairs of probe boxes qbb[q0 .. q0+nq) (query order: qorder or identity) against the BVH; returns count.
+// Writes at most cap pairs; a count above cap means the caller must grow the buffer and re-run.
+uint64_t traverse(gsj_ctx* c, const float4* qbb, const uint32_t* qorder, uint32_t q0, uint32_t nq, const DBvh& T, int upper,
+                  uint2* out, uint64_t cap);
+
+struct RefineArgs {
+  double tol_rel, eps_par, tol_abs;
+  int want_area, want_relate, snap_half_ulp;
+};
+// per-pair refinement (flag, area, ev, evb); returns the number of pairs that took the oversized path
+uint64_t refine(gsj_ctx* c, const gsj_layer* P, const gsj_layer* R, const uint2* pairs, uint64_t np, const RefineArgs& rp, int mode,
+                uint8_t* flag, double* area, double4* ev, uint32_t* evb);
+
+}  // namespace gsj

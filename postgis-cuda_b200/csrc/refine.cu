@@ -1,0 +1,365 @@
+// Exact refinement of candidate pairs: ST_Intersects, intersection area (Green's theorem over the boundary
+// pieces inside the other polygon, product-rule weights on shared boundaries) and DE-9IM evidence, one warp per
+// pair. Restates the decisions of the reference's k_refine / edge_contrib_loc (engine/engine.cuh:333-636) with
+// its lane ownership kept (lane l owns local edges l, l+32, ...; A's then B's; shfl_down tree 16..1), so the
+// FP64 area and boundary-length sums have one fixed rounding order: bit-identical to the CPU oracle.
+//
+// Pairs whose local edge lists fit CAP run from shared memory; larger pairs are queued and re-run by
+// k_refine_scratch with per-warp lists in global scratch (the same device code, so the same results).
+#include "engine.h"
+
+namespace gsj {
+
+constexpr int CAP = 128;                         // local edges per polygon per warp in shared memory
+constexpr int RB_WARPS = 4;                      // warps per block
+constexpr size_t EDGE_BYTES = 4 * sizeof(double) + sizeof(uint32_t);
+constexpr size_t LIST_BYTES = CAP * EDGE_BYTES;  // one list
+constexpr size_t RB_SMEM = (size_t)RB_WARPS * 2 * LIST_BYTES;
+
+__device__ __forceinline__ EList carve(unsigned char* base, int cap) {
+  EList L;
+  L.x0 = reinterpret_cast<double*>(base);
+  L.y0 = L.x0 + cap; L.x1 = L.y0 + cap; L.y1 = L.x1 + cap;
+  L.fl = reinterpret_cast<uint32_t*>(L.y1 + cap);
+  return L;
+}
+
+__device__ __forceinline__ bool edge_outside(double px, double py, double qx, double qy, const Box& o) {
+  return fmax(px, qx) < o.x0 || fmin(px, qx) > o.x1 || fmax(py, qy) < o.y0 || fmin(py, qy) > o.y1;
+}
+
+// all edges of geometry A meeting the overlap box, compacted in ring order with a warp ballot (engine.cuh:358-377)
+__device__ int collect(const Frame& A, const Box& ov, EList L, int cap, int lane) {
+  const DLayer& S = *A.L;
+  const unsigned lt = (1u << lane) - 1;
+  int cnt = 0;
+  for (uint32_t ra = A.r0; ra < A.r1; ra++) {
+    const uint64_t s = S.rvo[ra], e = S.rvo[ra + 1];
+    for (uint64_t base = s; base + 1 < e; base += 32) {
+      const uint64_t i = base + lane;
+      bool in = false;
+      double x0 = 0, y0 = 0, x1 = 0, y1 = 0; uint32_t fl = 0;
+      if (i + 1 < e) {
+        A.v(i, x0, y0); A.v(i + 1, x1, y1);
+        if (S.synb) {
+          fl = (uint32_t)S.syn(i) | (S.syn(i > s ? i - 1 : e - 2) ? 2u : 0u) | (S.syn(i + 2 < e ? i + 1 : s) ? 4u : 0u);
+        }
+        in = !edge_outside(x0, y0, x1, y1, ov);
+      }
+      const unsigned m = __ballot_sync(0xffffffffu, in);
+      const int pos = cnt + __popc(m & lt);
+      if (in && pos < cap) { L.x0[pos] = x0; L.y0[pos] = y0; L.x1[pos] = x1; L.y1[pos] = y1; L.fl[pos] = fl; }
+      cnt += __popc(m);
+    }
+  }
+  return cnt;
+}
+
+// crossing parity of segment (B's bbox left edge - 1, my) -> (mx, my) over all of B's edges (engine.cuh:382-397)
+__device__ bool pip_full_warp(const Frame& B, double mx, double my, int lane) {
+  const DLayer& S = *B.L;
+  const double ox = B.shx - (double)1, oy = my;
+  bool par = false;
+  for (uint32_t r = B.r0; r < B.r1; r++) {
+    const uint64_t s = S.rvo[r], e = S.rvo[r + 1];
+    for (uint64_t j = s + 1 + lane; j < e; j += 32) {
+      double x0, y0, x1, y1; B.v(j - 1, x0, y0); B.v(j, x1, y1);
+      if ((y0 > my) == (y1 > my) && y0 != my && y1 != my) continue;
+      bool so = left_of(x0, y0, x1, y1, ox, oy), sc = left_of(x0, y0, x1, y1, mx, my);
+      if (so == sc) continue;
+      bool su = orient(ox, oy, mx, my, x0, y0) > 0, sv = orient(ox, oy, mx, my, x1, y1) > 0;
+      if (su != sv) par = !par;
+    }
+  }
+  return (__popc(__ballot_sync(0xffffffffu, par)) & 1) != 0;
+}
+
+// inside(x) = inside(c) xor crossings of c -> x with the local edges (engine.cuh:400-412)
+__device__ __forceinline__ bool inside_from_c(const EList& L, int cnt, double cx, double cy, bool in_c, double x, double y) {
+  bool in = in_c;
+  const double sx0 = fmin(cx, x), sx1 = fmax(cx, x), sy0 = fmin(cy, y), sy1 = fmax(cy, y);
+  for (int k = 0; k < cnt; k++) {
+    const double ex0 = L.x0[k], ey0 = L.y0[k], ex1 = L.x1[k], ey1 = L.y1[k];
+    if (fmax(ex0, ex1) < sx0 || fmin(ex0, ex1) > sx1 || fmax(ey0, ey1) < sy0 || fmin(ey0, ey1) > sy1) continue;
+    bool sc = left_of(ex0, ey0, ex1, ey1, cx, cy), sx = left_of(ex0, ey0, ex1, ey1, x, y);
+    if (sc == sx) continue;
+    bool su = orient(cx, cy, x, y, ex0, ey0) > 0, sv = orient(cx, cy, x, y, ex1, ey1) > 0;
+    if (su != sv) in = !in;
+  }
+  return in;
+}
+
+struct PairGeo { Box ov; double tol, eps_par, snap, cx, cy; };
+
+// Green's-theorem contribution of edge p->q within the other polygon + relate lengths (engine.cuh:416-515)
+__device__ double edge_contrib(double px, double py, double qx, double qy, const EList& L, int cnt, bool in_c, const PairGeo& G, bool real,
+                               double* l_in, double* l_on, uint32_t* bits, uint32_t cut) {
+  const double dx = qx - px, dy = qy - py;
+  const double len2 = dx * dx + dy * dy;
+  if (len2 == 0) return 0.0;
+  const double tol = G.tol;
+  const double tol2len2 = tol * tol * len2, eps2 = G.eps_par * G.eps_par;
+  double ts[MAXS]; int ns = 0;
+  double ol0[MAXO], ol1[MAXO]; bool osame[MAXO]; int oidx[MAXO]; int no = 0;
+  ts[ns++] = 0; ts[ns++] = 1;
+  const double bx0 = fmin(px, qx) - tol, bx1 = fmax(px, qx) + tol, by0 = fmin(py, qy) - tol, by1 = fmax(py, qy) + tol;
+  const double snap2 = G.snap * G.snap;
+  for (int k = 0; k < cnt; k++) {
+    const double ex0 = L.x0[k], ey0 = L.y0[k], ex1 = L.x1[k], ey1 = L.y1[k];
+    if (fmax(ex0, ex1) < bx0 || fmin(ex0, ex1) > bx1 || fmax(ey0, ey1) < by0 || fmin(ey0, ey1) > by1) continue;
+    const uint32_t efl = L.fl[k];
+    const double fx = ex1 - ex0, fy = ey1 - ey0;
+    const double r = dx * fy - dy * fx;
+    const double flen2 = fx * fx + fy * fy;
+    const double c0 = orient(px, py, qx, qy, ex0, ey0), c1 = orient(px, py, qx, qy, ex1, ey1);
+    bool col = (c0 * c0 <= snap2 * len2 || ((efl & 2u) && c0 * c0 <= tol2len2)) && (c1 * c1 <= snap2 * len2 || ((efl & 4u) && c1 * c1 <= tol2len2));
+    if (!col && flen2 > 0) {
+      const double g0 = orient(ex0, ey0, ex1, ey1, px, py), g1 = orient(ex0, ey0, ex1, ey1, qx, qy), tf = tol * tol * flen2;
+      col = (g0 * g0 <= snap2 * flen2 || ((cut & 2u) && g0 * g0 <= tf)) && (g1 * g1 <= snap2 * flen2 || ((cut & 4u) && g1 * g1 <= tf));
+    }
+    if (col) {
+      const double tc = ((ex0 - px) * dx + (ey0 - py) * dy) / len2, te = ((ex1 - px) * dx + (ey1 - py) * dy) / len2;
+      const double lo = fmax((double)0, fmin(tc, te)), hi = fmin((double)1, fmax(tc, te));
+      if (hi > lo) {
+        if (lo > 0 && ns < MAXS) ts[ns++] = lo;
+        if (hi < 1 && ns < MAXS) ts[ns++] = hi;
+        if (no < MAXO) { ol0[no] = lo; ol1[no] = hi; osame[no] = (dx * fx + dy * fy) > 0; oidx[no] = k; no++; }
+      }
+    } else if (r * r > eps2 * len2 * flen2) {
+      const double wx = ex0 - px, wy = ey0 - py;
+      const double tn = wx * fy - wy * fx;
+      if (r > 0 ? (tn <= 0 || tn >= r) : (tn >= 0 || tn <= r)) continue;
+      const double t = tn / r, u = (wx * dy - wy * dx) / r;
+      const double du = tol / (flen2 > 0 ? sqrt(flen2) : (double)1);
+      if (u >= -du && u <= 1 + du && ns < MAXS) ts[ns++] = t;
+    }
+  }
+  for (int a = 1; a < ns; a++) { double v = ts[a]; int b = a - 1; while (b >= 0 && ts[b] > v) { ts[b + 1] = ts[b]; b--; } ts[b + 1] = v; }
+  double acc = 0.0;
+  for (int k = 0; k + 1 < ns; k++) {
+    const double t0 = ts[k], t1 = ts[k + 1];
+    if (!(t1 > t0)) continue;
+    const double tm = (double)0.5 * (t0 + t1);
+    const double mx = px + dx * tm, my = py + dy * tm;
+    const bool in_ov = mx >= G.ov.x0 && mx <= G.ov.x1 && my >= G.ov.y0 && my <= G.ov.y1;
+    int net = 0, first = -1, net_real = 0, n_real = 0;
+    for (int o = 0; o < no; o++)
+      if (tm > ol0[o] && tm < ol1[o]) {
+        const int sgn = osame[o] ? 1 : -1;
+        net += sgn; if (first < 0) first = o;
+        if (!(L.fl[oidx[o]] & 1u)) { net_real += sgn; n_real++; }
+      }
+    int vin = -1;
+    auto inside_m = [&]() {
+      if (vin < 0) vin = (in_ov && inside_from_c(L, cnt, G.cx, G.cy, in_c, mx, my)) ? 1 : 0;
+      return vin;
+    };
+    if (l_in && real) {
+      const double seg = sqrt(len2) * (t1 - t0);
+      if (net_real != 0) { *l_on += seg; *bits |= (net_real > 0 ? REL_COIN_SAME : REL_COIN_OPP) | REL_TOUCH; }
+      else if (n_real == 0 && (net == 1 || net == -1)) *l_in += 0.5 * seg;
+      else if (inside_m()) *l_in += seg;
+    }
+    double w;
+    if (first < 0) w = inside_m() ? 1.0 : 0.0;
+    else if (net == 1 || net == -1) w = 0.5;
+    else if (net == 0) w = inside_m() ? 1.0 : 0.0;
+    else {
+      const int fo = oidx[first];
+      const bool sb = left_of(L.x0[fo], L.y0[fo], L.x1[fo], L.y1[fo], mx, my);
+      const bool m_left = osame[first] ? sb : !sb;
+      const int v = inside_m();
+      int other = m_left ? v - net : v + net;
+      other = other < 0 ? 0 : (other > 1 ? 1 : other);
+      w = 0.5 * (v + other);
+    }
+    if (w != 0.0) {
+      const double ax = px + dx * t0 - G.cx, ay = py + dy * t0 - G.cy, bx = px + dx * t1 - G.cx, by = py + dy * t1 - G.cy;
+      acc += w * (double)(ax * by - ay * bx);
+    }
+  }
+  return acc;
+}
+
+__device__ __forceinline__ bool probe_vertex(const Frame& A, uint32_t r, double& x, double& y) {   // engine.cuh:322-327
+  const DLayer& S = *A.L;
+  uint64_t v = S.rvo[r], e = S.rvo[r + 1];
+  if (S.synb) { while (v + 1 < e && S.syn(v)) v++; if (v + 1 >= e) return false; }
+  A.v(v, x, y);
+  return true;
+}
+
+__device__ __forceinline__ double pair_snap(double2 oa, double2 ea) {   // engine.cuh:524-527
+  double m = fmax(fmax(fabs(oa.x), fabs(oa.x + ea.x)), fmax(fabs(oa.y), fabs(oa.y + ea.y)));
+  return 0.5 * (nextafter(m, INFINITY) - m);
+}
+
+__device__ __forceinline__ double warp_sum(double v) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// One pair, whole warp. Returns false when a local list exceeded cap (nothing written).
+__device__ bool refine_pair(const DLayer& P, const DLayer& R, uint32_t a, uint32_t b, const RefineArgs& rp, EList LA, EList LB, int cap,
+                            int lane, uint8_t& o_flag, double& o_area, double4& o_ev, uint32_t& o_evb) {
+  const double2 oa = P.origin[a], ob = R.origin[b], ea = P.ext[a], eb = R.ext[b];
+  const double sx = ob.x - oa.x, sy = ob.y - oa.y;
+  const double pad = 4.0 * fmax(rp.tol_abs, (double)rp.tol_rel * fmax(fmax(ea.x, ea.y), fmax(eb.x, eb.y)));
+  PairGeo G;
+  G.ov = Box{fmax(0.0, sx) - pad, fmax(0.0, sy) - pad, fmin(ea.x, sx + eb.x) + pad, fmin(ea.y, sy + eb.y) + pad};
+  const Frame A = frame_of(P, a, oa.x, oa.y), B = frame_of(R, b, oa.x, oa.y);
+  G.tol = fmax(rp.tol_abs, (double)rp.tol_rel * fmax(G.ov.x1 - G.ov.x0, G.ov.y1 - G.ov.y0));
+  G.eps_par = rp.eps_par;
+  G.snap = rp.snap_half_ulp ? pair_snap(oa, ea) : 0.0;
+  const int na = collect(A, G.ov, LA, cap, lane);
+  const int nb = collect(B, G.ov, LB, cap, lane);
+  if (na > cap || nb > cap) return false;
+  __syncwarp();
+  // boundary contact
+  bool hit = false, hit_any = false;
+  for (int i = lane; i < na && !hit; i += 32) {
+    const double px0 = LA.x0[i], py0 = LA.y0[i], px1 = LA.x1[i], py1 = LA.y1[i];
+    const uint32_t fa = LA.fl[i];
+    const double ax0 = fmin(px0, px1), ax1 = fmax(px0, px1), ay0 = fmin(py0, py1), ay1 = fmax(py0, py1);
+    for (int j = 0; j < nb; j++) {
+      const double qx0 = LB.x0[j], qy0 = LB.y0[j], qx1 = LB.x1[j], qy1 = LB.y1[j];
+      if (fmax(qx0, qx1) < ax0 || fmin(qx0, qx1) > ax1 || fmax(qy0, qy1) < ay0 || fmin(qy0, qy1) > ay1) continue;
+      if (seg_isect(px0, py0, px1, py1, qx0, qy0, qx1, qy1)) {
+        hit_any = true;
+        if (!((fa | LB.fl[j]) & 1u)) { hit = true; break; }
+      }
+    }
+  }
+  hit = __any_sync(0xffffffffu, hit);
+  hit_any = __any_sync(0xffffffffu, hit_any || hit);
+  const bool rtouch = hit;
+  G.cx = (double)(G.ov.x0 + 0.381966 * (G.ov.x1 - G.ov.x0));
+  G.cy = (double)(G.ov.y0 + 0.414213 * (G.ov.y1 - G.ov.y0));
+  bool inB_c = false, inA_c = false;
+  if (!hit || rp.want_area || rp.want_relate) { inB_c = pip_full_warp(B, G.cx, G.cy, lane); inA_c = pip_full_warp(A, G.cx, G.cy, lane); }
+  bool contain_any = false;
+  if (!hit) {
+    // no real boundary contact: intersects iff a real-edge vertex of one lies inside the other (engine.cuh:577-594)
+    bool h = false, ha = false;
+    for (uint32_t r = A.r0 + lane; r < A.r1 && !h; r += 32) {
+      double x, y; const bool real = probe_vertex(A, r, x, y);
+      if (!real) A.v(P.rvo[r], x, y);
+      if (x >= G.ov.x0 && x <= G.ov.x1 && y >= G.ov.y0 && y <= G.ov.y1 && inside_from_c(LB, nb, G.cx, G.cy, inB_c, x, y)) { ha = true; h = real; }
+    }
+    for (uint32_t r = B.r0 + lane; r < B.r1 && !h; r += 32) {
+      double x, y; const bool real = probe_vertex(B, r, x, y);
+      if (!real) B.v(R.rvo[r], x, y);
+      if (x >= G.ov.x0 && x <= G.ov.x1 && y >= G.ov.y0 && y <= G.ov.y1 && inside_from_c(LA, na, G.cx, G.cy, inA_c, x, y)) { ha = true; h = real; }
+    }
+    hit = __any_sync(0xffffffffu, h);
+    contain_any = __any_sync(0xffffffffu, ha);
+  }
+  double ar = 0.0; double4 e4 = make_double4(0, 0, 0, 0); uint32_t eb4 = 0;
+  if ((hit || hit_any || contain_any) && (rp.want_area || rp.want_relate)) {
+    double s2 = 0.0, ai = 0, ao = 0, bi = 0, bo = 0;
+    uint32_t bits = rtouch ? REL_TOUCH : 0;
+    const bool rel = rp.want_relate != 0;
+    for (int i = lane; i < na; i += 32) {
+      const uint32_t f = LA.fl[i];
+      s2 += edge_contrib(LA.x0[i], LA.y0[i], LA.x1[i], LA.y1[i], LB, nb, inB_c, G, !(f & 1u), rel ? &ai : nullptr, &ao, &bits, f);
+    }
+    for (int i = lane; i < nb; i += 32) {
+      const uint32_t f = LB.fl[i];
+      s2 += edge_contrib(LB.x0[i], LB.y0[i], LB.x1[i], LB.y1[i], LA, na, inA_c, G, !(f & 1u), rel ? &bi : nullptr, &bo, &bits, f);
+    }
+    s2 = warp_sum(s2); ai = warp_sum(ai); ao = warp_sum(ao); bi = warp_sum(bi); bo = warp_sum(bo);
+    ar = 0.5 * s2;
+    e4 = make_double4(ai, ao, bi, bo);
+    eb4 = __reduce_or_sync(0xffffffffu, bits);
+  } else if (rtouch) eb4 = REL_TOUCH;
+  const bool ev_any = e4.x != 0 || e4.y != 0 || e4.z != 0 || e4.w != 0;
+  o_flag = hit ? 1 : ((ar != 0.0 || ev_any) ? 2 : 0);
+  o_area = ar; o_ev = e4; o_evb = eb4;
+  return true;
+}
+
+__global__ void __launch_bounds__(RB_WARPS * 32) k_refine(DLayer P, DLayer R, const uint2* __restrict__ pairs, uint64_t np, RefineArgs rp,
+                                                          uint8_t* flag, double* area, double4* ev, uint32_t* evb, uint32_t* heavy,
+                                                          unsigned long long* nheavy) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  EList LA = carve(smem + (size_t)wib * 2 * LIST_BYTES, CAP);
+  EList LB = carve(smem + (size_t)wib * 2 * LIST_BYTES + LIST_BYTES, CAP);
+  const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  for (uint64_t p = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; p < np; p += nw) {
+    const uint2 pr = pairs[p];
+    uint8_t f; double ar; double4 e4; uint32_t b4;
+    const bool ok = refine_pair(P, R, pr.x, pr.y, rp, LA, LB, CAP, lane, f, ar, e4, b4);
+    if (lane == 0) {
+      if (!ok) { heavy[atomicAdd(nheavy, 1ull)] = (uint32_t)p; flag[p] = 0; }
+      else {
+        flag[p] = f;
+        if (area) area[p] = ar;
+        if (ev) { ev[p] = e4; evb[p] = b4; }
+      }
+    }
+    __syncwarp();
+  }
+}
+
+// oversized pairs: the same pair routine with per-warp edge lists in global scratch
+__global__ void __launch_bounds__(128) k_refine_scratch(DLayer P, DLayer R, const uint2* __restrict__ pairs, const uint32_t* __restrict__ heavy,
+                                                       uint64_t nh, RefineArgs rp, uint8_t* flag, double* area, double4* ev, uint32_t* evb,
+                                                       unsigned char* scratch, int cap, int* err) {
+  const int lane = threadIdx.x & 31;
+  const uint64_t w = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  unsigned char* base = scratch + w * 2 * (size_t)cap * EDGE_BYTES;
+  EList LA = carve(base, cap), LB = carve(base + (size_t)cap * EDGE_BYTES, cap);
+  for (uint64_t h = w; h < nh; h += nw) {
+    const uint32_t p = heavy[h];
+    const uint2 pr = pairs[p];
+    uint8_t f; double ar; double4 e4; uint32_t b4;
+    const bool ok = refine_pair(P, R, pr.x, pr.y, rp, LA, LB, cap, lane, f, ar, e4, b4);
+    if (lane == 0) {
+      if (!ok) *err = 1;
+      else {
+        flag[p] = f;
+        if (area) area[p] = ar;
+        if (ev) { ev[p] = e4; evb[p] = b4; }
+      }
+    }
+    __syncwarp();
+  }
+}
+
+uint64_t refine(gsj_ctx* c, const gsj_layer* P, const gsj_layer* R, const uint2* pairs, uint64_t np, const RefineArgs& rp, int mode,
+                uint8_t* flag, double* area, double4* ev, uint32_t* evb) {
+  (void)mode;
+  if (!np) return 0;
+  cudaStream_t s = c->stream;
+  if (!c->refine_attr) { GSJ_CK(cudaFuncSetAttribute(k_refine, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)RB_SMEM)); c->refine_attr = 1; }
+  unsigned long long* ctr = c->counters.as<unsigned long long>(8);
+  int* err = reinterpret_cast<int*>(ctr + 1);
+  GSJ_CK(cudaMemsetAsync(ctr, 0, 16, s));
+  uint32_t* heavy = c->heavy.as<uint32_t>(np);
+  const int blocks = (int)std::min<uint64_t>((np + RB_WARPS - 1) / RB_WARPS, (uint64_t)c->sm_count * 6);
+  k_refine<<<blocks, RB_WARPS * 32, RB_SMEM, s>>>(P->d, R->d, pairs, np, rp, flag, area, ev, evb, heavy, ctr);
+  GSJ_CK(cudaGetLastError());
+  unsigned long long* h = c->h_counters.as<unsigned long long>(2);
+  GSJ_CK(cudaMemcpyAsync(h, ctr, 16, cudaMemcpyDeviceToHost, s));
+  GSJ_CK(cudaStreamSynchronize(s));
+  const uint64_t nh = h[0];
+  if (nh) {
+    // list capacity rounded to 8 edges keeps every double array of the slab 8-byte aligned
+    const int cap = (int)((std::max<uint32_t>(std::max(P->max_geom_edges, R->max_geom_edges), 1u) + 7u) & ~7u);
+    const size_t per = 2 * (size_t)cap * EDGE_BYTES;
+    uint64_t nwarps = std::min<uint64_t>(nh, std::max<uint64_t>(1, (1ull << 30) / per));
+    nwarps = std::min<uint64_t>(nwarps, (uint64_t)c->sm_count * 32);
+    nwarps = (nwarps + 3) / 4 * 4;
+    unsigned char* scr = c->scratch.as<unsigned char>(per * nwarps);
+    GSJ_CK(cudaMemsetAsync(err, 0, 4, s));
+    k_refine_scratch<<<(int)(nwarps / 4), 128, 0, s>>>(P->d, R->d, pairs, heavy, nh, rp, flag, area, ev, evb, scr, cap, err);
+    GSJ_CK(cudaGetLastError());
+    GSJ_CK(cudaMemcpyAsync(h, ctr, 16, cudaMemcpyDeviceToHost, s));
+    GSJ_CK(cudaStreamSynchronize(s));
+    if (reinterpret_cast<int*>(h + 1)[0]) throw Error(GSJ_ERR_CUDA, "oversized pair exceeded the scratch edge capacity");
+  }
+  return nh;
+}
+
+}  // namespace gsj

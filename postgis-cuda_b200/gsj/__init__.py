@@ -1,0 +1,310 @@
+"""Python binding of the gsj C ABI (include/gsj.h) over ctypes.
+
+The engine is ``_build/libgsj.so`` (hand-written sm_100a kernels + C++ host drivers). This module only moves
+host arrays in and out; every join runs in the library. There is no CPU fallback: without a CUDA device (or
+without the built library) the calls raise.
+"""
+from __future__ import annotations
+
+import ctypes
+import dataclasses
+
+import numpy as np
+
+from ._build import lib_path
+
+GSJ_REFINE_PLAIN = 0
+GSJ_REFINE_FILTERED = 1
+
+_u32p = ctypes.POINTER(ctypes.c_uint32)
+_f64p = ctypes.POINTER(ctypes.c_double)
+_u8p = ctypes.POINTER(ctypes.c_uint8)
+_vp = ctypes.c_void_p
+
+JOIN_SINK = ctypes.CFUNCTYPE(ctypes.c_int, _vp, _u32p, _f64p, _u32p, ctypes.c_uint64)
+POINTS_SINK = ctypes.CFUNCTYPE(ctypes.c_int, _vp, _u32p, _u8p, ctypes.c_uint64)
+PAIRS_SINK = ctypes.CFUNCTYPE(ctypes.c_int, _vp, _u32p, ctypes.c_uint64)
+
+
+class RefineParams(ctypes.Structure):
+    _fields_ = [("tol_rel", ctypes.c_double), ("eps_par", ctypes.c_double), ("tol_abs", ctypes.c_double),
+                ("want_area", ctypes.c_int), ("want_relate", ctypes.c_int), ("snap_half_ulp", ctypes.c_int)]
+
+
+class JoinOpts(ctypes.Structure):
+    _fields_ = [("batch_q", ctypes.c_uint32), ("max_pairs", ctypes.c_uint64), ("upper", ctypes.c_int), ("no_agg", ctypes.c_int),
+                ("refine_mode", ctypes.c_int), ("cancel", ctypes.POINTER(ctypes.c_int))]
+
+
+class JoinStats(ctypes.Structure):
+    _fields_ = [("traverse_ms", ctypes.c_double), ("refine_ms", ctypes.c_double), ("compact_ms", ctypes.c_double),
+                ("copy_ms", ctypes.c_double), ("candidates", ctypes.c_uint64), ("hits", ctypes.c_uint64), ("heavy", ctypes.c_uint64),
+                ("batches", ctypes.c_uint64)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class LayerInfo(ctypes.Structure):
+    _fields_ = [("n", ctypes.c_uint64), ("nr", ctypes.c_uint64), ("nv", ctypes.c_uint64), ("nparent", ctypes.c_uint32),
+                ("is_points", ctypes.c_int), ("max_geom_edges", ctypes.c_uint32), ("device_bytes", ctypes.c_uint64)]
+
+
+class GsjError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"gsj error {code}: {msg}")
+        self.code = code
+
+
+_lib = None
+
+# exported symbols with their ctypes signatures (restype, argtypes)
+SIGNATURES = {
+    "gsj_ctx_create": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(_vp)]),
+    "gsj_ctx_destroy": (None, [_vp]),
+    "gsj_last_error": (ctypes.c_char_p, [_vp]),
+    "gsj_ctx_mem_info": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_int)]),
+    "gsj_layer_upload_polygons": (ctypes.c_int, [_vp, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64, _vp, _vp, _vp, _vp, _vp,
+                                                 ctypes.POINTER(_vp)]),
+    "gsj_layer_upload_points": (ctypes.c_int, [_vp, ctypes.c_uint64, _vp, ctypes.POINTER(_vp)]),
+    "gsj_layer_free": (None, [_vp, _vp]),
+    "gsj_layer_get_info": (ctypes.c_int, [_vp, ctypes.POINTER(LayerInfo)]),
+    "gsj_refine_params_default": (None, [ctypes.POINTER(RefineParams)]),
+    "gsj_join_opts_default": (None, [ctypes.POINTER(JoinOpts)]),
+    "gsj_join": (ctypes.c_int, [_vp, _vp, _vp, ctypes.POINTER(RefineParams), ctypes.POINTER(JoinOpts), JOIN_SINK, _vp, ctypes.POINTER(JoinStats)]),
+    "gsj_join_points": (ctypes.c_int, [_vp, _vp, _vp, ctypes.POINTER(JoinOpts), POINTS_SINK, _vp, ctypes.POINTER(JoinStats)]),
+    "gsj_cluster": (ctypes.c_int, [_vp, _vp, ctypes.c_uint32, ctypes.POINTER(JoinOpts), _vp, ctypes.POINTER(JoinStats)]),
+    "gsj_dwithin": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_double, ctypes.c_int, ctypes.POINTER(JoinOpts), PAIRS_SINK, _vp,
+                                   ctypes.POINTER(JoinStats)]),
+    "gsj_erode": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_double, ctypes.c_double, ctypes.c_int, _vp, ctypes.POINTER(JoinOpts), PAIRS_SINK,
+                                 _vp, ctypes.POINTER(JoinStats)]),
+    "gsj_points_dwithin": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_double, ctypes.POINTER(JoinOpts), PAIRS_SINK, _vp, ctypes.POINTER(JoinStats)]),
+    "gsj_points_erode": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_double, ctypes.POINTER(JoinOpts), PAIRS_SINK, _vp, ctypes.POINTER(JoinStats)]),
+    "gsj_candidates": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_int, PAIRS_SINK, _vp]),
+    "gsj_refine_pairs": (ctypes.c_int, [_vp, _vp, _vp, _vp, ctypes.c_uint64, ctypes.POINTER(RefineParams), ctypes.c_int, _vp, _vp, _vp, _vp]),
+    "gsj_de9im_str": (None, [ctypes.c_uint32, ctypes.c_char_p]),
+    "gsj_de9im_transpose": (ctypes.c_uint32, [ctypes.c_uint32]),
+    "gsj_de9im_match": (ctypes.c_int, [ctypes.c_uint32, ctypes.c_char_p]),
+}
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        L = ctypes.CDLL(lib_path("libgsj.so"))
+        for name, (res, args) in SIGNATURES.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def refine_params(want_area=True, want_relate=False, snap_half_ulp=False) -> RefineParams:
+    p = RefineParams()
+    lib().gsj_refine_params_default(ctypes.byref(p))
+    p.want_area, p.want_relate, p.snap_half_ulp = int(want_area), int(want_relate), int(snap_half_ulp)
+    return p
+
+
+def join_opts(upper=False, no_agg=False, refine_mode=GSJ_REFINE_FILTERED, batch_q=0) -> JoinOpts:
+    o = JoinOpts()
+    lib().gsj_join_opts_default(ctypes.byref(o))
+    o.upper, o.no_agg, o.refine_mode, o.batch_q = int(upper), int(no_agg), int(refine_mode), int(batch_q)
+    return o
+
+
+def de9im_str(code: int) -> str:
+    b = ctypes.create_string_buffer(10)
+    lib().gsj_de9im_str(code, b)
+    return b.raw[:9].decode()
+
+
+def de9im_transpose(code: int) -> int:
+    return lib().gsj_de9im_transpose(code)
+
+
+def de9im_match(code: int, pattern: str) -> bool:
+    return bool(lib().gsj_de9im_match(code, pattern.encode()))
+
+
+@dataclasses.dataclass
+class JoinResult:
+    pairs: np.ndarray          # (n, 2) uint32: (P parent, R parent)
+    area: np.ndarray | None    # (n,) float64
+    code: np.ndarray | None    # (n,) uint32 DE-9IM codes
+    stats: dict
+
+
+class Layer:
+    def __init__(self, eng: "Engine", handle, keep=()):
+        self.eng, self.h = eng, handle
+        self._keep = keep
+        info = LayerInfo()
+        lib().gsj_layer_get_info(handle, ctypes.byref(info))
+        self.info = {k: getattr(info, k) for k, _ in LayerInfo._fields_}
+
+    @property
+    def n(self):
+        return self.info["n"]
+
+    def free(self):
+        if self.h:
+            lib().gsj_layer_free(self.eng.ctx, self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            if self.h and self.eng.ctx:
+                self.free()
+        except Exception:
+            pass
+
+
+class Engine:
+    """One gsj context on a CUDA device."""
+
+    def __init__(self, device: int = 0):
+        h = _vp()
+        rc = lib().gsj_ctx_create(device, ctypes.byref(h))
+        if rc:
+            raise GsjError(rc, "cannot create a context (no CUDA device?)")
+        self.ctx = h
+
+    def close(self):
+        if self.ctx:
+            lib().gsj_ctx_destroy(self.ctx)
+            self.ctx = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc):
+        if rc:
+            raise GsjError(rc, lib().gsj_last_error(self.ctx).decode(errors="replace"))
+
+    def mem_info(self):
+        f, t, s = ctypes.c_uint64(), ctypes.c_uint64(), ctypes.c_int()
+        self._check(lib().gsj_ctx_mem_info(self.ctx, ctypes.byref(f), ctypes.byref(t), ctypes.byref(s)))
+        return f.value, t.value, s.value
+
+    # ---- layers ----
+    def upload_polygons(self, ps, parent=None, syn=None) -> Layer:
+        gro = np.ascontiguousarray(ps.gro, dtype=np.uint64)
+        rvo = np.ascontiguousarray(ps.rvo, dtype=np.uint64)
+        xy = np.ascontiguousarray(ps.xy, dtype=np.float64)
+        parent = parent if parent is not None else getattr(ps, "parent", None)
+        syn = syn if syn is not None else getattr(ps, "syn", None)
+        par = None if parent is None else np.ascontiguousarray(parent, dtype=np.uint32)
+        sy = None if syn is None else np.ascontiguousarray(syn, dtype=np.uint8)
+        h = _vp()
+        self._check(lib().gsj_layer_upload_polygons(self.ctx, len(gro) - 1, len(rvo) - 1, len(xy), gro.ctypes.data, rvo.ctypes.data,
+                                                     xy.ctypes.data, None if par is None else par.ctypes.data,
+                                                     None if sy is None else sy.ctypes.data, ctypes.byref(h)))
+        return Layer(self, h)
+
+    def upload_points(self, xy) -> Layer:
+        xy = np.ascontiguousarray(xy, dtype=np.float64)
+        h = _vp()
+        self._check(lib().gsj_layer_upload_points(self.ctx, len(xy), xy.ctypes.data, ctypes.byref(h)))
+        return Layer(self, h)
+
+    # ---- joins ----
+    def join(self, P: Layer, R: Layer, want_area=True, want_relate=False, upper=False, no_agg=False,
+             refine_mode=GSJ_REFINE_FILTERED, batch_q=0, snap_half_ulp=False) -> JoinResult:
+        rp = refine_params(want_area, want_relate, snap_half_ulp)
+        o = join_opts(upper, no_agg, refine_mode, batch_q)
+        chunks_p, chunks_a, chunks_c = [], [], []
+
+        def sink(user, pairs, area, code, n):
+            chunks_p.append(np.ctypeslib.as_array(pairs, (n * 2,)).copy())
+            if area:
+                chunks_a.append(np.ctypeslib.as_array(area, (n,)).copy())
+            if code:
+                chunks_c.append(np.ctypeslib.as_array(code, (n,)).copy())
+            return 0
+
+        cb = JOIN_SINK(sink)
+        st = JoinStats()
+        self._check(lib().gsj_join(self.ctx, P.h, R.h, ctypes.byref(rp), ctypes.byref(o), cb, None, ctypes.byref(st)))
+        pairs = np.concatenate(chunks_p).reshape(-1, 2) if chunks_p else np.zeros((0, 2), np.uint32)
+        area = (np.concatenate(chunks_a) if chunks_a else np.zeros(0)) if want_area else None
+        code = (np.concatenate(chunks_c) if chunks_c else np.zeros(0, np.uint32)) if want_relate else None
+        return JoinResult(pairs, area, code, st.as_dict())
+
+    def join_points(self, pts: Layer, R: Layer, batch_q=0):
+        o = join_opts(batch_q=batch_q)
+        cp, cw = [], []
+
+        def sink(user, pairs, where, n):
+            cp.append(np.ctypeslib.as_array(pairs, (n * 2,)).copy())
+            cw.append(np.ctypeslib.as_array(where, (n,)).copy())
+            return 0
+
+        cb = POINTS_SINK(sink)
+        st = JoinStats()
+        self._check(lib().gsj_join_points(self.ctx, pts.h, R.h, ctypes.byref(o), cb, None, ctypes.byref(st)))
+        pairs = np.concatenate(cp).reshape(-1, 2) if cp else np.zeros((0, 2), np.uint32)
+        where = np.concatenate(cw) if cw else np.zeros(0, np.uint8)
+        return pairs, where, st.as_dict()
+
+    def cluster(self, P: Layer, nparent: int | None = None):
+        nparent = P.info["nparent"] if nparent is None else nparent
+        root = np.empty(nparent, np.uint32)
+        st = JoinStats()
+        o = join_opts()
+        self._check(lib().gsj_cluster(self.ctx, P.h, nparent, ctypes.byref(o), root.ctypes.data, ctypes.byref(st)))
+        return root, st.as_dict()
+
+    def _pairs_call(self, fn, *args, opts=None):
+        chunks = []
+
+        def sink(user, pairs, n):
+            chunks.append(np.ctypeslib.as_array(pairs, (n * 2,)).copy())
+            return 0
+
+        cb = PAIRS_SINK(sink)
+        st = JoinStats()
+        o = opts if opts is not None else join_opts()
+        self._check(fn(self.ctx, *args, ctypes.byref(o), cb, None, ctypes.byref(st)))
+        pairs = np.concatenate(chunks).reshape(-1, 2) if chunks else np.zeros((0, 2), np.uint32)
+        return pairs, st.as_dict()
+
+    def dwithin(self, P: Layer, R: Layer, d: float, same=False, upper=None):
+        o = join_opts(upper=same if upper is None else upper)
+        return self._pairs_call(lib().gsj_dwithin, P.h, R.h, float(d), int(same), opts=o)
+
+    def erode(self, P: Layer, R: Layer, ra: float, rb: float, same=False, need_self=None):
+        ns = None if need_self is None else np.ascontiguousarray(need_self, dtype=np.uint8)
+        o = join_opts(upper=same)
+        return self._pairs_call(lib().gsj_erode, P.h, R.h, float(ra), float(rb), int(same), None if ns is None else ns.ctypes.data, opts=o)
+
+    def points_dwithin(self, pts: Layer, R: Layer, d: float):
+        return self._pairs_call(lib().gsj_points_dwithin, pts.h, R.h, float(d))
+
+    def points_erode(self, pts: Layer, R: Layer, r: float):
+        return self._pairs_call(lib().gsj_points_erode, pts.h, R.h, float(r))
+
+    # ---- parity / diagnostics ----
+    def candidates(self, P: Layer, R: Layer, upper=False) -> np.ndarray:
+        chunks = []
+
+        def sink(user, pairs, n):
+            chunks.append(np.ctypeslib.as_array(pairs, (n * 2,)).copy())
+            return 0
+
+        cb = PAIRS_SINK(sink)
+        self._check(lib().gsj_candidates(self.ctx, P.h, R.h, int(upper), cb, None))
+        return np.concatenate(chunks).reshape(-1, 2) if chunks else np.zeros((0, 2), np.uint32)
+
+    def refine_pairs(self, P: Layer, R: Layer, pairs, want_area=True, want_relate=False, refine_mode=GSJ_REFINE_FILTERED, snap_half_ulp=False):
+        pairs = np.ascontiguousarray(pairs, dtype=np.uint32)
+        n = len(pairs)
+        flag = np.zeros(n, np.uint8); area = np.zeros(n); ev = np.zeros((n, 4)); evb = np.zeros(n, np.uint32)
+        rp = refine_params(want_area, want_relate, snap_half_ulp)
+        self._check(lib().gsj_refine_pairs(self.ctx, P.h, R.h, pairs.ctypes.data, n, ctypes.byref(rp), refine_mode, flag.ctypes.data,
+                                           area.ctypes.data, ev.ctypes.data, evb.ctypes.data))
+        return flag, area, ev, evb
