@@ -1,0 +1,344 @@
+#!/usr/bin/env python3
+"""Benchmark: DE-9IM relate self-join of 2M synthetic parcels on one B200 (per rank).
+
+Workload (the configuration the headline metric is quoted on): Voronoi cells of 2M jittered-grid seeds in a
+2 x 2 degree lon/lat box (lon -119..-117, lat 33..35), 4-256 vertices per ring (log-uniform), 5% MultiPolygons
+with 2-4 parts, 2% with one interior hole; gpu_relate self-join with self_pairs 'distinct' (each unordered pair
+once, diagonal included); FP32-filtered + FP64 refinement vs the plain FP64 kernels, pair sets compared.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+A step is one full self-join of the resident layer. value = intersecting pairs / device time (CUDA events on the
+engine's stream). e2e = the same join through the C ABI from pinned host buffers: upload (H2D) + LBVH build +
+join + result D2H, every step. N > 1 (torchrun): every rank joins its own 2M-parcel layer (seed = rank), no
+data-path collective; value = all ranks' pairs / max-over-ranks time (weak scaling). --impl reference times the
+CPU FP64 restatement of the same predicates on the host cores (the reference engine has no CPU path).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "postgis-cuda_b200"))
+
+BOX = (-119.0, 33.0, -117.0, 35.0)
+N_SEEDS = 2_000_000
+METRIC = "join pairs/s (DE-9IM relate self-join, filtered+batched FP64)"
+WORKLOAD = "relate self-join, 2M jittered-grid Voronoi parcels, 2x2 deg, 4-256 vertices/ring, 5% multipolygons, 2% holes"
+
+
+def peaks():
+    try:
+        return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        return {}
+
+
+class Clocks:
+    """nvidia-smi sampler running during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu: int):
+        self.gpu, self.lines, self.p = gpu, [], None
+
+    def __enter__(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                       "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=lambda: self.lines.extend(self.p.stdout), daemon=True)
+            self.t.start()
+        except Exception:
+            self.p = None
+        return self
+
+    def __exit__(self, *a):
+        if self.p:
+            self.p.terminate()
+            try:
+                self.p.wait(5)
+            except Exception:
+                self.p.kill()
+            self.t.join(2)
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1])); mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        import torch
+        backend = "nccl" if torch.cuda.is_available() else "gloo"
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
+    return rank, local, ws
+
+
+def allreduce_max(x: float, ws: int) -> float:
+    if ws == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda" if dist.get_backend() == "nccl" else "cpu")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def allreduce_sum(x: float, ws: int) -> float:
+    if ws == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda" if dist.get_backend() == "nccl" else "cpu")
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def barrier(ws):
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def sub_layer(ps, box):
+    """Geometries of ps whose vertices all lie inside box (re-indexed), a spatially bounded sample."""
+    from gsj.gen import PolygonSet
+    gro, rvo, xy = ps.gro.astype(np.int64), ps.rvo.astype(np.int64), ps.xy
+    v0, v1 = rvo[gro[:-1]], rvo[gro[1:]]
+    vmin = np.minimum.reduceat(xy, v0, axis=0)
+    vmax = np.maximum.reduceat(xy, v0, axis=0)
+    sel = np.nonzero((vmin[:, 0] >= box[0]) & (vmin[:, 1] >= box[1]) & (vmax[:, 0] <= box[2]) & (vmax[:, 1] <= box[3]))[0]
+    ngro, nrvo, nxy = [0], [0], []
+    for g in sel:
+        for r in range(gro[g], gro[g + 1]):
+            nxy.append(xy[rvo[r]:rvo[r + 1]])
+            nrvo.append(nrvo[-1] + rvo[r + 1] - rvo[r])
+        ngro.append(len(nrvo) - 1)
+    return PolygonSet(np.array(ngro, np.uint64), np.array(nrvo, np.uint64), np.concatenate(nxy))
+
+
+def cpu_sample(ps, target_s):
+    """A corner sub-box of the layer sized so the CPU oracle's relate self-join takes about target_s here."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle as O
+    frac = 0.06
+    while True:
+        w = (BOX[2] - BOX[0]) * frac
+        sub = sub_layer(ps, (BOX[0], BOX[1], BOX[0] + w, BOX[1] + w))
+        S = O.OSet(sub)
+        t = time.perf_counter()
+        O.join(S, S, O.params(0, 1), upper=True)
+        dt = time.perf_counter() - t
+        if dt >= target_s / 3 or frac >= 1.0:
+            return S, sub, w
+        frac = min(1.0, frac * (target_s / max(dt, 0.02)) ** 0.5)
+
+
+def cpu_time(S):
+    import pyoracle as O
+    t = time.perf_counter()
+    p, a, c, nc = O.join(S, S, O.params(0, 1), upper=True)
+    dt = time.perf_counter() - t
+    return len(p), dt
+
+
+def cpu_oracle_rate(ps, target_s=15.0):
+    """The CPU FP64 oracle (OpenMP, all host threads) on a bounded spatial sample: pairs/s."""
+    S, sub, w = cpu_sample(ps, target_s)
+    n, dt = cpu_time(S)
+    return n / dt, dict(pairs=n, seconds=dt, parcels=sub.n, box_deg=w, threads=os.cpu_count())
+
+
+def run_reference(args, rank, ws):
+    """--impl reference: the CPU FP64 port of the reference's predicates, timed on the host cores."""
+    from gsj import gen
+    if rank != 0:
+        return
+    ps = gen.layer_parcels(args.seeds, BOX, seed=0)
+    S, sub, w = cpu_sample(ps, target_s=max(4.0, min(15.0, 90.0 / max(1, args.steps + args.warmup))))
+    runs = [cpu_time(S) for _ in range(args.warmup + args.steps)][args.warmup:]
+    n = runs[0][0]
+    secs = float(np.sum([r[1] for r in runs]))
+    value = n * len(runs) / secs
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "pairs/s", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1000.0 * secs / len(runs), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded Voronoi parcels)",
+            "config": {"workload": WORKLOAD, "sample": f"{sub.n} parcels in a {w:.3f} deg corner sub-box of the layer"},
+            "cpu_baseline": {"value": value, "unit": "pairs/s", "cores": os.cpu_count(), "kind": "port",
+                             "sample": f"CPU FP64 oracle (OpenMP), relate self-join of {sub.n} parcels ({n} pairs) per step"},
+            "e2e": {"value": value, "unit": "pairs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--seeds", type=int, default=N_SEEDS)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    rank, local, ws = dist_setup()
+    if args.impl == "reference":
+        run_reference(args, rank, ws)
+        barrier(ws)
+        return
+    import torch
+    import gsj
+    from gsj import gen
+
+    torch.cuda.set_device(local)
+    eng = gsj.Engine(local)
+    ext = torch.cuda.ExternalStream(eng.stream_handle(), device=local)
+    t0 = time.time()
+    ps = gen.layer_parcels(args.seeds, BOX, seed=rank)
+    t_gen = time.time() - t0
+    # pinned host copies for the end-to-end leg
+    pin = {k: torch.from_numpy(np.ascontiguousarray(getattr(ps, k))).pin_memory() for k in ("gro", "rvo", "xy")}
+    hps = gen.PolygonSet(pin["gro"].numpy(), pin["rvo"].numpy(), pin["xy"].numpy())
+    L = eng.upload_polygons(hps)
+
+    def timed_join(mode):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(ext):
+            e0.record()
+        r = eng.join(L, L, want_area=False, want_relate=True, upper=True, refine_mode=mode)
+        with torch.cuda.stream(ext):
+            e1.record()
+        e1.synchronize()
+        return r, e0.elapsed_time(e1)
+
+    for _ in range(args.warmup):
+        timed_join(gsj.GSJ_REFINE_FILTERED)
+    res = {}
+    for mode, name in ((gsj.GSJ_REFINE_FILTERED, "filtered"), (gsj.GSJ_REFINE_PLAIN, "plain")):
+        if name == "plain":
+            timed_join(mode)   # warm this variant too
+        barrier(ws)
+        torch.cuda.synchronize()
+        ms, pairs, stats = [], 0, []
+        with Clocks(local) as clk:
+            for _ in range(args.steps):
+                r, t = timed_join(mode)
+                ms.append(t); pairs += len(r.pairs); stats.append(r.stats)
+        torch.cuda.synchronize()
+        barrier(ws)
+        res[name] = dict(ms=ms, pairs=pairs, stats=stats, clocks=clk.summary(), result=r)
+    # identical results between the variants (0 pair diffs, same DE-9IM)
+    a, b = res["filtered"]["result"], res["plain"]["result"]
+    ia, ib = np.lexsort(a.pairs.T[::-1]), np.lexsort(b.pairs.T[::-1])
+    same_pairs = a.pairs.shape == b.pairs.shape and np.array_equal(a.pairs[ia], b.pairs[ib])
+    pair_diffs = 0 if same_pairs else len(set(map(tuple, a.pairs.tolist())) ^ set(map(tuple, b.pairs.tolist())))
+    code_diffs = int((a.code[ia] != b.code[ib]).sum()) if same_pairs else None
+
+    # end-to-end through the C ABI from pinned host buffers: upload + LBVH + join + D2H of the rows
+    e2e_ms, e2e_pairs = [], 0
+    for i in range(1 + args.steps):
+        t = time.perf_counter()
+        Lx = eng.upload_polygons(hps)
+        r = eng.join(Lx, Lx, want_area=False, want_relate=True, upper=True)
+        Lx.free()
+        dt = (time.perf_counter() - t) * 1000.0
+        if i:
+            e2e_ms.append(dt); e2e_pairs += len(r.pairs)
+    h2d = int(ps.gro.nbytes + ps.rvo.nbytes + ps.xy.nbytes)
+    d2h = int(len(r.pairs) * 12)
+
+    f = res["filtered"]
+    tot_ms = allreduce_max(float(np.sum(f["ms"])), ws)
+    all_pairs = allreduce_sum(float(f["pairs"]), ws)
+    value = all_pairs / (tot_ms / 1000.0)
+    plain_ms = allreduce_max(float(np.sum(res["plain"]["ms"])), ws)
+    plain_value = allreduce_sum(float(res["plain"]["pairs"]), ws) / (plain_ms / 1000.0)
+    e2e_tot = allreduce_max(float(np.sum(e2e_ms)), ws)
+    e2e_value = allreduce_sum(float(e2e_pairs), ws) / (e2e_tot / 1000.0)
+    pk = peaks()
+    # roofline of the dominant kernel (refinement): algorithmic bytes = both geometries' vertices per candidate pair
+    cand = eng.candidates(L, L, upper=True)
+    nvg = (ps.rvo[ps.gro[1:]] - ps.rvo[ps.gro[:-1]]).astype(np.int64)
+    alg_bytes = float(16 * (nvg[cand[:, 0]] + nvg[cand[:, 1]]).sum() + len(cand) * (8 + 1 + 32 + 4 + 2 * 40))
+    st = f["stats"]
+    refine_ms = float(np.mean([s["refine_ms"] for s in st]))
+    trav_ms = float(np.mean([s["traverse_ms"] for s in st]))
+    hbm = pk.get("hbm_gbs", 6650.0)
+    # algorithmic traversal bytes: 48-byte node records actually visited + probe box and order id + written pairs
+    trav_bytes = float(np.mean([s_["node_visits"] for s_ in st]) * 48 + ps.n * (16 + 4) + len(cand) * 8)
+    traffic = None
+    try:
+        for ln in open(os.path.join(ROOT, "profiles", "traffic_per_launch.txt")):
+            k, v = ln.split()[:2]
+            if k == "k_refine":
+                traffic = float(v)
+    except OSError:
+        pass
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        v, info = cpu_oracle_rate(ps)
+        cpu = {"value": v, "unit": "pairs/s", "cores": info["threads"], "kind": "port",
+               "sample": f"CPU FP64 oracle, relate self-join of {info['parcels']} parcels in a {info['box_deg']:.3f} deg corner sub-box "
+                         f"({info['pairs']} pairs, {info['seconds']:.1f} s)"}
+    lat = sorted(f["ms"])
+    line = {
+        "metric": METRIC, "value": value, "unit": "pairs/s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": tot_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded Voronoi parcels; the reference's parcel datasets are private)",
+        "config": {"workload": WORKLOAD, "parcels": int(L.info["n"]), "vertices": int(L.info["nv"]), "candidates": int(st[0]["candidates"]),
+                   "pairs_per_step": int(st[0]["hits"]), "parallelism": f"replicas x{ws} (own layer per rank)",
+                   "l2": "inputs > L2 (2.2 GB resident layer)", "gen_s": round(t_gen, 2)},
+        "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
+        "plain_fp64": {"value": plain_value, "ms_per_step": plain_ms / args.steps,
+                       "latency_ms": {"p50": float(np.percentile(res["plain"]["ms"], 50)), "p99": float(np.percentile(res["plain"]["ms"], 99))},
+                       "speedup_filtered": value / plain_value},
+        "pair_diffs_filtered_vs_plain": pair_diffs, "code_diffs_filtered_vs_plain": code_diffs,
+        "phases_ms": {k: float(np.mean([s[k] for s in st])) for k in ("traverse_ms", "refine_ms", "compact_ms", "copy_ms")},
+        "e2e": {"value": e2e_value, "unit": "pairs/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "ms_per_step": e2e_tot / args.steps},
+        "roofline": {"kernel": "k_refine (+k_refine_scratch)", "bound": "hbm", "achieved": alg_bytes / (refine_ms / 1000.0) / 1e9,
+                     "peak": hbm, "unit": "GB/s", "frac": alg_bytes / (refine_ms / 1000.0) / 1e9 / hbm, "traffic": traffic,
+                     "peak_source": "MEASURED_PEAKS.json hbm_gbs" if "hbm_gbs" in pk else "fallback",
+                     "note": "refinement is FP64-pipe / latency bound; bytes = both geometries' vertices per candidate pair"},
+        "roofline_traversal": {"kernel": "k_traverse", "bound": "hbm", "achieved": trav_bytes / (trav_ms / 1000.0) / 1e9, "peak": hbm,
+                               "unit": "GB/s", "frac": trav_bytes / (trav_ms / 1000.0) / 1e9 / hbm},
+        "gpu_launches": int(sum(s["launches"] for s in st)),
+        "clocks": f["clocks"],
+        "cpu_baseline": cpu,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    barrier(ws)
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -31,6 +31,9 @@ typedef struct gsj_layer gsj_layer;
 int gsj_ctx_create(int device, gsj_ctx** out);
 void gsj_ctx_destroy(gsj_ctx* ctx);
 const char* gsj_last_error(const gsj_ctx* ctx);
+/* The context's CUDA stream (a cudaStream_t): every kernel and copy of the context runs on it, in call order.
+ * Lets a caller bracket calls with its own CUDA events. */
+void* gsj_ctx_stream(gsj_ctx* ctx);
 /* Free device memory and the number of SMs, for admission decisions (gpujoind.cu:133-137). */
 int gsj_ctx_mem_info(gsj_ctx* ctx, uint64_t* free_bytes, uint64_t* total_bytes, int* sm_count);
 
@@ -81,6 +84,8 @@ void gsj_join_opts_default(gsj_join_opts* o);
 typedef struct gsj_join_stats {
   double traverse_ms, refine_ms, compact_ms, copy_ms;
   uint64_t candidates, hits, heavy, batches;
+  uint64_t launches;     /* kernels of this library launched by the call */
+  uint64_t node_visits;  /* LBVH nodes visited by the candidate search (48 bytes each) */
 } gsj_join_stats;
 
 /* Sink for a finished batch (the host callback of join_stream): pairs[2n] = (P index, R index) in parent ids,

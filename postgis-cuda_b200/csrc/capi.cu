@@ -70,6 +70,8 @@ void gsj_ctx_destroy(gsj_ctx* c) {
 
 const char* gsj_last_error(const gsj_ctx* c) { return c ? c->err.c_str() : "no context"; }
 
+void* gsj_ctx_stream(gsj_ctx* c) { return c ? (void*)c->stream : nullptr; }
+
 int gsj_ctx_mem_info(gsj_ctx* c, uint64_t* fr, uint64_t* tot, int* sms) {
   if (!c) return GSJ_ERR_ARG;
   return guard(c, [&] {

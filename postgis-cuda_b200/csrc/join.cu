@@ -102,7 +102,9 @@ static uint32_t read_last(gsj_ctx* c, const uint32_t* off, const uint32_t* flag,
 // Candidate search for probe rows [q0, q0 + nq) (in the given order), growing the pair buffer when needed.
 static uint64_t candidates(gsj_ctx* c, const float4* qbb, const uint32_t* qorder, uint32_t q0, uint32_t nq, const DBvh& T, int upper, uint2** out) {
   uint64_t cap = std::max<uint64_t>((uint64_t)nq * 16, 1 << 16);
-  if (c->cand.cap / sizeof(uint2) > cap) cap = c->cand.cap / sizeof(uint2) - 2;
+  // reuse the whole pooled buffer: as<uint2>(cap + 1) needs (cap + 1) * 8 + 16 bytes
+  const uint64_t pooled = c->cand.cap >= 64 ? (c->cand.cap - 16) / sizeof(uint2) - 1 : 0;
+  if (pooled > cap) cap = pooled;
   for (;;) {
     uint2* buf = c->cand.as<uint2>(cap + 1);
     uint64_t np = traverse(c, qbb, qorder, q0, nq, T, upper, buf, cap);
@@ -164,7 +166,7 @@ void run_join(gsj_ctx* c, const gsj_layer* P, const gsj_layer* R, const RefineAr
     tm.start();
     uint32_t* keep = c->keep.as<uint32_t>(np);
     uint32_t* off = c->idx.as<uint32_t>(np);
-    k_keep<<<grid_for(np, 256), 256, 0, s>>>(flag, np, agg ? 1 : 0, keep);
+    k_keep<<<grid_for(np, 256), 256, 0, s>>>(flag, np, agg ? 1 : 0, keep); c->launches++;
     exclusive_scan(c, keep, off, np);
     uint64_t nk = read_last(c, off, keep, np);
     JoinOut out{nullptr, nullptr, nullptr, 0};
@@ -173,35 +175,37 @@ void run_join(gsj_ctx* c, const gsj_layer* P, const gsj_layer* R, const RefineAr
       out.area = rp.want_area ? c->oarea.as<double>(nk) : nullptr;
       out.code = rel ? c->ocode.as<uint32_t>(nk) : nullptr;
       out.n = nk;
-      if (nk)
+      if (nk) {
         k_scatter_rows<<<grid_for(np, 256), 256, 0, s>>>(pairs, keep, off, np, area, ev, evb, P->d.blen, R->d.blen, out.pairs, out.area, out.code);
+        c->launches++;
+      }
     } else if (nk) {
       // fold piece pairs into parent pairs in (parent pair, piece a, piece b) order
       unsigned long long* k1 = c->keys.as<unsigned long long>(nk);
       unsigned long long* k2 = c->keys2.as<unsigned long long>(nk);
       uint32_t* i1 = c->idx2.as<uint32_t>(nk);
       uint32_t* i2 = c->misc1.as<uint32_t>(nk);
-      k_scatter_pieces<<<grid_for(np, 256), 256, 0, s>>>(pairs, keep, off, np, P->d.parent, R->d.parent, k1, i1);
+      k_scatter_pieces<<<grid_for(np, 256), 256, 0, s>>>(pairs, keep, off, np, P->d.parent, R->d.parent, k1, i1); c->launches++;
       size_t tb = 0;
       GSJ_CK(cub::DeviceRadixSort::SortPairs(nullptr, tb, k1, k2, i1, i2, (int64_t)nk, 0, 64, s));
       GSJ_CK(cub::DeviceRadixSort::SortPairs(c->tmp.get(tb), tb, k1, k2, i1, i2, (int64_t)nk, 0, 64, s));
-      k_parent_keys<<<grid_for(nk, 256), 256, 0, s>>>(i2, nk, pairs, P->d.parent, R->d.parent, k1);
+      k_parent_keys<<<grid_for(nk, 256), 256, 0, s>>>(i2, nk, pairs, P->d.parent, R->d.parent, k1); c->launches++;
       tb = 0;
       GSJ_CK(cub::DeviceRadixSort::SortPairs(nullptr, tb, k1, k2, i2, i1, (int64_t)nk, 0, 64, s));   // stable
       GSJ_CK(cub::DeviceRadixSort::SortPairs(c->tmp.get(tb), tb, k1, k2, i2, i1, (int64_t)nk, 0, 64, s));
       uint32_t* head = c->misc2.as<uint32_t>(nk);
       uint32_t* hoff = c->misc3.as<uint32_t>(nk);
-      k_seg_heads<<<grid_for(nk, 256), 256, 0, s>>>(k2, nk, head);
+      k_seg_heads<<<grid_for(nk, 256), 256, 0, s>>>(k2, nk, head); c->launches++;
       exclusive_scan(c, head, hoff, nk);
       uint64_t nseg = read_last(c, hoff, head, nk);
       uint32_t* start = c->keep.as<uint32_t>(std::max<uint64_t>(np, nseg));   // keep/off of the pieces are no longer needed
-      k_seg_starts<<<grid_for(nk, 256), 256, 0, s>>>(head, hoff, nk, start);
+      k_seg_starts<<<grid_for(nk, 256), 256, 0, s>>>(head, hoff, nk, start); c->launches++;
       uint2* fp = c->agg_flag.as<uint2>(nseg);
       double* fa = c->agg_area.as<double>(nseg);
       double4* fe = rel ? c->agg_ev.as<double4>(nseg) : nullptr;
       uint32_t* fb = rel ? c->agg_evb.as<uint32_t>(nseg) : nullptr;
       uint32_t* fk = c->misc2.as<uint32_t>(nseg);
-      k_fold<<<grid_for(nseg, 256), 256, 0, s>>>(k2, i1, start, nseg, nk, flag, area, ev, evb, fp, area ? fa : nullptr, fe, fb, fk);
+      k_fold<<<grid_for(nseg, 256), 256, 0, s>>>(k2, i1, start, nseg, nk, flag, area, ev, evb, fp, area ? fa : nullptr, fe, fb, fk); c->launches++;
       uint32_t* foff = c->misc3.as<uint32_t>(nseg);
       exclusive_scan(c, fk, foff, nseg);
       uint64_t nout = read_last(c, foff, fk, nseg);
@@ -209,9 +213,11 @@ void run_join(gsj_ctx* c, const gsj_layer* P, const gsj_layer* R, const RefineAr
       out.area = rp.want_area ? c->oarea.as<double>(nout) : nullptr;
       out.code = rel ? c->ocode.as<uint32_t>(nout) : nullptr;
       out.n = nout;
-      if (nout)
+      if (nout) {
         k_scatter_rows<<<grid_for(nseg, 256), 256, 0, s>>>(fp, fk, foff, nseg, area ? fa : nullptr, fe, fb,
                                                            P->d.blen, R->d.blen, out.pairs, out.area, out.code);
+        c->launches++;
+      }
     }
     st.compact_ms += tm.stop();
     st.hits += out.n;
@@ -290,13 +296,13 @@ void run_points(gsj_ctx* c, const gsj_layer* pts, const gsj_layer* R, const gsj_
     if (!np) continue;
     tm.start();
     uint8_t* hit = c->flag.as<uint8_t>(np);
-    k_pip<<<grid_for(np, 128), 128, 0, s>>>(pts->pts, R->d, pairs, np, hit);
+    k_pip<<<grid_for(np, 128), 128, 0, s>>>(pts->pts, R->d, pairs, np, hit); c->launches++;
     GSJ_CK(cudaGetLastError());
     st.refine_ms += tm.stop();
     tm.start();
     uint32_t* keep = c->keep.as<uint32_t>(np);
     uint32_t* off = c->idx.as<uint32_t>(np);
-    k_u8_nonzero<<<grid_for(np, 256), 256, 0, s>>>(hit, np, keep);
+    k_u8_nonzero<<<grid_for(np, 256), 256, 0, s>>>(hit, np, keep); c->launches++;
     exclusive_scan(c, keep, off, np);
     uint64_t nk = read_last(c, off, keep, np);
     uint2* opairs = c->opairs.as<uint2>(nk);
@@ -307,18 +313,18 @@ void run_points(gsj_ctx* c, const gsj_layer* pts, const gsj_layer* R, const gsj_
       unsigned long long* k2 = c->keys2.as<unsigned long long>(nk);
       uint8_t* v1 = reinterpret_cast<uint8_t*>(c->misc1.as<uint32_t>(nk / 4 + 1));
       uint8_t* v2 = reinterpret_cast<uint8_t*>(c->misc2.as<uint32_t>(nk / 4 + 1));
-      k_scatter_pts<<<grid_for(np, 256), 256, 0, s>>>(pairs, hit, keep, off, np, R->d.parent, k1, v1);
+      k_scatter_pts<<<grid_for(np, 256), 256, 0, s>>>(pairs, hit, keep, off, np, R->d.parent, k1, v1); c->launches++;
       size_t tb = 0;
       GSJ_CK(cub::DeviceRadixSort::SortPairs(nullptr, tb, k1, k2, v1, v2, (int64_t)nk, 0, 64, s));
       GSJ_CK(cub::DeviceRadixSort::SortPairs(c->tmp.get(tb), tb, k1, k2, v1, v2, (int64_t)nk, 0, 64, s));
       uint32_t* head = c->misc3.as<uint32_t>(nk);
       uint32_t* hoff = c->idx2.as<uint32_t>(nk);
-      k_seg_heads<<<grid_for(nk, 256), 256, 0, s>>>(k2, nk, head);
+      k_seg_heads<<<grid_for(nk, 256), 256, 0, s>>>(k2, nk, head); c->launches++;
       exclusive_scan(c, head, hoff, nk);
       nout = read_last(c, hoff, head, nk);
       uint32_t* start = c->keep.as<uint32_t>(std::max<uint64_t>(np, nout));
-      k_seg_starts<<<grid_for(nk, 256), 256, 0, s>>>(head, hoff, nk, start);
-      k_fold_max<<<grid_for(nout, 256), 256, 0, s>>>(k2, v2, start, nout, nk, opairs, owhere);
+      k_seg_starts<<<grid_for(nk, 256), 256, 0, s>>>(head, hoff, nk, start); c->launches++;
+      k_fold_max<<<grid_for(nout, 256), 256, 0, s>>>(k2, v2, start, nout, nk, opairs, owhere); c->launches++;
       GSJ_CK(cudaGetLastError());
     }
     st.compact_ms += tm.stop();
@@ -377,6 +383,7 @@ void join_host(gsj_ctx* c, const gsj_layer* P, const gsj_layer* R, const gsj_ref
   RefineArgs rp = to_args(rpp);
   gsj_join_opts o = opts_or_default(op);
   gsj_join_stats st{};
+  const uint64_t l0 = c->launches, v0 = c->node_visits;
   Timer tm(c->stream);
   run_join(c, P, R, rp, o, st, [&](const JoinOut& out) {
     if (!out.n) return;
@@ -390,12 +397,15 @@ void join_host(gsj_ctx* c, const gsj_layer* P, const gsj_layer* R, const gsj_ref
     st.copy_ms += tm.stop();
     if (sink && sink(user, hp, ha, hc, out.n)) throw Error(GSJ_ERR_SINK, "sink stopped the join");
   });
+  st.launches = c->launches - l0;
+  st.node_visits = c->node_visits - v0;
   if (stp) *stp = st;
 }
 
 void points_host(gsj_ctx* c, const gsj_layer* pts, const gsj_layer* R, const gsj_join_opts* op, gsj_points_sink sink, void* user, gsj_join_stats* stp) {
   gsj_join_opts o = opts_or_default(op);
   gsj_join_stats st{};
+  const uint64_t l0 = c->launches, v0 = c->node_visits;
   Timer tm(c->stream);
   run_points(c, pts, R, o, st, [&](const uint2* dp, const uint8_t* dw, uint64_t n) {
     if (!n) return;
@@ -407,6 +417,8 @@ void points_host(gsj_ctx* c, const gsj_layer* pts, const gsj_layer* R, const gsj
     st.copy_ms += tm.stop();
     if (sink && sink(user, hp, hw, n)) throw Error(GSJ_ERR_SINK, "sink stopped the join");
   });
+  st.launches = c->launches - l0;
+  st.node_visits = c->node_visits - v0;
   if (stp) *stp = st;
 }
 
@@ -418,17 +430,20 @@ void cluster_host(gsj_ctx* c, const gsj_layer* P, uint32_t nparent, const gsj_jo
   RefineArgs rp = to_args(nullptr);
   rp.want_area = 0; rp.want_relate = 0;
   gsj_join_stats st{};
+  const uint64_t l0 = c->launches, v0 = c->node_visits;
   cudaStream_t s = c->stream;
   uint32_t* par = c->uf.as<uint32_t>(2 * (size_t)nparent);
   uint32_t* droot = par + nparent;
-  k_uf_init<<<grid_for(nparent, 256), 256, 0, s>>>(par, nparent);
+  k_uf_init<<<grid_for(nparent, 256), 256, 0, s>>>(par, nparent); c->launches++;
   run_join(c, P, P, rp, o, st, [&](const JoinOut& out) {
-    if (out.n) k_uf_union<<<grid_for(out.n, 256), 256, 0, s>>>(out.pairs, out.n, par);
+    if (out.n) { k_uf_union<<<grid_for(out.n, 256), 256, 0, s>>>(out.pairs, out.n, par); c->launches++; }
   });
-  k_uf_roots<<<grid_for(nparent, 256), 256, 0, s>>>(par, nparent, droot);
+  k_uf_roots<<<grid_for(nparent, 256), 256, 0, s>>>(par, nparent, droot); c->launches++;
   GSJ_CK(cudaGetLastError());
   GSJ_CK(cudaMemcpyAsync(root, droot, (size_t)nparent * 4, cudaMemcpyDeviceToHost, s));
   GSJ_CK(cudaStreamSynchronize(s));
+  st.launches = c->launches - l0;
+  st.node_visits = c->node_visits - v0;
   if (stp) *stp = st;
 }
 

@@ -338,7 +338,7 @@ uint64_t refine(gsj_ctx* c, const gsj_layer* P, const gsj_layer* R, const uint2*
   GSJ_CK(cudaMemsetAsync(ctr, 0, 16, s));
   uint32_t* heavy = c->heavy.as<uint32_t>(np);
   const int blocks = (int)std::min<uint64_t>((np + RB_WARPS - 1) / RB_WARPS, (uint64_t)c->sm_count * 6);
-  k_refine<<<blocks, RB_WARPS * 32, RB_SMEM, s>>>(P->d, R->d, pairs, np, rp, flag, area, ev, evb, heavy, ctr);
+  k_refine<<<blocks, RB_WARPS * 32, RB_SMEM, s>>>(P->d, R->d, pairs, np, rp, flag, area, ev, evb, heavy, ctr); c->launches++;
   GSJ_CK(cudaGetLastError());
   unsigned long long* h = c->h_counters.as<unsigned long long>(2);
   GSJ_CK(cudaMemcpyAsync(h, ctr, 16, cudaMemcpyDeviceToHost, s));
@@ -353,7 +353,7 @@ uint64_t refine(gsj_ctx* c, const gsj_layer* P, const gsj_layer* R, const uint2*
     nwarps = (nwarps + 3) / 4 * 4;
     unsigned char* scr = c->scratch.as<unsigned char>(per * nwarps);
     GSJ_CK(cudaMemsetAsync(err, 0, 4, s));
-    k_refine_scratch<<<(int)(nwarps / 4), 128, 0, s>>>(P->d, R->d, pairs, heavy, nh, rp, flag, area, ev, evb, scr, cap, err);
+    k_refine_scratch<<<(int)(nwarps / 4), 128, 0, s>>>(P->d, R->d, pairs, heavy, nh, rp, flag, area, ev, evb, scr, cap, err); c->launches++;
     GSJ_CK(cudaGetLastError());
     GSJ_CK(cudaMemcpyAsync(h, ctr, 16, cudaMemcpyDeviceToHost, s));
     GSJ_CK(cudaStreamSynchronize(s));

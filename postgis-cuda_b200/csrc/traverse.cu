@@ -13,7 +13,7 @@ __device__ __forceinline__ bool box_hit(const float4& c, const float4& b) {
 
 __global__ void __launch_bounds__(128) k_traverse(const float4* __restrict__ qbb, const uint32_t* __restrict__ qorder, uint32_t q0, uint32_t nq,
                                                   DBvh T, int upper, uint2* __restrict__ out, unsigned long long cap,
-                                                  unsigned long long* counter, int* err) {
+                                                  unsigned long long* counter, int* err, unsigned long long* visits) {
   const int lane = threadIdx.x & 31;
   uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
   bool active = t < nq;
@@ -27,12 +27,14 @@ __global__ void __launch_bounds__(128) k_traverse(const float4* __restrict__ qbb
     stack[sp++] = 0;
   }
   const unsigned lt = (1u << lane) - 1;
+  unsigned long long nvis = 0;
   for (;;) {
     bool work = sp > 0;
     if (!__any_sync(0xffffffffu, work)) break;
     uint32_t h0 = 0, h1 = 0; int nh = 0;
     if (work) {
       int node = stack[--sp];
+      nvis++;
       const BNode nd = T.nodes[node];
       bool hl = box_hit(nd.lb, b), hr = box_hit(nd.rb, b);
       if (hr) {
@@ -56,6 +58,8 @@ __global__ void __launch_bounds__(128) k_traverse(const float4* __restrict__ qbb
       if (nh >= 2 && pos + 1 < cap) out[pos + 1] = make_uint2(qi, h1);
     }
   }
+  for (int o = 16; o > 0; o >>= 1) nvis += __shfl_xor_sync(0xffffffffu, nvis, o);
+  if (lane == 0 && nvis) atomicAdd(visits, nvis);
 }
 
 uint64_t traverse(gsj_ctx* c, const float4* qbb, const uint32_t* qorder, uint32_t q0, uint32_t nq, const DBvh& T, int upper, uint2* out,
@@ -63,13 +67,14 @@ uint64_t traverse(gsj_ctx* c, const float4* qbb, const uint32_t* qorder, uint32_
   if (nq == 0) return 0;
   unsigned long long* ctr = c->counters.as<unsigned long long>(8);
   int* err = reinterpret_cast<int*>(ctr + 1);
-  GSJ_CK(cudaMemsetAsync(ctr, 0, 16, c->stream));
-  k_traverse<<<grid_for(nq, 128), 128, 0, c->stream>>>(qbb, qorder, q0, nq, T, upper, out, cap, ctr, err);
+  GSJ_CK(cudaMemsetAsync(ctr, 0, 24, c->stream));
+  k_traverse<<<grid_for(nq, 128), 128, 0, c->stream>>>(qbb, qorder, q0, nq, T, upper, out, cap, ctr, err, ctr + 2); c->launches++;
   GSJ_CK(cudaGetLastError());
-  unsigned long long* h = c->h_counters.as<unsigned long long>(2);
-  GSJ_CK(cudaMemcpyAsync(h, ctr, 16, cudaMemcpyDeviceToHost, c->stream));
+  unsigned long long* h = c->h_counters.as<unsigned long long>(3);
+  GSJ_CK(cudaMemcpyAsync(h, ctr, 24, cudaMemcpyDeviceToHost, c->stream));
   GSJ_CK(cudaStreamSynchronize(c->stream));
   if (reinterpret_cast<int*>(h + 1)[0]) throw Error(GSJ_ERR_CUDA, "traversal stack overflow");
+  c->node_visits += h[2];
   return h[0];
 }
 

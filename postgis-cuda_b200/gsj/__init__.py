@@ -39,7 +39,7 @@ class JoinOpts(ctypes.Structure):
 class JoinStats(ctypes.Structure):
     _fields_ = [("traverse_ms", ctypes.c_double), ("refine_ms", ctypes.c_double), ("compact_ms", ctypes.c_double),
                 ("copy_ms", ctypes.c_double), ("candidates", ctypes.c_uint64), ("hits", ctypes.c_uint64), ("heavy", ctypes.c_uint64),
-                ("batches", ctypes.c_uint64)]
+                ("batches", ctypes.c_uint64), ("launches", ctypes.c_uint64), ("node_visits", ctypes.c_uint64)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -63,6 +63,7 @@ SIGNATURES = {
     "gsj_ctx_create": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(_vp)]),
     "gsj_ctx_destroy": (None, [_vp]),
     "gsj_last_error": (ctypes.c_char_p, [_vp]),
+    "gsj_ctx_stream": (_vp, [_vp]),
     "gsj_ctx_mem_info": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_int)]),
     "gsj_layer_upload_polygons": (ctypes.c_int, [_vp, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64, _vp, _vp, _vp, _vp, _vp,
                                                  ctypes.POINTER(_vp)]),
@@ -185,6 +186,10 @@ class Engine:
     def _check(self, rc):
         if rc:
             raise GsjError(rc, lib().gsj_last_error(self.ctx).decode(errors="replace"))
+
+    def stream_handle(self) -> int:
+        """cudaStream_t of the context (all its kernels run there), e.g. for torch.cuda.ExternalStream."""
+        return lib().gsj_ctx_stream(self.ctx)
 
     def mem_info(self):
         f, t, s = ctypes.c_uint64(), ctypes.c_uint64(), ctypes.c_int()

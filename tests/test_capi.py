@@ -1,0 +1,47 @@
+"""The C ABI library: it loads and exports every symbol include/gsj.h declares; no GPU needed."""
+import ctypes
+import os
+import re
+
+import gsj
+from gsj._build import lib_path
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_symbols():
+    src = open(os.path.join(ROOT, "include", "gsj.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b(gsj_[a-z0-9_]+)\s*\(", src)) - {"gsj_join_sink", "gsj_points_sink", "gsj_pairs_sink"})
+
+
+def test_exports_every_declared_symbol():
+    lib = ctypes.CDLL(lib_path("libgsj.so"))
+    names = declared_symbols()
+    assert len(names) >= 20
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+    assert set(names) <= set(gsj.SIGNATURES), set(names) - set(gsj.SIGNATURES)
+
+
+def test_de9im_helpers_without_gpu():
+    code = 1 | 3 << 12 | 2 << 14 | 3 << 16
+    assert gsj.de9im_str(code) == "0FFFFF212"
+    assert gsj.de9im_transpose(gsj.de9im_transpose(code)) == code
+    assert gsj.de9im_match(code, "0********") and not gsj.de9im_match(code, "F********")
+
+
+def test_defaults_match_reference_refine_params():
+    p = gsj.refine_params()
+    assert (p.tol_rel, p.eps_par, p.tol_abs, p.want_area, p.want_relate, p.snap_half_ulp) == (1e-12, 1e-7, 1e-11, 1, 0, 0)
+
+
+def test_errors_are_status_codes_not_exits():
+    """Without a usable device (CPU container) context creation fails with a status, it does not abort."""
+    import torch
+    if torch.cuda.is_available():
+        return
+    h = ctypes.c_void_p()
+    rc = gsj.lib().gsj_ctx_create(0, ctypes.byref(h))
+    assert rc != 0 and not h.value
+    assert gsj.lib().gsj_join(None, None, None, None, None, gsj.JOIN_SINK(lambda *a: 0), None, None) == 1

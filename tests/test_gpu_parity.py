@@ -1,0 +1,123 @@
+"""CUDA engine (through the C ABI) against the CPU FP64 oracle: bit-exact pair sets, flags, areas, DE-9IM."""
+import numpy as np
+import pytest
+
+import gsj
+import pyoracle as O
+import shapes
+from gsj import gen
+
+pytestmark = pytest.mark.gpu
+MODES = [gsj.GSJ_REFINE_PLAIN, gsj.GSJ_REFINE_FILTERED]
+SMALL_BOX = (-118.30, 33.95, -118.20, 34.05)
+
+
+def srt(p, *vals):
+    i = np.lexsort((p[:, 1], p[:, 0]))
+    return (p[i],) + tuple(None if v is None else v[i] for v in vals)
+
+
+@pytest.fixture(scope="module")
+def layers(engine):
+    hs = {
+        "zonesA": gen.voronoi(20000, gen.LA_BOX, 0, vmin=6, vmax=40),
+        "zonesB": gen.voronoi(50, gen.LA_BOX, 1, vmin=4, vmax=4),
+        "parcels": gen.layer_parcels(20000, (-118.3, 33.95, -118.1, 34.15), seed=5),
+        "parcels2": gen.layer_parcels(15000, (-118.3, 33.95, -118.1, 34.15), seed=6),
+        "one": gen.voronoi(1, gen.LA_BOX, 9, vmin=40, vmax=40),
+    }
+    return {k: (engine.upload_polygons(v), O.OSet(v), v) for k, v in hs.items()}
+
+
+PAIRS = [("zonesA", "zonesB", False), ("zonesA", "zonesA", True), ("parcels", "parcels", True), ("parcels", "parcels2", False),
+         ("parcels2", "zonesB", False), ("one", "parcels", False), ("parcels", "one", False)]
+
+
+@pytest.mark.parametrize("a,b,upper", PAIRS)
+def test_candidates(engine, layers, a, b, upper):
+    g = srt(engine.candidates(layers[a][0], layers[b][0], upper=upper))[0]
+    o = O.candidates(layers[a][1], layers[b][1], upper=upper)
+    assert np.array_equal(g, o)
+
+
+@pytest.mark.parametrize("mode", MODES)
+@pytest.mark.parametrize("a,b,upper", PAIRS)
+def test_refine_pairs_bitexact(engine, layers, a, b, upper, mode):
+    cand = O.candidates(layers[a][1], layers[b][1], upper=upper)
+    for rel in (False, True):
+        f, ar, ev, evb = engine.refine_pairs(layers[a][0], layers[b][0], cand, want_area=True, want_relate=rel, refine_mode=mode)
+        of, oa, oe, ob = O.refine_pairs(layers[a][1], layers[b][1], cand, O.params(1, int(rel)))
+        assert np.array_equal(f, of)
+        assert np.array_equal(ar, oa)            # same rounding order: bit-identical areas
+        if rel:
+            assert np.array_equal(ev, oe) and np.array_equal(evb, ob)
+
+
+@pytest.mark.parametrize("mode", MODES)
+@pytest.mark.parametrize("a,b,upper", PAIRS)
+def test_join_bitexact(engine, layers, a, b, upper, mode):
+    for area, rel in ((True, False), (False, True), (True, True)):
+        r = engine.join(layers[a][0], layers[b][0], want_area=area, want_relate=rel, upper=upper, refine_mode=mode)
+        p, oa, oc, nc = O.join(layers[a][1], layers[b][1], O.params(int(area), int(rel)), upper=upper)
+        gp, ga, gc = srt(r.pairs, r.area, r.code)
+        assert np.array_equal(gp, p)
+        if area:
+            assert np.array_equal(ga, oa)
+        if rel:
+            assert np.array_equal(gc, oc)
+        assert r.stats["candidates"] == nc and r.stats["launches"] >= 3
+
+
+def test_area_tiles_box(engine, layers):
+    r = engine.join(layers["zonesA"][0], layers["zonesB"][0])
+    assert abs(r.area.sum() - 0.25) < 1e-12
+
+
+@pytest.mark.parametrize("name,a,b,rel,area", shapes.CASES)
+def test_known_answers_gpu(engine, name, a, b, rel, area):
+    A, B = engine.upload_polygons(shapes.make_set([a])), engine.upload_polygons(shapes.make_set([b]))
+    r = engine.join(A, B, want_area=True, want_relate=True)
+    if rel is None:
+        assert len(r.pairs) == 0
+        return
+    assert len(r.pairs) == 1 and gsj.de9im_str(int(r.code[0])) == rel
+    assert abs(r.area[0] - area) <= 1e-9 * max(area, 1e-12) + 1e-20
+
+
+def test_batches_give_same_rows(engine, layers):
+    L = layers["parcels"][0]
+    whole = engine.join(L, L, want_area=True, want_relate=True, upper=True)
+    parts = engine.join(L, L, want_area=True, want_relate=True, upper=True, batch_q=3000)
+    assert parts.stats["batches"] > 1
+    a, b = srt(whole.pairs, whole.area, whole.code), srt(parts.pairs, parts.area, parts.code)
+    assert all(np.array_equal(x, y) for x, y in zip(a, b))
+
+
+def test_points_in_polygons(engine, layers):
+    pts = gen.points(50000, (-118.3, 33.95, -118.1, 34.15), 3)
+    # include vertices and edge midpoints (boundary cases) of the parcels
+    ps = layers["parcels"][2]
+    extra = np.concatenate([ps.xy[::97], 0.5 * (ps.xy[:-1:89] + ps.xy[1::89])])
+    pts = np.concatenate([pts, extra])
+    gp, gw, st = engine.join_points(engine.upload_points(pts), layers["parcels"][0])
+    op, ow, nc = O.pip(pts, layers["parcels"][1])
+    gp, gw = srt(gp, gw)
+    assert np.array_equal(gp, op) and np.array_equal(gw, ow)
+    assert (ow == 2).sum() > 100 and st["candidates"] == nc
+
+
+def test_cluster(engine, layers):
+    for k in ("parcels", "zonesA"):
+        root, st = engine.cluster(layers[k][0])
+        assert np.array_equal(root, O.cluster(layers[k][1], layers[k][1].n))
+    # two separate groups of squares
+    geoms = [[shapes.square(i * shapes.S, 0, shapes.S)] for i in range(3)] + [[shapes.square(10 * shapes.S + i * shapes.S, 0, shapes.S)] for i in range(2)]
+    root, _ = engine.cluster(engine.upload_polygons(shapes.make_set(geoms)))
+    assert root.tolist() == [0, 0, 0, 3, 3]
+
+
+def test_bad_arguments_are_errors(engine, layers):
+    with pytest.raises(gsj.GsjError):
+        engine.join(layers["parcels"][0], engine.upload_points(np.zeros((3, 2))))
+    with pytest.raises(gsj.GsjError):
+        engine.refine_pairs(layers["one"][0], layers["one"][0], np.array([[0, 5]], np.uint32))
