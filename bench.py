@@ -296,8 +296,8 @@ def main():
     try:
         for ln in open(os.path.join(ROOT, "profiles", "traffic_per_launch.txt")):
             k, v = ln.split()[:2]
-            if k == "k_refine":
-                traffic = float(v)
+            if k == "k_refine":   # measured on a smaller case, scaled by the candidate pairs of one launch
+                traffic = float(v) * float(st[0]["candidates"])
     except OSError:
         pass
     cpu = None

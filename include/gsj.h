@@ -133,6 +133,20 @@ int gsj_candidates(gsj_ctx* ctx, const gsj_layer* P, const gsj_layer* R, int upp
 int gsj_refine_pairs(gsj_ctx* ctx, const gsj_layer* P, const gsj_layer* R, const uint32_t* pairs, uint64_t np,
                      const gsj_refine_params* rp, int refine_mode, uint8_t* flag, double* area, double* ev, uint32_t* evb);
 
+/* Refinement of candidate pairs for callers that cannot allocate device memory. No counterpart in the
+ * reference: its engine allocates scratch on every call. For callers that must not call cudaMalloc once running
+ * (a server working inside a device-memory budget reserved up front, or a request path that cannot take
+ * cudaMalloc/cudaFree's implicit device synchronisation). Same outputs as gsj_refine_pairs, but every pointer is
+ * DEVICE memory owned by the caller: d_pairs[2np] (P index, R index), d_flag[np], optional d_area[np], optional
+ * d_ev[4np] with d_evb[np]. Its scratch is one static device array of GSJ_NOALLOC_SCRATCH_BYTES per GPU (held by
+ * every GPU that loads the library, until exit); layers whose largest geometry needs a larger per-warp slab
+ * (more than ~466k edges) are rejected with GSJ_ERR_ARG. All calls share that array: calls that overlap on the GPU
+ * race and must be serialised. The first call on a device looks up the array's address; make it before any
+ * stream capture. Runs on the context's stream and returns after it finished. */
+#define GSJ_NOALLOC_SCRATCH_BYTES (32u << 20)
+int gsj_refine_pairs_noalloc(gsj_ctx* ctx, const gsj_layer* P, const gsj_layer* R, const uint32_t* d_pairs, uint64_t np,
+                             const gsj_refine_params* rp, uint8_t* d_flag, double* d_area, double* d_ev, uint32_t* d_evb);
+
 /* DE-9IM helpers: de9im_str / de9im_transpose / de9im_match (engine.cuh:871-888). out gets 9 chars (no NUL). */
 void gsj_de9im_str(uint32_t code, char* out9);
 uint32_t gsj_de9im_transpose(uint32_t code);

@@ -83,6 +83,7 @@ SIGNATURES = {
     "gsj_points_erode": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_double, ctypes.POINTER(JoinOpts), PAIRS_SINK, _vp, ctypes.POINTER(JoinStats)]),
     "gsj_candidates": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_int, PAIRS_SINK, _vp]),
     "gsj_refine_pairs": (ctypes.c_int, [_vp, _vp, _vp, _vp, ctypes.c_uint64, ctypes.POINTER(RefineParams), ctypes.c_int, _vp, _vp, _vp, _vp]),
+    "gsj_refine_pairs_noalloc": (ctypes.c_int, [_vp, _vp, _vp, _vp, ctypes.c_uint64, ctypes.POINTER(RefineParams), _vp, _vp, _vp, _vp]),
     "gsj_de9im_str": (None, [ctypes.c_uint32, ctypes.c_char_p]),
     "gsj_de9im_transpose": (ctypes.c_uint32, [ctypes.c_uint32]),
     "gsj_de9im_match": (ctypes.c_int, [ctypes.c_uint32, ctypes.c_char_p]),
