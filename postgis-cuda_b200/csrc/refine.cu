@@ -6,15 +6,27 @@
 //
 // Pairs whose local edge lists fit CAP run from shared memory; larger pairs are queued and re-run by
 // k_refine_scratch with per-warp lists in global scratch (the same device code, so the same results).
+//
+// Two variants of the same pair routine (template flag F):
+//  - plain (F = false): FP64 box tests, as the reference.
+//  - filtered (F = true): the box rejection tests that dominate the inner loops are written as plain comparisons
+//    (max(a, b) < x  <=>  a < x && b < x for finite values) instead of FP64 min/max, which on sm_100a issue on the
+//    XU pipe - the pipe the plain kernel saturates (ncu: XU 77 % of peak, FP64 25 %). The same booleans, so every
+//    decision and every FP64 value is unchanged. Containment probes are tested by the whole warp (crossing parity
+//    is order-free).
 #include "engine.h"
 
 namespace gsj {
 
-constexpr int CAP = 128;                         // local edges per polygon per warp in shared memory
+constexpr int CAP = 128;                         // plain: local edges per polygon per warp in shared memory
 constexpr int RB_WARPS = 4;                      // warps per block
 constexpr size_t EDGE_BYTES = 4 * sizeof(double) + sizeof(uint32_t);
 constexpr size_t LIST_BYTES = CAP * EDGE_BYTES;  // one list
 constexpr size_t RB_SMEM = (size_t)RB_WARPS * 2 * LIST_BYTES;
+constexpr int CAP_F = 128;                       // filtered: local edges per polygon per warp
+constexpr size_t EDGE_BYTES_F = EDGE_BYTES;
+constexpr size_t LIST_BYTES_F = CAP_F * EDGE_BYTES_F;
+constexpr size_t RB_SMEM_F = (size_t)RB_WARPS * 2 * LIST_BYTES_F;
 
 __device__ __forceinline__ EList carve(unsigned char* base, int cap) {
   EList L;
@@ -23,12 +35,17 @@ __device__ __forceinline__ EList carve(unsigned char* base, int cap) {
   L.fl = reinterpret_cast<uint32_t*>(L.y1 + cap);
   return L;
 }
-
+__device__ __forceinline__ EList carve_f(unsigned char* base, int cap) { return carve(base, cap); }
+// edge (x0, y0)-(x1, y1) entirely outside box [bx0, bx1] x [by0, by1], by comparisons only
+__device__ __forceinline__ bool out_cmp(double x0, double y0, double x1, double y1, double bx0, double by0, double bx1, double by1) {
+  return (x0 < bx0 && x1 < bx0) || (x0 > bx1 && x1 > bx1) || (y0 < by0 && y1 < by0) || (y0 > by1 && y1 > by1);
+}
 __device__ __forceinline__ bool edge_outside(double px, double py, double qx, double qy, const Box& o) {
   return fmax(px, qx) < o.x0 || fmin(px, qx) > o.x1 || fmax(py, qy) < o.y0 || fmin(py, qy) > o.y1;
 }
 
 // all edges of geometry A meeting the overlap box, compacted in ring order with a warp ballot (engine.cuh:358-377)
+template <bool F>
 __device__ int collect(const Frame& A, const Box& ov, EList L, int cap, int lane) {
   const DLayer& S = *A.L;
   const unsigned lt = (1u << lane) - 1;
@@ -44,11 +61,13 @@ __device__ int collect(const Frame& A, const Box& ov, EList L, int cap, int lane
         if (S.synb) {
           fl = (uint32_t)S.syn(i) | (S.syn(i > s ? i - 1 : e - 2) ? 2u : 0u) | (S.syn(i + 2 < e ? i + 1 : s) ? 4u : 0u);
         }
-        in = !edge_outside(x0, y0, x1, y1, ov);
+        in = F ? !out_cmp(x0, y0, x1, y1, ov.x0, ov.y0, ov.x1, ov.y1) : !edge_outside(x0, y0, x1, y1, ov);
       }
       const unsigned m = __ballot_sync(0xffffffffu, in);
       const int pos = cnt + __popc(m & lt);
-      if (in && pos < cap) { L.x0[pos] = x0; L.y0[pos] = y0; L.x1[pos] = x1; L.y1[pos] = y1; L.fl[pos] = fl; }
+      if (in && pos < cap) {
+        L.x0[pos] = x0; L.y0[pos] = y0; L.x1[pos] = x1; L.y1[pos] = y1; L.fl[pos] = fl;
+      }
       cnt += __popc(m);
     }
   }
@@ -75,23 +94,45 @@ __device__ bool pip_full_warp(const Frame& B, double mx, double my, int lane) {
 }
 
 // inside(x) = inside(c) xor crossings of c -> x with the local edges (engine.cuh:400-412)
+template <bool F>
 __device__ __forceinline__ bool inside_from_c(const EList& L, int cnt, double cx, double cy, bool in_c, double x, double y) {
   bool in = in_c;
   const double sx0 = fmin(cx, x), sx1 = fmax(cx, x), sy0 = fmin(cy, y), sy1 = fmax(cy, y);
-  for (int k = 0; k < cnt; k++) {
+  auto step = [&](int k) {
     const double ex0 = L.x0[k], ey0 = L.y0[k], ex1 = L.x1[k], ey1 = L.y1[k];
-    if (fmax(ex0, ex1) < sx0 || fmin(ex0, ex1) > sx1 || fmax(ey0, ey1) < sy0 || fmin(ey0, ey1) > sy1) continue;
+    if (F ? out_cmp(ex0, ey0, ex1, ey1, sx0, sy0, sx1, sy1)
+          : (fmax(ex0, ex1) < sx0 || fmin(ex0, ex1) > sx1 || fmax(ey0, ey1) < sy0 || fmin(ey0, ey1) > sy1)) return false;
+    bool sc = left_of(ex0, ey0, ex1, ey1, cx, cy), sx = left_of(ex0, ey0, ex1, ey1, x, y);
+    if (sc == sx) return false;
+    bool su = orient(cx, cy, x, y, ex0, ey0) > 0, sv = orient(cx, cy, x, y, ex1, ey1) > 0;
+    if (su != sv) in = !in;
+    return false;
+  };
+  for (int k = 0; k < cnt; k++) step(k);
+  return in;
+}
+
+// The same parity for one query point shared by the whole warp: lanes split the edges, a ballot counts crossings
+// (the parity does not depend on the order of the edges).
+__device__ bool inside_from_c_warp(const EList& L, int cnt, double cx, double cy, bool in_c, double x, double y, int lane) {
+  const double sx0 = fmin(cx, x), sx1 = fmax(cx, x), sy0 = fmin(cy, y), sy1 = fmax(cy, y);
+  bool par = false;
+  for (int k = lane; k < cnt; k += 32) {
+    const double ex0 = L.x0[k], ey0 = L.y0[k], ex1 = L.x1[k], ey1 = L.y1[k];
+    if (out_cmp(ex0, ey0, ex1, ey1, sx0, sy0, sx1, sy1)) continue;
     bool sc = left_of(ex0, ey0, ex1, ey1, cx, cy), sx = left_of(ex0, ey0, ex1, ey1, x, y);
     if (sc == sx) continue;
     bool su = orient(cx, cy, x, y, ex0, ey0) > 0, sv = orient(cx, cy, x, y, ex1, ey1) > 0;
-    if (su != sv) in = !in;
+    if (su != sv) par = !par;
   }
-  return in;
+  const bool odd = (__popc(__ballot_sync(0xffffffffu, par)) & 1) != 0;
+  return in_c != odd;
 }
 
 struct PairGeo { Box ov; double tol, eps_par, snap, cx, cy; };
 
 // Green's-theorem contribution of edge p->q within the other polygon + relate lengths (engine.cuh:416-515)
+template <bool F>
 __device__ double edge_contrib(double px, double py, double qx, double qy, const EList& L, int cnt, bool in_c, const PairGeo& G, bool real,
                                double* l_in, double* l_on, uint32_t* bits, uint32_t cut) {
   const double dx = qx - px, dy = qy - py;
@@ -104,9 +145,10 @@ __device__ double edge_contrib(double px, double py, double qx, double qy, const
   ts[ns++] = 0; ts[ns++] = 1;
   const double bx0 = fmin(px, qx) - tol, bx1 = fmax(px, qx) + tol, by0 = fmin(py, qy) - tol, by1 = fmax(py, qy) + tol;
   const double snap2 = G.snap * G.snap;
-  for (int k = 0; k < cnt; k++) {
+  auto visit = [&](int k) {
     const double ex0 = L.x0[k], ey0 = L.y0[k], ex1 = L.x1[k], ey1 = L.y1[k];
-    if (fmax(ex0, ex1) < bx0 || fmin(ex0, ex1) > bx1 || fmax(ey0, ey1) < by0 || fmin(ey0, ey1) > by1) continue;
+    if (F ? out_cmp(ex0, ey0, ex1, ey1, bx0, by0, bx1, by1)
+          : (fmax(ex0, ex1) < bx0 || fmin(ex0, ex1) > bx1 || fmax(ey0, ey1) < by0 || fmin(ey0, ey1) > by1)) return false;
     const uint32_t efl = L.fl[k];
     const double fx = ex1 - ex0, fy = ey1 - ey0;
     const double r = dx * fy - dy * fx;
@@ -128,12 +170,14 @@ __device__ double edge_contrib(double px, double py, double qx, double qy, const
     } else if (r * r > eps2 * len2 * flen2) {
       const double wx = ex0 - px, wy = ey0 - py;
       const double tn = wx * fy - wy * fx;
-      if (r > 0 ? (tn <= 0 || tn >= r) : (tn >= 0 || tn <= r)) continue;
+      if (r > 0 ? (tn <= 0 || tn >= r) : (tn >= 0 || tn <= r)) return false;
       const double t = tn / r, u = (wx * dy - wy * dx) / r;
       const double du = tol / (flen2 > 0 ? sqrt(flen2) : (double)1);
       if (u >= -du && u <= 1 + du && ns < MAXS) ts[ns++] = t;
     }
-  }
+    return false;
+  };
+  for (int k = 0; k < cnt; k++) visit(k);
   for (int a = 1; a < ns; a++) { double v = ts[a]; int b = a - 1; while (b >= 0 && ts[b] > v) { ts[b + 1] = ts[b]; b--; } ts[b + 1] = v; }
   double acc = 0.0;
   for (int k = 0; k + 1 < ns; k++) {
@@ -151,7 +195,7 @@ __device__ double edge_contrib(double px, double py, double qx, double qy, const
       }
     int vin = -1;
     auto inside_m = [&]() {
-      if (vin < 0) vin = (in_ov && inside_from_c(L, cnt, G.cx, G.cy, in_c, mx, my)) ? 1 : 0;
+      if (vin < 0) vin = (in_ov && inside_from_c<F>(L, cnt, G.cx, G.cy, in_c, mx, my)) ? 1 : 0;
       return vin;
     };
     if (l_in && real) {
@@ -200,8 +244,9 @@ __device__ __forceinline__ double warp_sum(double v) {
 }
 
 // One pair, whole warp. Returns false when a local list exceeded cap (nothing written).
-__device__ bool refine_pair(const DLayer& P, const DLayer& R, uint32_t a, uint32_t b, const RefineArgs& rp, EList LA, EList LB, int cap,
-                            int lane, uint8_t& o_flag, double& o_area, double4& o_ev, uint32_t& o_evb) {
+template <bool F>
+__device__ bool refine_pair_t(const DLayer& P, const DLayer& R, uint32_t a, uint32_t b, const RefineArgs& rp, EList LA, EList LB, int cap,
+                              int lane, uint8_t& o_flag, double& o_area, double4& o_ev, uint32_t& o_evb) {
   const double2 oa = P.origin[a], ob = R.origin[b], ea = P.ext[a], eb = R.ext[b];
   const double sx = ob.x - oa.x, sy = ob.y - oa.y;
   const double pad = 4.0 * fmax(rp.tol_abs, (double)rp.tol_rel * fmax(fmax(ea.x, ea.y), fmax(eb.x, eb.y)));
@@ -211,25 +256,29 @@ __device__ bool refine_pair(const DLayer& P, const DLayer& R, uint32_t a, uint32
   G.tol = fmax(rp.tol_abs, (double)rp.tol_rel * fmax(G.ov.x1 - G.ov.x0, G.ov.y1 - G.ov.y0));
   G.eps_par = rp.eps_par;
   G.snap = rp.snap_half_ulp ? pair_snap(oa, ea) : 0.0;
-  const int na = collect(A, G.ov, LA, cap, lane);
-  const int nb = collect(B, G.ov, LB, cap, lane);
+  const int na = collect<F>(A, G.ov, LA, cap, lane);
+  const int nb = collect<F>(B, G.ov, LB, cap, lane);
   if (na > cap || nb > cap) return false;
   __syncwarp();
   // boundary contact
   bool hit = false, hit_any = false;
-  for (int i = lane; i < na && !hit; i += 32) {
+  auto seg_loop = [&](int i) {
     const double px0 = LA.x0[i], py0 = LA.y0[i], px1 = LA.x1[i], py1 = LA.y1[i];
     const uint32_t fa = LA.fl[i];
     const double ax0 = fmin(px0, px1), ax1 = fmax(px0, px1), ay0 = fmin(py0, py1), ay1 = fmax(py0, py1);
-    for (int j = 0; j < nb; j++) {
+    auto test = [&](int j) {
       const double qx0 = LB.x0[j], qy0 = LB.y0[j], qx1 = LB.x1[j], qy1 = LB.y1[j];
-      if (fmax(qx0, qx1) < ax0 || fmin(qx0, qx1) > ax1 || fmax(qy0, qy1) < ay0 || fmin(qy0, qy1) > ay1) continue;
+      if (F ? out_cmp(qx0, qy0, qx1, qy1, ax0, ay0, ax1, ay1)
+            : (fmax(qx0, qx1) < ax0 || fmin(qx0, qx1) > ax1 || fmax(qy0, qy1) < ay0 || fmin(qy0, qy1) > ay1)) return false;
       if (seg_isect(px0, py0, px1, py1, qx0, qy0, qx1, qy1)) {
         hit_any = true;
-        if (!((fa | LB.fl[j]) & 1u)) { hit = true; break; }
+        if (!((fa | LB.fl[j]) & 1u)) { hit = true; return true; }
       }
-    }
-  }
+      return false;
+    };
+    for (int j = 0; j < nb; j++) if (test(j)) break;
+  };
+  for (int i = lane; i < na && !hit; i += 32) seg_loop(i);
   hit = __any_sync(0xffffffffu, hit);
   hit_any = __any_sync(0xffffffffu, hit_any || hit);
   const bool rtouch = hit;
@@ -241,18 +290,38 @@ __device__ bool refine_pair(const DLayer& P, const DLayer& R, uint32_t a, uint32
   if (!hit) {
     // no real boundary contact: intersects iff a real-edge vertex of one lies inside the other (engine.cuh:577-594)
     bool h = false, ha = false;
-    for (uint32_t r = A.r0 + lane; r < A.r1 && !h; r += 32) {
-      double x, y; const bool real = probe_vertex(A, r, x, y);
-      if (!real) A.v(P.rvo[r], x, y);
-      if (x >= G.ov.x0 && x <= G.ov.x1 && y >= G.ov.y0 && y <= G.ov.y1 && inside_from_c(LB, nb, G.cx, G.cy, inB_c, x, y)) { ha = true; h = real; }
+    if constexpr (F) {
+      // one probe at a time, the warp splitting the other polygon's edges (crossing parity is order-free)
+      for (int side = 0; side < 2 && !h; side++) {
+        const Frame& S = side ? B : A;
+        const DLayer& SL = side ? R : P;
+        const EList& LO = side ? LA : LB;
+        const int no_ = side ? na : nb;
+        const bool inc = side ? inA_c : inB_c;
+        for (uint32_t r = S.r0; r < S.r1 && !h; r++) {
+          double x, y; const bool real = probe_vertex(S, r, x, y);
+          if (!real) S.v(SL.rvo[r], x, y);
+          if (x >= G.ov.x0 && x <= G.ov.x1 && y >= G.ov.y0 && y <= G.ov.y1 && inside_from_c_warp(LO, no_, G.cx, G.cy, inc, x, y, lane)) {
+            ha = true; h = real;
+          }
+        }
+      }
+      hit = h;
+      contain_any = ha;
+    } else {
+      for (uint32_t r = A.r0 + lane; r < A.r1 && !h; r += 32) {
+        double x, y; const bool real = probe_vertex(A, r, x, y);
+        if (!real) A.v(P.rvo[r], x, y);
+        if (x >= G.ov.x0 && x <= G.ov.x1 && y >= G.ov.y0 && y <= G.ov.y1 && inside_from_c<F>(LB, nb, G.cx, G.cy, inB_c, x, y)) { ha = true; h = real; }
+      }
+      for (uint32_t r = B.r0 + lane; r < B.r1 && !h; r += 32) {
+        double x, y; const bool real = probe_vertex(B, r, x, y);
+        if (!real) B.v(R.rvo[r], x, y);
+        if (x >= G.ov.x0 && x <= G.ov.x1 && y >= G.ov.y0 && y <= G.ov.y1 && inside_from_c<F>(LA, na, G.cx, G.cy, inA_c, x, y)) { ha = true; h = real; }
+      }
+      hit = __any_sync(0xffffffffu, h);
+      contain_any = __any_sync(0xffffffffu, ha);
     }
-    for (uint32_t r = B.r0 + lane; r < B.r1 && !h; r += 32) {
-      double x, y; const bool real = probe_vertex(B, r, x, y);
-      if (!real) B.v(R.rvo[r], x, y);
-      if (x >= G.ov.x0 && x <= G.ov.x1 && y >= G.ov.y0 && y <= G.ov.y1 && inside_from_c(LA, na, G.cx, G.cy, inA_c, x, y)) { ha = true; h = real; }
-    }
-    hit = __any_sync(0xffffffffu, h);
-    contain_any = __any_sync(0xffffffffu, ha);
   }
   double ar = 0.0; double4 e4 = make_double4(0, 0, 0, 0); uint32_t eb4 = 0;
   if ((hit || hit_any || contain_any) && (rp.want_area || rp.want_relate)) {
@@ -261,11 +330,11 @@ __device__ bool refine_pair(const DLayer& P, const DLayer& R, uint32_t a, uint32
     const bool rel = rp.want_relate != 0;
     for (int i = lane; i < na; i += 32) {
       const uint32_t f = LA.fl[i];
-      s2 += edge_contrib(LA.x0[i], LA.y0[i], LA.x1[i], LA.y1[i], LB, nb, inB_c, G, !(f & 1u), rel ? &ai : nullptr, &ao, &bits, f);
+      s2 += edge_contrib<F>(LA.x0[i], LA.y0[i], LA.x1[i], LA.y1[i], LB, nb, inB_c, G, !(f & 1u), rel ? &ai : nullptr, &ao, &bits, f);
     }
     for (int i = lane; i < nb; i += 32) {
       const uint32_t f = LB.fl[i];
-      s2 += edge_contrib(LB.x0[i], LB.y0[i], LB.x1[i], LB.y1[i], LA, na, inA_c, G, !(f & 1u), rel ? &bi : nullptr, &bo, &bits, f);
+      s2 += edge_contrib<F>(LB.x0[i], LB.y0[i], LB.x1[i], LB.y1[i], LA, na, inA_c, G, !(f & 1u), rel ? &bi : nullptr, &bo, &bits, f);
     }
     s2 = warp_sum(s2); ai = warp_sum(ai); ao = warp_sum(ao); bi = warp_sum(bi); bo = warp_sum(bo);
     ar = 0.5 * s2;
@@ -278,18 +347,32 @@ __device__ bool refine_pair(const DLayer& P, const DLayer& R, uint32_t a, uint32
   return true;
 }
 
-__global__ void __launch_bounds__(RB_WARPS * 32) k_refine(DLayer P, DLayer R, const uint2* __restrict__ pairs, uint64_t np, RefineArgs rp,
-                                                          uint8_t* flag, double* area, double4* ev, uint32_t* evb, uint32_t* heavy,
-                                                          unsigned long long* nheavy) {
+// the plain routine, callable from other translation units (the allocation-free entry point)
+__device__ bool refine_pair(const DLayer& P, const DLayer& R, uint32_t a, uint32_t b, const RefineArgs& rp, EList LA, EList LB, int cap, int lane,
+                            uint8_t& o_flag, double& o_area, double4& o_ev, uint32_t& o_evb) {
+  return refine_pair_t<false>(P, R, a, b, rp, LA, LB, cap, lane, o_flag, o_area, o_ev, o_evb);
+}
+
+template <bool F> struct Cfg;
+template <> struct Cfg<false> { static constexpr int cap = CAP; static constexpr size_t list = LIST_BYTES, smem = RB_SMEM, edge = EDGE_BYTES; static constexpr int minb = 3; };
+template <> struct Cfg<true> { static constexpr int cap = CAP_F; static constexpr size_t list = LIST_BYTES_F, smem = RB_SMEM_F, edge = EDGE_BYTES_F; static constexpr int minb = 4; };
+
+template <bool F>
+__device__ __forceinline__ EList carve_t(unsigned char* base, int cap) { return F ? carve_f(base, cap) : carve(base, cap); }
+
+template <bool F>
+__global__ void __launch_bounds__(RB_WARPS * 32, Cfg<F>::minb) k_refine(DLayer P, DLayer R, const uint2* __restrict__ pairs, uint64_t np,
+                                                                        RefineArgs rp, uint8_t* flag, double* area, double4* ev, uint32_t* evb,
+                                                                        uint32_t* heavy, unsigned long long* nheavy) {
   extern __shared__ __align__(16) unsigned char smem[];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-  EList LA = carve(smem + (size_t)wib * 2 * LIST_BYTES, CAP);
-  EList LB = carve(smem + (size_t)wib * 2 * LIST_BYTES + LIST_BYTES, CAP);
+  EList LA = carve_t<F>(smem + (size_t)wib * 2 * Cfg<F>::list, Cfg<F>::cap);
+  EList LB = carve_t<F>(smem + (size_t)wib * 2 * Cfg<F>::list + Cfg<F>::list, Cfg<F>::cap);
   const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
   for (uint64_t p = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; p < np; p += nw) {
     const uint2 pr = pairs[p];
     uint8_t f; double ar; double4 e4; uint32_t b4;
-    const bool ok = refine_pair(P, R, pr.x, pr.y, rp, LA, LB, CAP, lane, f, ar, e4, b4);
+    const bool ok = refine_pair_t<F>(P, R, pr.x, pr.y, rp, LA, LB, Cfg<F>::cap, lane, f, ar, e4, b4);
     if (lane == 0) {
       if (!ok) { heavy[atomicAdd(nheavy, 1ull)] = (uint32_t)p; flag[p] = 0; }
       else {
@@ -303,18 +386,19 @@ __global__ void __launch_bounds__(RB_WARPS * 32) k_refine(DLayer P, DLayer R, co
 }
 
 // oversized pairs: the same pair routine with per-warp edge lists in global scratch
+template <bool F>
 __global__ void __launch_bounds__(128) k_refine_scratch(DLayer P, DLayer R, const uint2* __restrict__ pairs, const uint32_t* __restrict__ heavy,
                                                        uint64_t nh, RefineArgs rp, uint8_t* flag, double* area, double4* ev, uint32_t* evb,
                                                        unsigned char* scratch, int cap, int* err) {
   const int lane = threadIdx.x & 31;
   const uint64_t w = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
-  unsigned char* base = scratch + w * 2 * (size_t)cap * EDGE_BYTES;
-  EList LA = carve(base, cap), LB = carve(base + (size_t)cap * EDGE_BYTES, cap);
+  unsigned char* base = scratch + w * 2 * (size_t)cap * Cfg<F>::edge;
+  EList LA = carve_t<F>(base, cap), LB = carve_t<F>(base + (size_t)cap * Cfg<F>::edge, cap);
   for (uint64_t h = w; h < nh; h += nw) {
     const uint32_t p = heavy[h];
     const uint2 pr = pairs[p];
     uint8_t f; double ar; double4 e4; uint32_t b4;
-    const bool ok = refine_pair(P, R, pr.x, pr.y, rp, LA, LB, cap, lane, f, ar, e4, b4);
+    const bool ok = refine_pair_t<F>(P, R, pr.x, pr.y, rp, LA, LB, cap, lane, f, ar, e4, b4);
     if (lane == 0) {
       if (!ok) *err = 1;
       else {
@@ -327,18 +411,20 @@ __global__ void __launch_bounds__(128) k_refine_scratch(DLayer P, DLayer R, cons
   }
 }
 
-uint64_t refine(gsj_ctx* c, const gsj_layer* P, const gsj_layer* R, const uint2* pairs, uint64_t np, const RefineArgs& rp, int mode,
-                uint8_t* flag, double* area, double4* ev, uint32_t* evb) {
-  (void)mode;
-  if (!np) return 0;
+template <bool F>
+static uint64_t refine_t(gsj_ctx* c, const gsj_layer* P, const gsj_layer* R, const uint2* pairs, uint64_t np, const RefineArgs& rp, uint8_t* flag,
+                         double* area, double4* ev, uint32_t* evb) {
   cudaStream_t s = c->stream;
-  if (!c->refine_attr) { GSJ_CK(cudaFuncSetAttribute(k_refine, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)RB_SMEM)); c->refine_attr = 1; }
+  if (!(c->refine_attr & (F ? 2 : 1))) {
+    GSJ_CK(cudaFuncSetAttribute(k_refine<F>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cfg<F>::smem));
+    c->refine_attr |= F ? 2 : 1;
+  }
   unsigned long long* ctr = c->counters.as<unsigned long long>(8);
   int* err = reinterpret_cast<int*>(ctr + 1);
   GSJ_CK(cudaMemsetAsync(ctr, 0, 16, s));
   uint32_t* heavy = c->heavy.as<uint32_t>(np);
-  const int blocks = (int)std::min<uint64_t>((np + RB_WARPS - 1) / RB_WARPS, (uint64_t)c->sm_count * 6);
-  k_refine<<<blocks, RB_WARPS * 32, RB_SMEM, s>>>(P->d, R->d, pairs, np, rp, flag, area, ev, evb, heavy, ctr); c->launches++;
+  const int blocks = (int)std::min<uint64_t>((np + RB_WARPS - 1) / RB_WARPS, (uint64_t)c->sm_count * 8);
+  k_refine<F><<<blocks, RB_WARPS * 32, Cfg<F>::smem, s>>>(P->d, R->d, pairs, np, rp, flag, area, ev, evb, heavy, ctr); c->launches++;
   GSJ_CK(cudaGetLastError());
   unsigned long long* h = c->h_counters.as<unsigned long long>(2);
   GSJ_CK(cudaMemcpyAsync(h, ctr, 16, cudaMemcpyDeviceToHost, s));
@@ -347,19 +433,26 @@ uint64_t refine(gsj_ctx* c, const gsj_layer* P, const gsj_layer* R, const uint2*
   if (nh) {
     // list capacity rounded to 8 edges keeps every double array of the slab 8-byte aligned
     const int cap = (int)((std::max<uint32_t>(std::max(P->max_geom_edges, R->max_geom_edges), 1u) + 7u) & ~7u);
-    const size_t per = 2 * (size_t)cap * EDGE_BYTES;
+    const size_t per = 2 * (size_t)cap * Cfg<F>::edge;
     uint64_t nwarps = std::min<uint64_t>(nh, std::max<uint64_t>(1, (1ull << 30) / per));
     nwarps = std::min<uint64_t>(nwarps, (uint64_t)c->sm_count * 32);
     nwarps = (nwarps + 3) / 4 * 4;
     unsigned char* scr = c->scratch.as<unsigned char>(per * nwarps);
     GSJ_CK(cudaMemsetAsync(err, 0, 4, s));
-    k_refine_scratch<<<(int)(nwarps / 4), 128, 0, s>>>(P->d, R->d, pairs, heavy, nh, rp, flag, area, ev, evb, scr, cap, err); c->launches++;
+    k_refine_scratch<F><<<(int)(nwarps / 4), 128, 0, s>>>(P->d, R->d, pairs, heavy, nh, rp, flag, area, ev, evb, scr, cap, err); c->launches++;
     GSJ_CK(cudaGetLastError());
     GSJ_CK(cudaMemcpyAsync(h, ctr, 16, cudaMemcpyDeviceToHost, s));
     GSJ_CK(cudaStreamSynchronize(s));
     if (reinterpret_cast<int*>(h + 1)[0]) throw Error(GSJ_ERR_CUDA, "oversized pair exceeded the scratch edge capacity");
   }
   return nh;
+}
+
+uint64_t refine(gsj_ctx* c, const gsj_layer* P, const gsj_layer* R, const uint2* pairs, uint64_t np, const RefineArgs& rp, int mode,
+                uint8_t* flag, double* area, double4* ev, uint32_t* evb) {
+  if (!np) return 0;
+  return mode == GSJ_REFINE_FILTERED ? refine_t<true>(c, P, R, pairs, np, rp, flag, area, ev, evb)
+                                     : refine_t<false>(c, P, R, pairs, np, rp, flag, area, ev, evb);
 }
 
 }  // namespace gsj
