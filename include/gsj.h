@@ -109,6 +109,22 @@ int gsj_join_points(gsj_ctx* ctx, const gsj_layer* pts, const gsj_layer* R, cons
 int gsj_cluster(gsj_ctx* ctx, const gsj_layer* P, uint32_t nparent, const gsj_join_opts* o, uint32_t* root,
                 gsj_join_stats* stats);
 
+/* Host-side layer preparation (no device involved). Outputs are allocated by the library; free each with
+ * gsj_host_free. Both return GSJ_OK or an error code.
+ * Subdivision (engine/subdivide.h:71-129): geometries with more than maxv vertices are cut recursively at the middle
+ * of their bbox's longer side (Sutherland-Hodgman, FP64); parent[piece] = geometry, syn[v] = 1 for edges created
+ * by a cut (ignored for boundary contact). Feed the result to gsj_layer_upload_polygons with parent and syn. */
+int gsj_subdivide(uint64_t n, uint64_t nr, uint64_t nv, const uint64_t* gro, const uint64_t* rvo, const double* xy, int maxv,
+                  uint64_t* out_n, uint64_t* out_nr, uint64_t* out_nv, uint64_t** out_gro, uint64_t** out_rvo, double** out_xy,
+                  uint32_t** out_parent, uint8_t** out_syn);
+/* Exact deduplication of identical geometries (engine/dedup.h:51-124): distinct geometries in order of first
+ * occurrence (morton = 1: in Z-order of their bbox centres); members of distinct geometry g are the original
+ * indices midx[moff[g] .. moff[g+1]). Results on the distinct set expand to members x members. */
+int gsj_dedup(uint64_t n, uint64_t nr, uint64_t nv, const uint64_t* gro, const uint64_t* rvo, const double* xy, int morton,
+              uint64_t* out_n, uint64_t* out_nr, uint64_t* out_nv, uint64_t** out_gro, uint64_t** out_rvo, double** out_xy,
+              uint64_t** out_moff, uint32_t** out_midx);
+void gsj_host_free(void* p);
+
 /* Pair sink for distance / buffer joins: (P parent, R parent) pairs. */
 typedef int (*gsj_pairs_sink)(void* user, const uint32_t* pairs, uint64_t n);
 /* ST_DWithin(a::geography, b::geography, d) polygon x polygon: dwithin_join_stream (engine/buffer.cuh:892-991).

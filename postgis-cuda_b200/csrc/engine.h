@@ -87,7 +87,7 @@ struct gsj_ctx {
   int sm_count = 148;
   cudaStream_t stream = nullptr;
   std::string err;
-  int refine_attr = 0;
+  int refine_attr = 0, dw_attr = 0, er_attr = 0;
   uint64_t launches = 0;
   uint64_t node_visits = 0;   // LBVH nodes visited by traversals (roofline accounting)   // kernels launched by this context (reported per call in the stats)
   // scratch pools

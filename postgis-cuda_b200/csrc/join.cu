@@ -100,7 +100,7 @@ static uint32_t read_last(gsj_ctx* c, const uint32_t* off, const uint32_t* flag,
 }
 
 // Candidate search for probe rows [q0, q0 + nq) (in the given order), growing the pair buffer when needed.
-static uint64_t candidates(gsj_ctx* c, const float4* qbb, const uint32_t* qorder, uint32_t q0, uint32_t nq, const DBvh& T, int upper, uint2** out) {
+uint64_t candidates_for(gsj_ctx* c, const float4* qbb, const uint32_t* qorder, uint32_t q0, uint32_t nq, const DBvh& T, int upper, uint2** out) {
   uint64_t cap = std::max<uint64_t>((uint64_t)nq * 16, 1 << 16);
   // reuse the whole pooled buffer: as<uint2>(cap + 1) needs (cap + 1) * 8 + 16 bytes
   const uint64_t pooled = c->cand.cap >= 64 ? (c->cand.cap - 16) / sizeof(uint2) - 1 : 0;
@@ -150,7 +150,7 @@ void run_join(gsj_ctx* c, const gsj_layer* P, const gsj_layer* R, const RefineAr
     if (o.cancel && *o.cancel) throw Error(GSJ_ERR_CANCELLED, "cancelled");
     tm.start();
     uint2* pairs = nullptr;
-    uint64_t np = candidates(c, P->d.bb, whole ? P->bvh.order : nullptr, bt.q0, bt.nq, R->bvh, o.upper, &pairs);
+    uint64_t np = candidates_for(c, P->d.bb, whole ? P->bvh.order : nullptr, bt.q0, bt.nq, R->bvh, o.upper, &pairs);
     st.traverse_ms += tm.stop();
     st.candidates += np;
     st.batches++;
@@ -291,7 +291,7 @@ void run_points(gsj_ctx* c, const gsj_layer* pts, const gsj_layer* R, const gsj_
     const uint32_t nq = std::min(bq, n - q0);
     tm.start();
     uint2* pairs = nullptr;
-    uint64_t np = candidates(c, pts->d.bb, bq == n ? pts->bvh.order : nullptr, q0, nq, R->bvh, 0, &pairs);
+    uint64_t np = candidates_for(c, pts->d.bb, bq == n ? pts->bvh.order : nullptr, q0, nq, R->bvh, 0, &pairs);
     st.traverse_ms += tm.stop(); st.candidates += np; st.batches++;
     if (!np) continue;
     tm.start();
@@ -449,7 +449,7 @@ void cluster_host(gsj_ctx* c, const gsj_layer* P, uint32_t nparent, const gsj_jo
 
 void candidates_host(gsj_ctx* c, const gsj_layer* P, const gsj_layer* R, int upper, gsj_pairs_sink sink, void* user) {
   uint2* pairs = nullptr;
-  uint64_t np = candidates(c, P->d.bb, P->bvh.order, 0, P->d.n, R->bvh, upper, &pairs);
+  uint64_t np = candidates_for(c, P->d.bb, P->bvh.order, 0, P->d.n, R->bvh, upper, &pairs);
   uint32_t* hp = c->h_pairs.as<uint32_t>(2 * np + 2);
   GSJ_CK(cudaMemcpyAsync(hp, pairs, np * 8, cudaMemcpyDeviceToHost, c->stream));
   GSJ_CK(cudaStreamSynchronize(c->stream));

@@ -84,6 +84,11 @@ SIGNATURES = {
     "gsj_candidates": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_int, PAIRS_SINK, _vp]),
     "gsj_refine_pairs": (ctypes.c_int, [_vp, _vp, _vp, _vp, ctypes.c_uint64, ctypes.POINTER(RefineParams), ctypes.c_int, _vp, _vp, _vp, _vp]),
     "gsj_refine_pairs_noalloc": (ctypes.c_int, [_vp, _vp, _vp, _vp, ctypes.c_uint64, ctypes.POINTER(RefineParams), _vp, _vp, _vp, _vp]),
+    "gsj_subdivide": (ctypes.c_int, [ctypes.c_uint64] * 3 + [_vp] * 3 + [ctypes.c_int] + [ctypes.POINTER(ctypes.c_uint64)] * 3 +
+                      [ctypes.POINTER(_vp)] * 5),
+    "gsj_dedup": (ctypes.c_int, [ctypes.c_uint64] * 3 + [_vp] * 3 + [ctypes.c_int] + [ctypes.POINTER(ctypes.c_uint64)] * 3 +
+                  [ctypes.POINTER(_vp)] * 5),
+    "gsj_host_free": (None, [_vp]),
     "gsj_de9im_str": (None, [ctypes.c_uint32, ctypes.c_char_p]),
     "gsj_de9im_transpose": (ctypes.c_uint32, [ctypes.c_uint32]),
     "gsj_de9im_match": (ctypes.c_int, [ctypes.c_uint32, ctypes.c_char_p]),
@@ -128,6 +133,42 @@ def de9im_transpose(code: int) -> int:
 
 def de9im_match(code: int, pattern: str) -> bool:
     return bool(lib().gsj_de9im_match(code, pattern.encode()))
+
+
+def _take(ptr, count, dtype):
+    a = np.ctypeslib.as_array(ctypes.cast(ptr, ctypes.POINTER(np.ctypeslib.as_ctypes_type(dtype))), (max(count, 1),))[:count].copy()
+    lib().gsj_host_free(ptr)
+    return a
+
+
+def subdivide(ps, maxv: int):
+    """Pieces of at most ~maxv vertices (gsj_subdivide): a PolygonSet with .parent and .syn set."""
+    from .gen import PolygonSet
+    gro = np.ascontiguousarray(ps.gro, np.uint64); rvo = np.ascontiguousarray(ps.rvo, np.uint64); xy = np.ascontiguousarray(ps.xy, np.float64)
+    n, nr, nv = ctypes.c_uint64(), ctypes.c_uint64(), ctypes.c_uint64()
+    ptrs = [_vp() for _ in range(5)]
+    rc = lib().gsj_subdivide(len(gro) - 1, len(rvo) - 1, len(xy), gro.ctypes.data, rvo.ctypes.data, xy.ctypes.data, int(maxv),
+                             ctypes.byref(n), ctypes.byref(nr), ctypes.byref(nv), *[ctypes.byref(p) for p in ptrs])
+    if rc:
+        raise GsjError(rc, "gsj_subdivide failed")
+    return PolygonSet(_take(ptrs[0], n.value + 1, np.uint64), _take(ptrs[1], nr.value + 1, np.uint64),
+                      _take(ptrs[2], 2 * nv.value, np.float64).reshape(-1, 2), parent=_take(ptrs[3], n.value, np.uint32),
+                      syn=_take(ptrs[4], nv.value, np.uint8))
+
+
+def dedup(ps, morton=False):
+    """(distinct PolygonSet, moff, midx) (gsj_dedup)."""
+    from .gen import PolygonSet
+    gro = np.ascontiguousarray(ps.gro, np.uint64); rvo = np.ascontiguousarray(ps.rvo, np.uint64); xy = np.ascontiguousarray(ps.xy, np.float64)
+    n, nr, nv = ctypes.c_uint64(), ctypes.c_uint64(), ctypes.c_uint64()
+    ptrs = [_vp() for _ in range(5)]
+    rc = lib().gsj_dedup(len(gro) - 1, len(rvo) - 1, len(xy), gro.ctypes.data, rvo.ctypes.data, xy.ctypes.data, int(morton),
+                         ctypes.byref(n), ctypes.byref(nr), ctypes.byref(nv), *[ctypes.byref(p) for p in ptrs])
+    if rc:
+        raise GsjError(rc, "gsj_dedup failed")
+    u = PolygonSet(_take(ptrs[0], n.value + 1, np.uint64), _take(ptrs[1], nr.value + 1, np.uint64),
+                   _take(ptrs[2], 2 * nv.value, np.float64).reshape(-1, 2))
+    return u, _take(ptrs[3], n.value + 1, np.uint64), _take(ptrs[4], len(gro) - 1, np.uint32)
 
 
 @dataclasses.dataclass

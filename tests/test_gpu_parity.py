@@ -121,3 +121,38 @@ def test_bad_arguments_are_errors(engine, layers):
         engine.join(layers["parcels"][0], engine.upload_points(np.zeros((3, 2))))
     with pytest.raises(gsj.GsjError):
         engine.refine_pairs(layers["one"][0], layers["one"][0], np.array([[0, 5]], np.uint32))
+
+
+@pytest.fixture(scope="module")
+def pieces(engine):
+    import gsj
+    a = gsj.subdivide(gen.layer_parcels(8000, (-118.3, 33.95, -118.2, 34.05), seed=5), 24)
+    b = gsj.subdivide(gen.voronoi(50, gen.LA_BOX, 1, vmin=40, vmax=80), 16)
+    return {k: (engine.upload_polygons(v), O.OSet(v), v) for k, v in (("a", a), ("b", b))}
+
+
+@pytest.mark.parametrize("mode", MODES)
+def test_subdivided_join_bitexact(engine, pieces, mode):
+    for (x, y, upper) in (("a", "a", True), ("a", "b", False)):
+        for area, rel in ((True, False), (False, True)):
+            r = engine.join(pieces[x][0], pieces[y][0], want_area=area, want_relate=rel, upper=upper, refine_mode=mode)
+            p, oa, oc, nc = O.join(pieces[x][1], pieces[y][1], O.params(int(area), int(rel)), upper=upper)
+            gp, ga, gc = srt(r.pairs, r.area, r.code)
+            assert np.array_equal(gp, p)
+            if area:
+                assert np.array_equal(ga, oa)
+            if rel:
+                assert np.array_equal(gc, oc)
+
+
+def test_subdivided_points_cluster_dwithin(engine, pieces):
+    pts = gen.points(20000, (-118.3, 33.95, -118.2, 34.05), 8)
+    gp, gw, _ = engine.join_points(engine.upload_points(pts), pieces["a"][0])
+    op, ow, _ = O.pip(pts, pieces["a"][1])
+    gp, gw = srt(gp, gw)
+    assert np.array_equal(gp, op) and np.array_equal(gw, ow)
+    root, _ = engine.cluster(pieces["a"][0])
+    assert np.array_equal(root, O.cluster(pieces["a"][1], pieces["a"][0].info["nparent"]))
+    g, _ = engine.dwithin(pieces["a"][0], pieces["a"][0], 5.0, same=True)
+    o, _ = O.dwithin(pieces["a"][1], pieces["a"][1], 5.0, same=True)
+    assert set(map(tuple, g.tolist())) == set(map(tuple, o.tolist()))
