@@ -303,3 +303,479 @@ int64_t orc_pt_dwithin(const double* pts, uint64_t npts, const orc_set* Ro, doub
 }
 
 }  // extern "C"
+
+// ===== negative-buffer (erosion) intersects (buffer.cuh:275-889) ==============================================
+namespace {
+
+struct BEd { double x0, y0, x1, y1, ux, uy, L, ci, si; int succ, vt; };   // buffer.cuh:280
+struct BEl { double x0, y0, x1, y1; };
+constexpr double FILLET_QUANTUM = M_PI / 16.0;
+constexpr int ER_CAPE = 64, ER_CAPL = 128, ER_MAX_DEPTH = 12;              // buffer.cuh:590, 593
+
+// strictly inside the region within r of the boundary (buffer.cuh:285-319)
+bool in_excl(const std::vector<BEd>& E, double r, double x, double y, double eps) {
+  if (r <= 0) return false;
+  const double ri = r - eps;
+  for (size_t k = 0; k < E.size(); k++) {
+    const BEd& e = E[k];
+    if (x < std::fmin(e.x0, e.x1) - r || x > std::fmax(e.x0, e.x1) + r || y < std::fmin(e.y0, e.y1) - r || y > std::fmax(e.y0, e.y1) + r) continue;
+    double dx = x - e.x0, dy = y - e.y0;
+    double t = dx * e.ux + dy * e.uy, s = dy * e.ux - dx * e.uy;
+    if (std::fabs(s) < ri && t > -eps && t < e.L + eps) return true;
+    if (e.vt == 0) continue;
+    double vx = x - e.x1, vy = y - e.y1, d2 = vx * vx + vy * vy;
+    if (d2 >= r * r) continue;
+    const BEd& f = E[e.succ];
+    if (e.vt == 1) {
+      double s2 = vy * f.ux - vx * f.uy;
+      if (d2 < ri * ri && !(s > eps && s2 > eps)) return true;
+      continue;
+    }
+    double nkx = -e.uy, nky = e.ux, nsx = -f.uy, nsy = f.ux;
+    if (nkx * vy - nky * vx > eps) continue;
+    if (nsx * vy - nsy * vx < -eps) continue;
+    double chh = std::sqrt(0.5 * (1.0 + e.ci)), shh = std::sqrt(std::fmax(0.0, 0.5 * (1.0 - e.ci)));
+    double ch = r * chh - eps;
+    if (d2 < ch * ch) return true;
+    double mx = nkx * chh + nky * shh, my = -nkx * shh + nky * chh;
+    bool in = true;
+    for (int i = 0, m = e.vt - 1; i < m && in; i++) {
+      if (mx * vx + my * vy >= ch) in = false;
+      double t2 = mx * e.ci + my * e.si; my = -mx * e.si + my * e.ci; mx = t2;
+    }
+    if (in) return true;
+  }
+  return false;
+}
+// parity from c (buffer.cuh:322-334)
+bool inside_m(const std::vector<BEd>& E, double cx, double cy, bool in_c, double x, double y) {
+  bool in = in_c;
+  double sx0 = std::fmin(cx, x), sx1 = std::fmax(cx, x), sy0 = std::fmin(cy, y), sy1 = std::fmax(cy, y);
+  for (const BEd& e : E) {
+    if (std::fmax(e.x0, e.x1) < sx0 || std::fmin(e.x0, e.x1) > sx1 || std::fmax(e.y0, e.y1) < sy0 || std::fmin(e.y0, e.y1) > sy1) continue;
+    bool sc = left_of(e.x0, e.y0, e.x1, e.y1, cx, cy), sx = left_of(e.x0, e.y0, e.x1, e.y1, x, y);
+    if (sc == sx) continue;
+    bool su = orient(cx, cy, x, y, e.x0, e.y0) > 0, sv = orient(cx, cy, x, y, e.x1, e.y1) > 0;
+    if (su != sv) in = !in;
+  }
+  return in;
+}
+struct ESide { uint32_t g0, g1; double r; double bminx, bminy, bmaxx, bmaxy; };
+struct EFrame { double ox, oy, kx, ky; };
+inline void fv(const Set& S, double shx, double shy, uint64_t v, const EFrame& F, double& x, double& y) {   // buffer.cuh:352-355
+  x = (shx + S.q[2 * v]) * F.kx;
+  y = (shy + S.q[2 * v + 1]) * F.ky;
+}
+// c inside the parent (buffer.cuh:359-381)
+bool pip_parent(const Set& S, const ESide& s, const EFrame& F, double cx, double cy) {
+  bool in = false;
+  for (uint32_t g = s.g0; g < s.g1 && !in; g++) {
+    double bx0 = (S.ox[g] - F.ox) * F.kx, by0 = (S.oy[g] - F.oy) * F.ky, bx1 = (S.ox[g] + S.ex[g] - F.ox) * F.kx, by1 = (S.oy[g] + S.ey[g] - F.oy) * F.ky;
+    if (cx < bx0 - 1e-6 || cx > bx1 + 1e-6 || cy < by0 - 1e-6 || cy > by1 + 1e-6) continue;
+    double shx = S.ox[g] - F.ox, shy = S.oy[g] - F.oy, ox = bx0 - 1.0;
+    bool par = false;
+    for (uint64_t r = S.gro[g]; r < S.gro[g + 1]; r++)
+      for (uint64_t j = S.rvo[r] + 1; j < S.rvo[r + 1]; j++) {
+        double x0, y0, x1, y1; fv(S, shx, shy, j - 1, F, x0, y0); fv(S, shx, shy, j, F, x1, y1);
+        if ((y0 > cy) == (y1 > cy) && y0 != cy && y1 != cy) continue;
+        bool so = left_of(x0, y0, x1, y1, ox, cy), sc = left_of(x0, y0, x1, y1, cx, cy);
+        if (so == sc) continue;
+        bool su = orient(ox, cy, cx, cy, x0, y0) > 0, sv = orient(ox, cy, cx, cy, x1, y1) > 0;
+        if (su != sv) par = !par;
+      }
+    in = par;
+  }
+  return in;
+}
+// the parent's real edges meeting box C (buffer.cuh:384-408); returns the count (all kept: no cap here)
+void collect_side(const Set& S, const ESide& s, const EFrame& F, double cx0, double cy0, double cx1, double cy1, std::vector<BEd>& E) {
+  E.clear();
+  for (uint32_t g = s.g0; g < s.g1; g++) {
+    if ((S.ox[g] + S.ex[g] - F.ox) * F.kx < cx0 || (S.ox[g] - F.ox) * F.kx > cx1 || (S.oy[g] + S.ey[g] - F.oy) * F.ky < cy0 || (S.oy[g] - F.oy) * F.ky > cy1) continue;
+    double shx = S.ox[g] - F.ox, shy = S.oy[g] - F.oy;
+    for (uint64_t r = S.gro[g]; r < S.gro[g + 1]; r++)
+      for (uint64_t i = S.rvo[r]; i + 1 < S.rvo[r + 1]; i++) {
+        if (S.synv(i)) continue;
+        BEd ed{};
+        fv(S, shx, shy, i, F, ed.x0, ed.y0); fv(S, shx, shy, i + 1, F, ed.x1, ed.y1);
+        bool v = !(ed.x0 == ed.x1 && ed.y0 == ed.y1) &&
+                 !(std::fmax(ed.x0, ed.x1) < cx0 || std::fmin(ed.x0, ed.x1) > cx1 || std::fmax(ed.y0, ed.y1) < cy0 || std::fmin(ed.y0, ed.y1) > cy1);
+        if (v) E.push_back(ed);
+      }
+  }
+}
+// directions, successors, end-vertex regions (buffer.cuh:411-439)
+void prepare_side(std::vector<BEd>& E, double r) {
+  const int n = (int)E.size();
+  for (int k = 0; k < n; k++) {
+    double dx = E[k].x1 - E[k].x0, dy = E[k].y1 - E[k].y0, L = std::sqrt(dx * dx + dy * dy);
+    E[k].ux = dx / L; E[k].uy = dy / L; E[k].L = L;
+  }
+  for (int k = 0; k < n; k++) {
+    const BEd e = E[k];
+    int s = -1;
+    if (k + 1 < n && E[k + 1].x0 == e.x1 && E[k + 1].y0 == e.y1) s = k + 1;
+    else for (int j = 0; j < n; j++) if (j != k && E[j].x0 == e.x1 && E[j].y0 == e.y1) { s = j; break; }
+    int vt = 0; double ci = 1, si = 0;
+    if (s >= 0 && r > 0) {
+      const BEd& f = E[s];
+      double cr = e.ux * f.uy - e.uy * f.ux, dt = e.ux * f.ux + e.uy * f.uy;
+      if (cr > 0) vt = 1;
+      else if (cr < 0 || dt < 0) {
+        double th = std::atan2(-cr, dt);
+        if (cr == 0) th = M_PI;
+        int m = (int)(th / FILLET_QUANTUM + 0.5);
+        if (m < 1) m = 1;
+        double inc = th / m; ci = std::cos(inc); si = std::sin(inc);
+        vt = m + 1;
+      }
+    }
+    E[k].succ = s; E[k].vt = vt; E[k].ci = ci; E[k].si = si;
+  }
+}
+// raw offset curve elements meeting W +- eps, in the warp's order: per 32-edge chunk, element index, edge (buffer.cuh:442-472)
+void build_elements(const std::vector<BEd>& E, double r, double wx0, double wy0, double wx1, double wy1, double eps, std::vector<BEl>& L) {
+  L.clear();
+  const int n = (int)E.size();
+  for (int base = 0; base < n; base += 32) {
+    int mx = 0;
+    for (int k = base; k < std::min(n, base + 32); k++) mx = std::max(mx, 1 + (E[k].vt >= 2 ? E[k].vt - 1 : 0));
+    struct St { double wxr, wyr, px, py; };
+    std::vector<St> st(32);
+    for (int l = 0; l < 32 && base + l < n; l++) {
+      const BEd& e = E[base + l];
+      double nkx = -e.uy, nky = e.ux;
+      st[l] = St{nkx, nky, e.x1 + r * nkx, e.y1 + r * nky};
+    }
+    for (int it = 0; it < mx; it++)
+      for (int l = 0; l < 32 && base + l < n; l++) {
+        const BEd& e = E[base + l];
+        int ne = 1 + (e.vt >= 2 ? e.vt - 1 : 0);
+        if (it >= ne) continue;
+        double nkx = -e.uy, nky = e.ux, nsx = 0, nsy = 0;
+        if (e.vt >= 2) { nsx = -E[e.succ].uy; nsy = E[e.succ].ux; }
+        BEl el;
+        if (it == 0) { el.x0 = e.x0 + r * nkx; el.y0 = e.y0 + r * nky; el.x1 = e.x1 + r * nkx; el.y1 = e.y1 + r * nky; }
+        else {
+          St& s = st[l];
+          double t2 = s.wxr * e.ci + s.wyr * e.si; s.wyr = -s.wxr * e.si + s.wyr * e.ci; s.wxr = t2;
+          double qx, qy;
+          if (it == ne - 1) { qx = e.x1 + r * nsx; qy = e.y1 + r * nsy; } else { qx = e.x1 + r * s.wxr; qy = e.y1 + r * s.wyr; }
+          el.x0 = s.px; el.y0 = s.py; el.x1 = qx; el.y1 = qy; s.px = qx; s.py = qy;
+        }
+        if (!(std::fmax(el.x0, el.x1) < wx0 - eps || std::fmin(el.x0, el.x1) > wx1 + eps || std::fmax(el.y0, el.y1) < wy0 - eps || std::fmin(el.y0, el.y1) > wy1 + eps))
+          L.push_back(el);
+      }
+  }
+}
+// intersection points of two intersecting segments (buffer.cuh:475-493)
+int seg_points(const BEl& p, const BEl& q, double* xs, double* ys) {
+  double rx = p.x1 - p.x0, ry = p.y1 - p.y0, sx = q.x1 - q.x0, sy = q.y1 - q.y0;
+  double den = rx * sy - ry * sx;
+  if (den != 0) {
+    double t = ((q.x0 - p.x0) * sy - (q.y0 - p.y0) * sx) / den;
+    t = std::fmin(1.0, std::fmax(0.0, t));
+    xs[0] = p.x0 + t * rx; ys[0] = p.y0 + t * ry;
+    return 1;
+  }
+  double l2 = rx * rx + ry * ry;
+  if (l2 == 0) { xs[0] = p.x0; ys[0] = p.y0; return 1; }
+  double t0 = ((q.x0 - p.x0) * rx + (q.y0 - p.y0) * ry) / l2, t1 = ((q.x1 - p.x0) * rx + (q.y1 - p.y0) * ry) / l2;
+  double lo = std::fmax(0.0, std::fmin(t0, t1)), hi = std::fmin(1.0, std::fmax(t0, t1));
+  if (lo > hi) { double m = 0.5 * (lo + hi); lo = hi = std::fmin(1.0, std::fmax(0.0, m)); }
+  xs[0] = p.x0 + lo * rx; ys[0] = p.y0 + lo * ry;
+  xs[1] = p.x0 + hi * rx; ys[1] = p.y0 + hi * ry;
+  xs[2] = p.x0 + 0.5 * (lo + hi) * rx; ys[2] = p.y0 + 0.5 * (lo + hi) * ry;
+  return 3;
+}
+
+struct Win { double x0, y0, x1, y1; };
+
+// er_pair (buffer.cuh:499-588): 1 / 0, or -1 when a list exceeded the caps (capE / capL < 0: unlimited)
+int er_pair(const Set& P, const Set& R, uint32_t a0, uint32_t a1, uint32_t b0, uint32_t b1, double ra_nom, double rb_nom, int capE, int capL,
+            const Win* tile, Win* wout) {
+  ESide A{a0, a1, 0, 1e300, 1e300, -1e300, -1e300}, B{b0, b1, 0, 1e300, 1e300, -1e300, -1e300};
+  if (A.g0 >= A.g1 || B.g0 >= B.g1) return 0;
+  auto bbox = [](const Set& S, ESide& s) {
+    for (uint32_t g = s.g0; g < s.g1; g++) {
+      s.bminx = std::fmin(s.bminx, S.ox[g]); s.bminy = std::fmin(s.bminy, S.oy[g]);
+      s.bmaxx = std::fmax(s.bmaxx, S.ox[g] + S.ex[g]); s.bmaxy = std::fmax(s.bmaxy, S.oy[g] + S.ey[g]);
+    }
+  };
+  bbox(P, A); bbox(R, B);
+  double dax, day, dbx, dby;
+  deg_cover(A.bminy, A.bmaxy, ra_nom * 0.998, false, dax, day);
+  deg_cover(B.bminy, B.bmaxy, rb_nom * 0.998, false, dbx, dby);
+  double wx0 = std::fmax(A.bminx + dax, B.bminx + dbx), wx1 = std::fmin(A.bmaxx - dax, B.bmaxx - dbx);
+  double wy0 = std::fmax(A.bminy + day, B.bminy + dby), wy1 = std::fmin(A.bmaxy - day, B.bmaxy - dby);
+  if (tile) { wx0 = std::fmax(wx0, tile->x0); wy0 = std::fmax(wy0, tile->y0); wx1 = std::fmin(wx1, tile->x1); wy1 = std::fmin(wy1, tile->y1); }
+  if (wx0 > wx1 || wy0 > wy1) return 0;
+  if (wout) *wout = Win{wx0, wy0, wx1, wy1};
+  double clon = 0.5 * (wx0 + wx1), clat = 0.5 * (wy0 + wy1);
+  A.r = ra_nom > 0 ? ra_nom / utm_k(0.5 * (A.bminx + A.bmaxx), 0.5 * (A.bminy + A.bmaxy), clon, clat) : 0.0;
+  B.r = rb_nom > 0 ? rb_nom / utm_k(0.5 * (B.bminx + B.bmaxx), 0.5 * (B.bminy + B.bmaxy), clon, clat) : 0.0;
+  EFrame F; F.ox = P.ox[A.g0]; F.oy = P.oy[A.g0]; m_per_deg(clat, F.kx, F.ky);
+  double Wx0 = (wx0 - F.ox) * F.kx, Wx1 = (wx1 - F.ox) * F.kx, Wy0 = (wy0 - F.oy) * F.ky, Wy1 = (wy1 - F.oy) * F.ky;
+  double ext = std::fmax(std::fmax(std::fabs(Wx0), std::fabs(Wx1)), std::fmax(std::fabs(Wy0), std::fabs(Wy1))) + std::fmax(A.r, B.r);
+  const double eps = 1e-9 + 1e-12 * ext;
+  double fe = 1.0 + 2.0 * 0.5 * (wy1 - wy0) * DEG * (std::fabs(std::tan(clat * DEG)) + 0.05);
+  double ma = A.r * fe + 1e-6, mb = B.r * fe + 1e-6;
+  std::vector<BEd> EA, EB; std::vector<BEl> LA, LB;
+  collect_side(P, A, F, Wx0 - ma, Wy0 - ma, Wx1 + ma, Wy1 + ma, EA);
+  collect_side(R, B, F, Wx0 - mb, Wy0 - mb, Wx1 + mb, Wy1 + mb, EB);
+  if (capE >= 0 && ((int)EA.size() > capE || (int)EB.size() > capE)) return -1;
+  prepare_side(EA, A.r); prepare_side(EB, B.r);
+  build_elements(EA, A.r, Wx0, Wy0, Wx1, Wy1, eps, LA);
+  build_elements(EB, B.r, Wx0, Wy0, Wx1, Wy1, eps, LB);
+  if (capL >= 0 && ((int)LA.size() > capL || (int)LB.size() > capL)) return -1;
+  auto inW = [&](double x, double y) { return x >= Wx0 - eps && x <= Wx1 + eps && y >= Wy0 - eps && y <= Wy1 + eps; };
+  for (const BEl& p : LA) {
+    double px0 = std::fmin(p.x0, p.x1), px1 = std::fmax(p.x0, p.x1), py0 = std::fmin(p.y0, p.y1), py1 = std::fmax(p.y0, p.y1);
+    for (const BEl& q : LB) {
+      if (std::fmax(q.x0, q.x1) < px0 || std::fmin(q.x0, q.x1) > px1 || std::fmax(q.y0, q.y1) < py0 || std::fmin(q.y0, q.y1) > py1) continue;
+      if (!seg_isect(p.x0, p.y0, p.x1, p.y1, q.x0, q.y0, q.x1, q.y1)) continue;
+      double xs[3], ys[3]; int k = seg_points(p, q, xs, ys);
+      for (int t = 0; t < k; t++)
+        if (inW(xs[t], ys[t]) && !in_excl(EA, A.r, xs[t], ys[t], eps) && !in_excl(EB, B.r, xs[t], ys[t], eps)) return 1;
+    }
+  }
+  const double cx = Wx0 + 0.381966 * (Wx1 - Wx0), cy = Wy0 + 0.414213 * (Wy1 - Wy0);
+  bool inA_c = pip_parent(P, A, F, cx, cy);
+  bool inB_c = pip_parent(R, B, F, cx, cy);
+  for (int side = 0; side < 2; side++) {
+    const std::vector<BEd>& ES = side ? EB : EA; const std::vector<BEd>& EO = side ? EA : EB;
+    const std::vector<BEl>& LS = side ? LB : LA;
+    double rs = side ? B.r : A.r, ro = side ? A.r : B.r;
+    bool inO_c = side ? inA_c : inB_c;
+    auto vio = [&](double x, double y) {
+      return inW(x, y) && !in_excl(ES, rs, x, y, eps) && inside_m(EO, cx, cy, inO_c, x, y) && !in_excl(EO, ro, x, y, eps);
+    };
+    for (size_t i = 0; i < LS.size(); i++) {
+      const BEl& p = LS[i];
+      if (vio(p.x0, p.y0) || vio(p.x1, p.y1)) return 1;
+      double px0 = std::fmin(p.x0, p.x1), px1 = std::fmax(p.x0, p.x1), py0 = std::fmin(p.y0, p.y1), py1 = std::fmax(p.y0, p.y1);
+      for (size_t j = i + 1; j < LS.size(); j++) {
+        const BEl& q = LS[j];
+        if (std::fmax(q.x0, q.x1) < px0 || std::fmin(q.x0, q.x1) > px1 || std::fmax(q.y0, q.y1) < py0 || std::fmin(q.y0, q.y1) > py1) continue;
+        if (!seg_isect(p.x0, p.y0, p.x1, p.y1, q.x0, q.y0, q.x1, q.y1)) continue;
+        double xs[3], ys[3]; int k = seg_points(p, q, xs, ys);
+        for (int t = 0; t < k; t++) if (vio(xs[t], ys[t])) return 1;
+      }
+    }
+  }
+  return 0;
+}
+
+// the reference's overflow handling: window quadrants while larger than the radius (depth <= 12), then one
+// evaluation with unlimited lists (k_erode_tiles / er_overflow / k_erode_slab, buffer.cuh:608-684)
+int er_eval(const Set& P, const Set& R, uint32_t a0, uint32_t a1, uint32_t b0, uint32_t b1, double ra, double rb, const Win* tile, int depth) {
+  Win win;
+  int r = er_pair(P, R, a0, a1, b0, b1, ra, rb, ER_CAPE, ER_CAPL, tile, &win);
+  if (r >= 0) return r;
+  double kx, ky; m_per_deg(0.5 * (win.y0 + win.y1), kx, ky);
+  double ext = std::fmax((win.x1 - win.x0) * kx, (win.y1 - win.y0) * ky);
+  if (depth < ER_MAX_DEPTH && ext > std::fmax(ra, rb)) {
+    double xm = 0.5 * (win.x0 + win.x1), ym = 0.5 * (win.y0 + win.y1);
+    Win q[4] = {{win.x0, win.y0, xm, ym}, {xm, win.y0, win.x1, ym}, {win.x0, ym, xm, win.y1}, {xm, ym, win.x1, win.y1}};
+    for (int i = 0; i < 4; i++) if (er_eval(P, R, a0, a1, b0, b1, ra, rb, &q[i], depth + 1) == 1) return 1;
+    return 0;
+  }
+  return er_pair(P, R, a0, a1, b0, b1, ra, rb, -1, -1, &win, nullptr) == 1 ? 1 : 0;
+}
+
+inline void piece_range(const Set& S, uint32_t p, const std::vector<uint32_t>& pf, uint32_t& g0, uint32_t& g1) {
+  if (S.has_parent) { g0 = pf[p]; g1 = pf[p + 1]; } else { g0 = p; g1 = p + 1; }
+}
+std::vector<uint32_t> piece_first(const Set& S) {   // k_piece_first (buffer.cuh:342-348)
+  std::vector<uint32_t> pf(S.nparent + 1, (uint32_t)S.n);
+  for (int64_t g = (int64_t)S.n - 1; g >= 0; g--) pf[S.parent[g]] = (uint32_t)g;
+  for (int64_t p = (int64_t)S.nparent - 1; p >= 0; p--) if (pf[p] == S.n && p + 1 <= (int64_t)S.nparent) pf[p] = pf[p + 1];
+  return pf;
+}
+
+}  // namespace
+
+extern "C" {
+
+// erode_join_stream (buffer.cuh:765-889): pass 1 = intersects + area join (with the shrunk-bbox prefilter), then
+// the area filter and the erosion test on the surviving parent pairs
+int64_t orc_erode(const orc_set* Po, const orc_set* Ro, double ra, double rb, int same, const uint8_t* need_self, int nthreads, uint32_t** out_pairs) {
+  const Set& P = Po->s; const Set& R = Ro->s;
+  int nth = nthreads_or_default(nthreads);
+  uint32_t* cand = nullptr;
+  int64_t nc = candidates_bb(P.bb.data(), P.n, R, same, nth, &cand);
+  // k_er_prefilter (buffer.cuh:742-762): whole-geometry pieces whose shrunk bboxes are disjoint cannot meet
+  auto whole = [](const Set& S, uint32_t g) {
+    if (!S.has_parent) return true;
+    uint32_t q = S.parent[g];
+    return (g == 0 || S.parent[g - 1] != q) && (g + 1 >= S.n || S.parent[g + 1] != q);
+  };
+  std::vector<uint32_t> kept;
+  for (int64_t i = 0; i < nc; i++) {
+    uint32_t a = cand[2 * i], b = cand[2 * i + 1];
+    bool k = true;
+    if ((ra > 0 || rb > 0) && whole(P, a) && whole(R, b)) {
+      double dax, day, dbx, dby;
+      deg_cover(P.oy[a], P.oy[a] + P.ey[a], ra * 0.998, false, dax, day);
+      deg_cover(R.oy[b], R.oy[b] + R.ey[b], rb * 0.998, false, dbx, dby);
+      double wx0 = std::fmax(P.ox[a] + dax, R.ox[b] + dbx), wx1 = std::fmin(P.ox[a] + P.ex[a] - dax, R.ox[b] + R.ex[b] - dbx);
+      double wy0 = std::fmax(P.oy[a] + day, R.oy[b] + dby), wy1 = std::fmin(P.oy[a] + P.ey[a] - day, R.oy[b] + R.ey[b] - dby);
+      k = wx0 <= wx1 && wy0 <= wy1;
+    }
+    if (k) { kept.push_back(a); kept.push_back(b); }
+  }
+  free(cand);
+  // pass 1: exact intersects + area over the kept piece pairs, folded to parents (engine.cuh:963-1042 semantics)
+  int64_t nk = (int64_t)kept.size() / 2;
+  orc_params rp{1e-12, 1e-7, 1e-11, 1, 0, 0};
+  std::vector<uint8_t> flag(nk); std::vector<double> area(nk);
+  orc_refine_pairs(Po, Ro, kept.data(), nk, &rp, flag.data(), area.data(), nullptr, nullptr, nth);
+  const bool agg = P.has_parent || R.has_parent;
+  std::vector<std::pair<uint64_t, double>> parents;   // (parent key, area) of parent pairs with real contact
+  {
+    std::vector<int64_t> idx;
+    for (int64_t i = 0; i < nk; i++) if (agg ? flag[i] != 0 : flag[i] == 1) idx.push_back(i);
+    auto key = [&](int64_t i) { return ((uint64_t)P.pid(kept[2 * i]) << 32) | R.pid(kept[2 * i + 1]); };
+    std::stable_sort(idx.begin(), idx.end(), [&](int64_t x, int64_t y) { return key(x) < key(y); });
+    for (size_t k = 0; k < idx.size();) {
+      size_t m = k; uint64_t kk = key(idx[k]); double a = 0; uint8_t f = 255;
+      for (; m < idx.size() && key(idx[m]) == kk; m++) { a += area[idx[m]]; f = std::min(f, flag[idx[m]]); }
+      if (f == 1) parents.push_back({kk, a});
+      k = m;
+    }
+  }
+  // k_er_filter (buffer.cuh:720-738)
+  const double rmin = (ra > 0 && rb > 0) ? std::min(ra, rb) : (ra > 0 || rb > 0 ? 0.0 : -1.0);
+  std::vector<uint32_t> pfP, pfR;
+  if (P.has_parent) pfP = piece_first(P);
+  if (R.has_parent) pfR = piece_first(R);
+  std::vector<uint64_t> ep;
+  for (auto& pa : parents) {
+    uint32_t x = (uint32_t)(pa.first >> 32), y = (uint32_t)pa.first;
+    bool k = true;
+    if (same && x == y && need_self) k = need_self[x] != 0;
+    if (k && rmin >= 0) {
+      uint32_t g = P.has_parent ? pfP[x] : x;
+      double y0 = P.oy[g], y1 = y0 + P.ey[g];
+      double lat = (y0 <= 0 && y1 >= 0) ? 0.0 : (std::fabs(y0) < std::fabs(y1) ? y0 : y1);
+      double kx, ky; m_per_deg(lat, kx, ky);
+      double a_m2 = pa.second * kx * ky * 1.001;
+      double r = 0.98 * rmin;
+      k = rmin > 0 ? a_m2 >= M_PI * r * r : pa.second > 0;
+    }
+    if (k) ep.push_back(pa.first);
+  }
+  std::vector<uint8_t> hit(ep.size());
+#pragma omp parallel for num_threads(nth) schedule(dynamic, 16)
+  for (int64_t i = 0; i < (int64_t)ep.size(); i++) {
+    uint32_t x = (uint32_t)(ep[i] >> 32), y = (uint32_t)ep[i], a0, a1, b0, b1;
+    piece_range(P, x, pfP, a0, a1); piece_range(R, y, pfR, b0, b1);
+    hit[i] = (uint8_t)er_eval(P, R, a0, a1, b0, b1, ra, rb, nullptr, 0);
+  }
+  std::vector<std::pair<uint32_t, uint32_t>> out;
+  for (size_t i = 0; i < ep.size(); i++) if (hit[i]) out.push_back({(uint32_t)(ep[i] >> 32), (uint32_t)ep[i]});
+  return emit(out, out_pairs);
+}
+
+}  // extern "C"
+
+namespace {
+// inside the exclusion region of vertex v (edges with unit directions e -> f), w relative to v (buffer.cuh:1059-1083)
+bool vertex_excl(double ex, double ey, double fx, double fy, double r, double wx, double wy, double eps) {
+  double d2 = wx * wx + wy * wy;
+  if (d2 >= r * r) return false;
+  double cr = ex * fy - ey * fx, dt = ex * fx + ey * fy;
+  if (cr > 0) {
+    double ri = r - eps, s1 = wy * ex - wx * ey, s2 = wy * fx - wx * fy;
+    return d2 < ri * ri && !(s1 > eps && s2 > eps);
+  }
+  if (cr == 0 && dt >= 0) return false;
+  double th = cr == 0 ? M_PI : std::atan2(-cr, dt);
+  int m = (int)(th / FILLET_QUANTUM + 0.5);
+  if (m < 1) m = 1;
+  double inc = th / m, ci = std::cos(inc), si = std::sin(inc);
+  double nkx = -ey, nky = ex, nsx = -fy, nsy = fx;
+  if (nkx * wy - nky * wx > eps || nsx * wy - nsy * wx < -eps) return false;
+  double chh = std::sqrt(0.5 * (1.0 + ci)), shh = std::sqrt(std::fmax(0.0, 0.5 * (1.0 - ci)));
+  double ch = r * chh - eps;
+  if (d2 < ch * ch) return true;
+  double mx = nkx * chh + nky * shh, my = -nkx * shh + nky * chh;
+  for (int i = 0; i < m; i++) {
+    if (mx * wx + my * wy >= ch) return false;
+    double t2 = mx * ci + my * si; my = -mx * si + my * ci; mx = t2;
+  }
+  return true;
+}
+}  // namespace
+
+extern "C" {
+
+// k_pt_erode (buffer.cuh:1087-1132) + the (point, parent) OR fold of points_buffer_join_stream (:1187-1208)
+int64_t orc_pt_erode(const double* pts, uint64_t npts, const orc_set* Ro, double r_nom, int nthreads, uint32_t** out_pairs) {
+  const Set& R = Ro->s;
+  int nth = nthreads_or_default(nthreads);
+  const double grow = r_nom * 1.002;
+  std::vector<float> qbb(4 * npts);
+  for (uint64_t i = 0; i < npts; i++) {
+    if (grow > 0) expand_box(pts[2 * i], pts[2 * i + 1], pts[2 * i], pts[2 * i + 1], grow, &qbb[4 * i]);
+    else { qbb[4 * i] = f_down(pts[2 * i]); qbb[4 * i + 1] = f_down(pts[2 * i + 1]); qbb[4 * i + 2] = f_up(pts[2 * i]); qbb[4 * i + 3] = f_up(pts[2 * i + 1]); }
+  }
+  uint32_t* cand = nullptr;
+  int64_t nc = candidates_bb(qbb.data(), npts, R, 0, nth, &cand);
+  std::vector<uint8_t> bits(nc);
+#pragma omp parallel for num_threads(nth) schedule(dynamic, 1024)
+  for (int64_t i = 0; i < nc; i++) {
+    uint32_t p = cand[2 * i], g = cand[2 * i + 1];
+    double ptx = pts[2 * p], pty = pts[2 * p + 1];
+    double r = r_nom / utm_k(R.ox[g] + 0.5 * R.ex[g], R.oy[g] + 0.5 * R.ey[g], ptx, pty);
+    double kx, ky; m_per_deg(pty, kx, ky);
+    const double eps = 1e-9;
+    double shx = R.ox[g] - ptx, shy = R.oy[g] - pty, ox = shx * kx - 1.0;
+    auto vx = [&](uint64_t j, double& x, double& y) { x = (shx + R.q[2 * j]) * kx; y = (shy + R.q[2 * j + 1]) * ky; };
+    bool par = false, ex = false;
+    for (uint64_t rr = R.gro[g]; rr < R.gro[g + 1] && !ex; rr++) {
+      uint64_t s0 = R.rvo[rr], e = R.rvo[rr + 1];
+      if (e - s0 < 2) continue;
+      bool pv = false; double pux = 0, puy = 0;
+      { uint64_t j = e - 2; if (!R.synv(j)) { double a, b, c, dd; vx(j, a, b); vx(j + 1, c, dd); double L = std::hypot(c - a, dd - b);
+          if (L > 0) { pv = true; pux = (c - a) / L; puy = (dd - b) / L; } } }
+      double x0, y0; vx(s0, x0, y0);
+      for (uint64_t j = s0; j + 1 < e && !ex; j++) {
+        double x1, y1; vx(j + 1, x1, y1);
+        if (!((y0 > 0) == (y1 > 0) && y0 != 0 && y1 != 0)) {
+          bool so = left_of(x0, y0, x1, y1, ox, 0.0), sp = left_of(x0, y0, x1, y1, 0.0, 0.0);
+          if (so != sp) {
+            bool su = orient(ox, 0.0, 0.0, 0.0, x0, y0) > 0, sv = orient(ox, 0.0, 0.0, 0.0, x1, y1) > 0;
+            if (su != sv) par = !par;
+          }
+        }
+        double L = std::hypot(x1 - x0, y1 - y0);
+        if (R.synv(j) || L == 0) { if (R.synv(j)) pv = false; x0 = x1; y0 = y1; continue; }
+        double ux = (x1 - x0) / L, uy = (y1 - y0) / L;
+        if (r > 0) {
+          double t = -x0 * ux - y0 * uy, s = -y0 * ux + x0 * uy;
+          if (std::fabs(s) < r - eps && t > -eps && t < L + eps) ex = true;
+          else if (pv && vertex_excl(pux, puy, ux, uy, r, -x0, -y0, eps)) ex = true;
+        }
+        pv = true; pux = ux; puy = uy;
+        x0 = x1; y0 = y1;
+      }
+    }
+    bits[i] = ex ? 2 : (par ? 1 : 0);
+  }
+  // OR per (point, parent), keep == 1
+  std::vector<std::pair<uint64_t, uint8_t>> kv;
+  for (int64_t i = 0; i < nc; i++) kv.push_back({((uint64_t)cand[2 * i] << 32) | R.pid(cand[2 * i + 1]), bits[i]});
+  free(cand);
+  std::sort(kv.begin(), kv.end());
+  std::vector<std::pair<uint32_t, uint32_t>> out;
+  for (size_t k = 0; k < kv.size();) {
+    size_t m = k; uint8_t o = 0;
+    for (; m < kv.size() && kv[m].first == kv[k].first; m++) o |= kv[m].second;
+    if (o == 1) out.push_back({(uint32_t)(kv[k].first >> 32), (uint32_t)kv[k].first});
+    k = m;
+  }
+  return emit(out, out_pairs);
+}
+
+}  // extern "C"

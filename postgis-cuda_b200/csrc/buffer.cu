@@ -364,8 +364,6 @@ struct PairsOut {
   }
 };
 
-gsj_join_opts opts_or_default(const gsj_join_opts* o);
-uint64_t candidates_for(gsj_ctx* c, const float4* qbb, const uint32_t* qorder, uint32_t q0, uint32_t nq, const DBvh& T, int upper, uint2** out);
 
 void dwithin_host(gsj_ctx* c, const gsj_layer* P, const gsj_layer* R, double d, int same, const gsj_join_opts* op, gsj_pairs_sink sink, void* user,
                   gsj_join_stats* stp) {
@@ -433,15 +431,645 @@ void dwithin_host(gsj_ctx* c, const gsj_layer* P, const gsj_layer* R, double d, 
   if (stp) *stp = st;
 }
 
-void erode_host(gsj_ctx*, const gsj_layer*, const gsj_layer*, double, double, int, const uint8_t*, const gsj_join_opts*, gsj_pairs_sink, void*,
-                gsj_join_stats*) {
-  throw Error(GSJ_ERR_ARG, "erode: not built yet");
+// ---- negative-buffer intersects: warp per parent pair (buffer.cuh:275-889) ------------------------------------------
+// An element list per side: the eroded boundary lies on the edges offset inward by r and the GEOS-style chord fillets
+// at reflex vertices; X_A and X_B meet iff elements cross outside both exclusion zones, or a vertex of one eroded
+// boundary lies inside the other eroded polygon. Tested in W = shrink(bbox A, ra) x shrink(bbox B, rb).
+struct BEd { double x0, y0, x1, y1, ux, uy, L, ci, si; int succ, vt; };   // real edge in frame meters + end-vertex region
+struct BEl { double x0, y0, x1, y1; };                                  // element of the raw offset curve
+constexpr double FILLET_QUANTUM = 3.14159265358979323846 / 16.0;       // 8 segments per quarter circle (GEOS default)
+constexpr int ER_WARPS = 2, ER_CAPE = 64, ER_CAPL = 128, ER_MAX_DEPTH = 12;
+constexpr size_t ER_SMEM_WARP = 2 * ER_CAPE * sizeof(BEd) + 2 * ER_CAPL * sizeof(BEl);
+constexpr size_t ER_SMEM = (size_t)ER_WARPS * ER_SMEM_WARP;
+struct ErScratch { BEd* EA; BEd* EB; BEl* LA; BEl* LB; int capE, capL; };
+struct ETile { uint32_t pair, depth; double4 box; };
+struct ErCtr { unsigned int ntile, nslab; int needE, needL; };
+struct EFrame { double ox, oy, kx, ky; };
+
+__device__ bool in_excl(const BEd* E, int n, double r, double x, double y, double eps) {   // buffer.cuh:285-319
+  if (r <= 0) return false;
+  const double ri = r - eps;
+  for (int k = 0; k < n; k++) {
+    const BEd& e = E[k];
+    if (x < fmin(e.x0, e.x1) - r || x > fmax(e.x0, e.x1) + r || y < fmin(e.y0, e.y1) - r || y > fmax(e.y0, e.y1) + r) continue;
+    const double dx = x - e.x0, dy = y - e.y0;
+    const double t = dx * e.ux + dy * e.uy, s = dy * e.ux - dx * e.uy;   // s > 0: interior side
+    if (fabs(s) < ri && t > -eps && t < e.L + eps) return true;
+    if (e.vt == 0) continue;
+    const double vx = x - e.x1, vy = y - e.y1, d2 = vx * vx + vy * vy;
+    if (d2 >= r * r) continue;
+    const BEd& f = E[e.succ];
+    if (e.vt == 1) {
+      const double s2 = vy * f.ux - vx * f.uy;
+      if (d2 < ri * ri && !(s > eps && s2 > eps)) return true;
+      continue;
+    }
+    const double nkx = -e.uy, nky = e.ux, nsx = -f.uy, nsy = f.ux;
+    if (nkx * vy - nky * vx > eps) continue;
+    if (nsx * vy - nsy * vx < -eps) continue;
+    const double chh = sqrt(0.5 * (1.0 + e.ci)), shh = sqrt(fmax(0.0, 0.5 * (1.0 - e.ci)));
+    const double ch = r * chh - eps;
+    if (d2 < ch * ch) return true;
+    double mx = nkx * chh + nky * shh, my = -nkx * shh + nky * chh;
+    bool in = true;
+    for (int i = 0, m = e.vt - 1; i < m && in; i++) {
+      if (mx * vx + my * vy >= ch) in = false;
+      const double t2 = mx * e.ci + my * e.si; my = -mx * e.si + my * e.ci; mx = t2;
+    }
+    if (in) return true;
+  }
+  return false;
+}
+__device__ __forceinline__ bool inside_m(const BEd* E, int n, double cx, double cy, bool in_c, double x, double y) {   // buffer.cuh:322-334
+  bool in = in_c;
+  const double sx0 = fmin(cx, x), sx1 = fmax(cx, x), sy0 = fmin(cy, y), sy1 = fmax(cy, y);
+  for (int k = 0; k < n; k++) {
+    const BEd& e = E[k];
+    if (fmax(e.x0, e.x1) < sx0 || fmin(e.x0, e.x1) > sx1 || fmax(e.y0, e.y1) < sy0 || fmin(e.y0, e.y1) > sy1) continue;
+    const bool sc = left_of(e.x0, e.y0, e.x1, e.y1, cx, cy), sx = left_of(e.x0, e.y0, e.x1, e.y1, x, y);
+    if (sc == sx) continue;
+    const bool su = orient(cx, cy, x, y, e.x0, e.y0) > 0, sv = orient(cx, cy, x, y, e.x1, e.y1) > 0;
+    if (su != sv) in = !in;
+  }
+  return in;
+}
+__device__ __forceinline__ void fv(const DLayer& S, double shx, double shy, uint64_t v, const EFrame& F, double& x, double& y) {
+  const double2 q = S.xy[v];
+  x = (shx + q.x) * F.kx; y = (shy + q.y) * F.ky;
+}
+// c inside the parent: the piece whose box holds c decides by crossing parity (buffer.cuh:359-381)
+__device__ bool pip_parent(const DLayer& S, uint32_t g0, uint32_t g1, const EFrame& F, double cx, double cy, int lane) {
+  bool in = false;
+  for (uint32_t g = g0; g < g1 && !in; g++) {
+    const double2 o = S.origin[g], e = S.ext[g];
+    const double bx0 = (o.x - F.ox) * F.kx, by0 = (o.y - F.oy) * F.ky, bx1 = (o.x + e.x - F.ox) * F.kx, by1 = (o.y + e.y - F.oy) * F.ky;
+    if (cx < bx0 - 1e-6 || cx > bx1 + 1e-6 || cy < by0 - 1e-6 || cy > by1 + 1e-6) continue;
+    const double shx = o.x - F.ox, shy = o.y - F.oy, ox = bx0 - 1.0;
+    bool par = false;
+    for (uint32_t r = S.gro[g]; r < S.gro[g + 1]; r++) {
+      const uint64_t s0 = S.rvo[r], ee = S.rvo[r + 1];
+      for (uint64_t j = s0 + 1 + lane; j < ee; j += 32) {
+        double x0, y0, x1, y1; fv(S, shx, shy, j - 1, F, x0, y0); fv(S, shx, shy, j, F, x1, y1);
+        if ((y0 > cy) == (y1 > cy) && y0 != cy && y1 != cy) continue;
+        const bool so = left_of(x0, y0, x1, y1, ox, cy), sc = left_of(x0, y0, x1, y1, cx, cy);
+        if (so == sc) continue;
+        const bool su = orient(ox, cy, cx, cy, x0, y0) > 0, sv = orient(ox, cy, cx, cy, x1, y1) > 0;
+        if (su != sv) par = !par;
+      }
+    }
+    in = (__popc(__ballot_sync(0xffffffffu, par)) & 1) != 0;
+  }
+  return in;
+}
+// the parent's real, non-degenerate edges meeting box C, in piece / ring / edge order (buffer.cuh:384-408)
+__device__ int collect_side(const DLayer& S, uint32_t g0, uint32_t g1, const EFrame& F, double cx0, double cy0, double cx1, double cy1, BEd* E, int cap,
+                            int lane) {
+  const unsigned lt = (1u << lane) - 1;
+  int cnt = 0;
+  for (uint32_t g = g0; g < g1; g++) {
+    const double2 o = S.origin[g], ex = S.ext[g];
+    if ((o.x + ex.x - F.ox) * F.kx < cx0 || (o.x - F.ox) * F.kx > cx1 || (o.y + ex.y - F.oy) * F.ky < cy0 || (o.y - F.oy) * F.ky > cy1) continue;
+    const double shx = o.x - F.ox, shy = o.y - F.oy;
+    for (uint32_t r = S.gro[g]; r < S.gro[g + 1]; r++) {
+      const uint64_t s0 = S.rvo[r], e = S.rvo[r + 1];
+      for (uint64_t base = s0; base + 1 < e; base += 32) {
+        const uint64_t i = base + lane;
+        bool v = false; BEd ed;
+        if (i + 1 < e && !S.syn(i)) {
+          fv(S, shx, shy, i, F, ed.x0, ed.y0); fv(S, shx, shy, i + 1, F, ed.x1, ed.y1);
+          v = !(ed.x0 == ed.x1 && ed.y0 == ed.y1) &&
+              !(fmax(ed.x0, ed.x1) < cx0 || fmin(ed.x0, ed.x1) > cx1 || fmax(ed.y0, ed.y1) < cy0 || fmin(ed.y0, ed.y1) > cy1);
+        }
+        const unsigned m = __ballot_sync(0xffffffffu, v);
+        const int pos = cnt + __popc(m & lt);
+        if (v && pos < cap) E[pos] = ed;
+        cnt += __popc(m);
+      }
+    }
+  }
+  return cnt;
+}
+// unit directions, successor edge and end-vertex region (convex disk / reflex fillet) (buffer.cuh:411-439)
+__device__ void prepare_side(BEd* E, int n, double r, int lane) {
+  for (int k = lane; k < n; k += 32) {
+    const double dx = E[k].x1 - E[k].x0, dy = E[k].y1 - E[k].y0, L = sqrt(dx * dx + dy * dy);
+    E[k].ux = dx / L; E[k].uy = dy / L; E[k].L = L;
+  }
+  __syncwarp();
+  for (int k = lane; k < n; k += 32) {
+    const double ex1 = E[k].x1, ey1 = E[k].y1, eux = E[k].ux, euy = E[k].uy;
+    int s = -1;
+    if (k + 1 < n && E[k + 1].x0 == ex1 && E[k + 1].y0 == ey1) s = k + 1;
+    else for (int j = 0; j < n; j++) if (j != k && E[j].x0 == ex1 && E[j].y0 == ey1) { s = j; break; }
+    int vt = 0; double ci = 1, si = 0;
+    if (s >= 0 && r > 0) {
+      const double fux = E[s].ux, fuy = E[s].uy;
+      const double cr = eux * fuy - euy * fux, dt = eux * fux + euy * fuy;
+      if (cr > 0) vt = 1;
+      else if (cr < 0 || dt < 0) {   // right turn or reversal: fillet
+        double th = atan2(-cr, dt);
+        if (cr == 0) th = 3.14159265358979323846;
+        int m = (int)(th / FILLET_QUANTUM + 0.5);
+        if (m < 1) m = 1;
+        const double inc = th / m; ci = cos(inc); si = sin(inc);
+        vt = m + 1;
+      }
+    }
+    E[k].succ = s; E[k].vt = vt; E[k].ci = ci; E[k].si = si;
+  }
+  __syncwarp();
+}
+// raw offset curve elements meeting W +- eps (buffer.cuh:442-472)
+__device__ int build_elements(const BEd* E, int n, double r, double wx0, double wy0, double wx1, double wy1, double eps, BEl* L, int cap, int lane) {
+  const unsigned lt = (1u << lane) - 1;
+  int cnt = 0;
+  for (int base = 0; base < n; base += 32) {
+    const int k = base + lane;
+    const bool valid = k < n;
+    BEd e; if (valid) e = E[k];
+    const int ne = valid ? 1 + (e.vt >= 2 ? e.vt - 1 : 0) : 0;
+    const int mx = __reduce_max_sync(0xffffffffu, ne);
+    double nkx = 0, nky = 0, wxr = 0, wyr = 0, px = 0, py = 0, nsx = 0, nsy = 0;
+    if (valid) {
+      nkx = -e.uy; nky = e.ux; wxr = nkx; wyr = nky; px = e.x1 + r * nkx; py = e.y1 + r * nky;
+      if (e.vt >= 2) { nsx = -E[e.succ].uy; nsy = E[e.succ].ux; }
+    }
+    for (int it = 0; it < mx; it++) {
+      bool has = it < ne; BEl el;
+      if (has) {
+        if (it == 0) { el.x0 = e.x0 + r * nkx; el.y0 = e.y0 + r * nky; el.x1 = e.x1 + r * nkx; el.y1 = e.y1 + r * nky; }
+        else {
+          const double t2 = wxr * e.ci + wyr * e.si; wyr = -wxr * e.si + wyr * e.ci; wxr = t2;
+          double qx, qy;
+          if (it == ne - 1) { qx = e.x1 + r * nsx; qy = e.y1 + r * nsy; } else { qx = e.x1 + r * wxr; qy = e.y1 + r * wyr; }
+          el.x0 = px; el.y0 = py; el.x1 = qx; el.y1 = qy; px = qx; py = qy;
+        }
+        has = !(fmax(el.x0, el.x1) < wx0 - eps || fmin(el.x0, el.x1) > wx1 + eps || fmax(el.y0, el.y1) < wy0 - eps || fmin(el.y0, el.y1) > wy1 + eps);
+      }
+      const unsigned m = __ballot_sync(0xffffffffu, has);
+      const int pos = cnt + __popc(m & lt);
+      if (has && pos < cap) L[pos] = el;
+      cnt += __popc(m);
+    }
+  }
+  return cnt;
+}
+__device__ int seg_points(const BEl& p, const BEl& q, double* xs, double* ys) {   // buffer.cuh:475-493
+  const double rx = p.x1 - p.x0, ry = p.y1 - p.y0, sx = q.x1 - q.x0, sy = q.y1 - q.y0;
+  const double den = rx * sy - ry * sx;
+  if (den != 0) {
+    double t = ((q.x0 - p.x0) * sy - (q.y0 - p.y0) * sx) / den;
+    t = fmin(1.0, fmax(0.0, t));
+    xs[0] = p.x0 + t * rx; ys[0] = p.y0 + t * ry;
+    return 1;
+  }
+  const double l2 = rx * rx + ry * ry;
+  if (l2 == 0) { xs[0] = p.x0; ys[0] = p.y0; return 1; }
+  const double t0 = ((q.x0 - p.x0) * rx + (q.y0 - p.y0) * ry) / l2, t1 = ((q.x1 - p.x0) * rx + (q.y1 - p.y0) * ry) / l2;
+  double lo = fmax(0.0, fmin(t0, t1)), hi = fmin(1.0, fmax(t0, t1));
+  if (lo > hi) { const double m = 0.5 * (lo + hi); lo = hi = fmin(1.0, fmax(0.0, m)); }
+  xs[0] = p.x0 + lo * rx; ys[0] = p.y0 + lo * ry;
+  xs[1] = p.x0 + hi * rx; ys[1] = p.y0 + hi * ry;
+  xs[2] = p.x0 + 0.5 * (lo + hi) * rx; ys[2] = p.y0 + 0.5 * (lo + hi) * ry;
+  return 3;
+}
+
+// X_A meets X_B within the window (intersected with tile when given): 1 / 0, or -1 when a list overflowed
+// (needE / needL = sizes required, *wout = the window tested) (buffer.cuh:499-588)
+__device__ int er_pair(const DLayer& P, const DLayer& R, uint2 ga, uint2 gb, double ra_nom, double rb_nom, const ErScratch& sc, int lane, int* needE,
+                       int* needL, const double4* tile, double4* wout) {
+  if (ga.x >= ga.y || gb.x >= gb.y) return 0;
+  double abx0 = 1e300, aby0 = 1e300, abx1 = -1e300, aby1 = -1e300, bbx0 = 1e300, bby0 = 1e300, bbx1 = -1e300, bby1 = -1e300;
+  for (uint32_t g = ga.x; g < ga.y; g++) {
+    const double2 o = P.origin[g], e = P.ext[g];
+    abx0 = fmin(abx0, o.x); aby0 = fmin(aby0, o.y); abx1 = fmax(abx1, o.x + e.x); aby1 = fmax(aby1, o.y + e.y);
+  }
+  for (uint32_t g = gb.x; g < gb.y; g++) {
+    const double2 o = R.origin[g], e = R.ext[g];
+    bbx0 = fmin(bbx0, o.x); bby0 = fmin(bby0, o.y); bbx1 = fmax(bbx1, o.x + e.x); bby1 = fmax(bby1, o.y + e.y);
+  }
+  double dax, day, dbx, dby;
+  deg_cover(aby0, aby1, ra_nom * 0.998, false, dax, day);   // shrink by a lower bound of the true radius
+  deg_cover(bby0, bby1, rb_nom * 0.998, false, dbx, dby);
+  double wx0 = fmax(abx0 + dax, bbx0 + dbx), wx1 = fmin(abx1 - dax, bbx1 - dbx);
+  double wy0 = fmax(aby0 + day, bby0 + dby), wy1 = fmin(aby1 - day, bby1 - dby);
+  if (tile) { wx0 = fmax(wx0, tile->x); wy0 = fmax(wy0, tile->y); wx1 = fmin(wx1, tile->z); wy1 = fmin(wy1, tile->w); }
+  if (wx0 > wx1 || wy0 > wy1) return 0;
+  if (wout) *wout = make_double4(wx0, wy0, wx1, wy1);
+  const double clon = 0.5 * (wx0 + wx1), clat = 0.5 * (wy0 + wy1);
+  const double rA = ra_nom > 0 ? ra_nom / utm_k(0.5 * (abx0 + abx1), 0.5 * (aby0 + aby1), clon, clat) : 0.0;
+  const double rB = rb_nom > 0 ? rb_nom / utm_k(0.5 * (bbx0 + bbx1), 0.5 * (bby0 + bby1), clon, clat) : 0.0;
+  EFrame F; { const double2 o = P.origin[ga.x]; F.ox = o.x; F.oy = o.y; } m_per_deg(clat, F.kx, F.ky);
+  const double Wx0 = (wx0 - F.ox) * F.kx, Wx1 = (wx1 - F.ox) * F.kx, Wy0 = (wy0 - F.oy) * F.ky, Wy1 = (wy1 - F.oy) * F.ky;
+  const double ext = fmax(fmax(fabs(Wx0), fabs(Wx1)), fmax(fabs(Wy0), fabs(Wy1))) + fmax(rA, rB);
+  const double eps = 1e-9 + 1e-12 * ext;
+  const double fe = 1.0 + 2.0 * 0.5 * (wy1 - wy0) * DEG * (fabs(tan(clat * DEG)) + 0.05);
+  const double ma = rA * fe + 1e-6, mb = rB * fe + 1e-6;
+  const int na = collect_side(P, ga.x, ga.y, F, Wx0 - ma, Wy0 - ma, Wx1 + ma, Wy1 + ma, sc.EA, sc.capE, lane);
+  const int nb = collect_side(R, gb.x, gb.y, F, Wx0 - mb, Wy0 - mb, Wx1 + mb, Wy1 + mb, sc.EB, sc.capE, lane);
+  if (na > sc.capE || nb > sc.capE) { if (needE) *needE = max(na, nb); return -1; }
+  __syncwarp();
+  prepare_side(sc.EA, na, rA, lane);
+  prepare_side(sc.EB, nb, rB, lane);
+  const int la = build_elements(sc.EA, na, rA, Wx0, Wy0, Wx1, Wy1, eps, sc.LA, sc.capL, lane);
+  const int lb = build_elements(sc.EB, nb, rB, Wx0, Wy0, Wx1, Wy1, eps, sc.LB, sc.capL, lane);
+  if (la > sc.capL || lb > sc.capL) { if (needE) *needE = max(na, nb); if (needL) *needL = max(la, lb); return -1; }
+  __syncwarp();
+  const BEd* EA = sc.EA; const BEd* EB = sc.EB; const BEl* LA = sc.LA; const BEl* LB = sc.LB;
+  auto inW = [&](double x, double y) { return x >= Wx0 - eps && x <= Wx1 + eps && y >= Wy0 - eps && y <= Wy1 + eps; };
+  // (a) the eroded boundaries cross outside both exclusion zones
+  bool hit = false;
+  for (int i = lane; i < la && !hit; i += 32) {
+    const BEl p = LA[i];
+    const double px0 = fmin(p.x0, p.x1), px1 = fmax(p.x0, p.x1), py0 = fmin(p.y0, p.y1), py1 = fmax(p.y0, p.y1);
+    for (int j = 0; j < lb && !hit; j++) {
+      const BEl q = LB[j];
+      if (fmax(q.x0, q.x1) < px0 || fmin(q.x0, q.x1) > px1 || fmax(q.y0, q.y1) < py0 || fmin(q.y0, q.y1) > py1) continue;
+      if (!seg_isect(p.x0, p.y0, p.x1, p.y1, q.x0, q.y0, q.x1, q.y1)) continue;
+      double xs[3], ys[3]; const int k = seg_points(p, q, xs, ys);
+      for (int t = 0; t < k && !hit; t++)
+        if (inW(xs[t], ys[t]) && !in_excl(EA, na, rA, xs[t], ys[t], eps) && !in_excl(EB, nb, rB, xs[t], ys[t], eps)) hit = true;
+    }
+  }
+  if (__any_sync(0xffffffffu, hit)) return 1;
+  // (b), (c) a vertex of one eroded boundary inside the other eroded polygon
+  const double cx = Wx0 + 0.381966 * (Wx1 - Wx0), cy = Wy0 + 0.414213 * (Wy1 - Wy0);
+  const bool inA_c = pip_parent(P, ga.x, ga.y, F, cx, cy, lane);
+  const bool inB_c = pip_parent(R, gb.x, gb.y, F, cx, cy, lane);
+  for (int side = 0; side < 2; side++) {
+    const BEd* ES = side ? EB : EA; const BEd* EO = side ? EA : EB;
+    const BEl* LS = side ? LB : LA;
+    const int ns = side ? nb : na, no = side ? na : nb, ls = side ? lb : la;
+    const double rs = side ? rB : rA, ro = side ? rA : rB;
+    const bool inO_c = side ? inA_c : inB_c;
+    auto vio = [&](double x, double y) {
+      return inW(x, y) && !in_excl(ES, ns, rs, x, y, eps) && inside_m(EO, no, cx, cy, inO_c, x, y) && !in_excl(EO, no, ro, x, y, eps);
+    };
+    for (int i = lane; i < ls && !hit; i += 32) {
+      const BEl p = LS[i];
+      if (vio(p.x0, p.y0) || vio(p.x1, p.y1)) { hit = true; break; }
+      const double px0 = fmin(p.x0, p.x1), px1 = fmax(p.x0, p.x1), py0 = fmin(p.y0, p.y1), py1 = fmax(p.y0, p.y1);
+      for (int j = i + 1; j < ls && !hit; j++) {
+        const BEl q = LS[j];
+        if (fmax(q.x0, q.x1) < px0 || fmin(q.x0, q.x1) > px1 || fmax(q.y0, q.y1) < py0 || fmin(q.y0, q.y1) > py1) continue;
+        if (!seg_isect(p.x0, p.y0, p.x1, p.y1, q.x0, q.y0, q.x1, q.y1)) continue;
+        double xs[3], ys[3]; const int k = seg_points(p, q, xs, ys);
+        for (int t = 0; t < k && !hit; t++) if (vio(xs[t], ys[t])) hit = true;
+      }
+    }
+    if (__any_sync(0xffffffffu, hit)) return 1;
+  }
+  return 0;
+}
+
+__device__ __forceinline__ uint2 piece_range(const uint32_t* pf, uint32_t p) { return pf ? make_uint2(pf[p], pf[p + 1]) : make_uint2(p, p + 1); }
+__device__ __forceinline__ ErScratch er_smem(unsigned char* raw, int wib) {
+  unsigned char* base = raw + (size_t)wib * ER_SMEM_WARP;
+  ErScratch sc;
+  sc.EA = reinterpret_cast<BEd*>(base); sc.EB = sc.EA + ER_CAPE;
+  sc.LA = reinterpret_cast<BEl*>(sc.EB + ER_CAPE); sc.LB = sc.LA + ER_CAPL;
+  sc.capE = ER_CAPE; sc.capL = ER_CAPL;
+  return sc;
+}
+// pf[q] = first piece whose parent is >= q, q in [0, np] (parents non-decreasing)
+__global__ void k_piece_first(const uint32_t* __restrict__ parent, uint32_t n, uint32_t np, uint32_t* pf) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const uint32_t p = parent[i], lo = i ? parent[i - 1] + 1 : 0;
+  for (uint32_t q = lo; q <= p; q++) pf[q] = i;
+  if (i == n - 1) for (uint32_t q = p + 1; q <= np; q++) pf[q] = n;
+}
+// candidate piece pairs that cannot meet after erosion: both whole geometries with disjoint shrunk bboxes
+__global__ void k_er_prefilter(DLayer P, DLayer R, const uint2* __restrict__ pairs, uint64_t n, double ra, double rb, uint32_t* keep) {
+  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const uint2 p = pairs[i];
+  auto whole = [](const DLayer& S, uint32_t g) {
+    if (!S.parent) return true;
+    const uint32_t q = S.parent[g];
+    return (g == 0 || S.parent[g - 1] != q) && (g + 1 >= S.n || S.parent[g + 1] != q);
+  };
+  bool k = true;
+  if (whole(P, p.x) && whole(R, p.y)) {
+    const double2 oa = P.origin[p.x], ea = P.ext[p.x], ob = R.origin[p.y], eb = R.ext[p.y];
+    double dax, day, dbx, dby;
+    deg_cover(oa.y, oa.y + ea.y, ra * 0.998, false, dax, day);
+    deg_cover(ob.y, ob.y + eb.y, rb * 0.998, false, dbx, dby);
+    const double wx0 = fmax(oa.x + dax, ob.x + dbx), wx1 = fmin(oa.x + ea.x - dax, ob.x + eb.x - dbx);
+    const double wy0 = fmax(oa.y + day, ob.y + dby), wy1 = fmin(oa.y + ea.y - day, ob.y + eb.y - dby);
+    k = wx0 <= wx1 && wy0 <= wy1;
+  }
+  keep[i] = k;
+}
+__global__ void k_compact_pairs(const uint2* __restrict__ in, const uint32_t* __restrict__ keep, const uint32_t* __restrict__ off, uint64_t n, uint2* out) {
+  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n && keep[i]) out[off[i]] = in[i];
+}
+// erosion input: intersecting parent pairs whose overlap area can hold a disk of radius rmin (buffer.cuh:720-738)
+__global__ void k_er_filter(const uint2* __restrict__ pr, const double* __restrict__ area, uint64_t n, DLayer P, const uint32_t* pfP, double rmin,
+                            int same, const uint8_t* need_self, uint32_t* keep) {
+  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const uint2 p = pr[i];
+  bool k = true;
+  if (same && p.x == p.y && need_self) k = need_self[p.x] != 0;
+  if (k && rmin >= 0) {
+    const uint32_t g = pfP ? pfP[p.x] : p.x;
+    const double y0 = P.origin[g].y, y1 = y0 + P.ext[g].y;
+    const double lat = (y0 <= 0 && y1 >= 0) ? 0.0 : (fabs(y0) < fabs(y1) ? y0 : y1);
+    double kx, ky; m_per_deg(lat, kx, ky);
+    const double a_m2 = area[i] * kx * ky * 1.001;
+    const double r = 0.98 * rmin;
+    k = rmin > 0 ? a_m2 >= 3.14159265358979323846 * r * r : area[i] > 0;
+  }
+  keep[i] = k;
+}
+__global__ void __launch_bounds__(ER_WARPS * 32) k_erode_main(DLayer P, DLayer R, const uint32_t* pfP, const uint32_t* pfR, const uint2* __restrict__ pairs,
+                                                              uint64_t np, double ra, double rb, uint8_t* flag, uint32_t* heavy, unsigned int* nheavy) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int lane = threadIdx.x & 31;
+  const ErScratch sc = er_smem(smem, threadIdx.x >> 5);
+  const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  for (uint64_t p = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; p < np; p += nw) {
+    const int r = er_pair(P, R, piece_range(pfP, pairs[p].x), piece_range(pfR, pairs[p].y), ra, rb, sc, lane, nullptr, nullptr, nullptr, nullptr);
+    if (lane == 0) { flag[p] = r > 0 ? 1 : 0; if (r < 0) heavy[atomicAdd(nheavy, 1u)] = (uint32_t)p; }
+    __syncwarp();
+  }
+}
+__global__ void k_tiles_init(const uint32_t* __restrict__ heavy, uint64_t n, ETile* items) {
+  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) items[i] = ETile{heavy[i], 0, make_double4(-INFINITY, -INFINITY, INFINITY, INFINITY)};
+}
+// split an overflowing tile into quadrants while it is larger than the radius, else send it to the slab pass
+__device__ void er_overflow(uint32_t p, uint32_t depth, double4 w, double rmax, int ne, int nl, ETile* next, ETile* slab, ErCtr* c) {
+  double kx, ky; m_per_deg(0.5 * (w.y + w.w), kx, ky);
+  const double ext = fmax((w.z - w.x) * kx, (w.w - w.y) * ky);
+  if (depth < ER_MAX_DEPTH && ext > rmax) {
+    const double xm = 0.5 * (w.x + w.z), ym = 0.5 * (w.y + w.w);
+    const unsigned k = atomicAdd(&c->ntile, 4u);
+    next[k] = ETile{p, depth + 1, make_double4(w.x, w.y, xm, ym)};
+    next[k + 1] = ETile{p, depth + 1, make_double4(xm, w.y, w.z, ym)};
+    next[k + 2] = ETile{p, depth + 1, make_double4(w.x, ym, xm, w.w)};
+    next[k + 3] = ETile{p, depth + 1, make_double4(xm, ym, w.z, w.w)};
+  } else {
+    slab[atomicAdd(&c->nslab, 1u)] = ETile{p, depth, w};
+    atomicMax(&c->needE, ne); atomicMax(&c->needL, nl);
+  }
+}
+__global__ void __launch_bounds__(ER_WARPS * 32) k_erode_tiles(DLayer P, DLayer R, const uint32_t* pfP, const uint32_t* pfR, const uint2* __restrict__ pairs,
+                                                               const ETile* items, uint64_t ni, double ra, double rb, uint8_t* flag, ETile* next, ETile* slab,
+                                                               ErCtr* c) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int lane = threadIdx.x & 31;
+  const ErScratch sc = er_smem(smem, threadIdx.x >> 5);
+  const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  for (uint64_t i = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < ni; i += nw) {
+    ETile t = items[i];
+    if (flag[t.pair]) continue;   // another tile already found an intersection
+    int ne = 0, nl = 0; double4 win = t.box;
+    const int r = er_pair(P, R, piece_range(pfP, pairs[t.pair].x), piece_range(pfR, pairs[t.pair].y), ra, rb, sc, lane, &ne, &nl, &t.box, &win);
+    if (lane == 0) {
+      if (r > 0) flag[t.pair] = 1;
+      else if (r < 0) er_overflow(t.pair, t.depth, win, fmax(ra, rb), ne, nl, next, slab, c);
+    }
+    __syncwarp();
+  }
+}
+// tiles that cannot usefully be split: per-warp lists in global scratch sized by the reported need
+__global__ void k_erode_slab(DLayer P, DLayer R, const uint32_t* pfP, const uint32_t* pfR, const uint2* __restrict__ pairs, const ETile* items, uint64_t ni,
+                             double ra, double rb, uint8_t* flag, unsigned char* scratch, int capE, int capL, ETile* again, ErCtr* c) {
+  const int lane = threadIdx.x & 31;
+  const uint64_t w = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  unsigned char* base = scratch + w * (2 * (size_t)capE * sizeof(BEd) + 2 * (size_t)capL * sizeof(BEl));
+  ErScratch sc;
+  sc.EA = reinterpret_cast<BEd*>(base); sc.EB = sc.EA + capE;
+  sc.LA = reinterpret_cast<BEl*>(sc.EB + capE); sc.LB = sc.LA + capL;
+  sc.capE = capE; sc.capL = capL;
+  for (uint64_t i = w; i < ni; i += nw) {
+    ETile t = items[i];
+    if (flag[t.pair]) continue;
+    int ne = 0, nl = 0;
+    const int r = er_pair(P, R, piece_range(pfP, pairs[t.pair].x), piece_range(pfR, pairs[t.pair].y), ra, rb, sc, lane, &ne, &nl, &t.box, nullptr);
+    if (lane == 0) {
+      if (r > 0) flag[t.pair] = 1;
+      else if (r < 0) { again[atomicAdd(&c->nslab, 1u)] = t; atomicMax(&c->needE, ne); atomicMax(&c->needL, nl); }
+    }
+    __syncwarp();
+  }
+}
+
+static const uint32_t* piece_first_dev(gsj_ctx* c, const gsj_layer* S, DevBuf& buf) {
+  if (!S->d.parent) return nullptr;
+  uint32_t* pf = buf.as<uint32_t>((size_t)S->nparent + 1);
+  k_piece_first<<<grid_for(S->d.n, 256), 256, 0, c->stream>>>(S->d.parent, S->d.n, S->nparent, pf); c->launches++;
+  GSJ_CK(cudaGetLastError());
+  return pf;
+}
+
+void erode_host(gsj_ctx* c, const gsj_layer* P, const gsj_layer* R, double ra, double rb, int same, const uint8_t* need_self_h, const gsj_join_opts* op,
+                gsj_pairs_sink sink, void* user, gsj_join_stats* stp) {
+  if (P->is_points || R->is_points) throw Error(GSJ_ERR_ARG, "gsj_erode joins two polygon layers (points: gsj_points_erode)");
+  if (same && P != R) throw Error(GSJ_ERR_ARG, "same = 1 needs P == R");
+  gsj_join_opts o = opts_or_default(op);
+  gsj_join_stats st{};
+  const uint64_t l0 = c->launches;
+  cudaStream_t s = c->stream;
+  DevBuf pfPb, pfRb, nsb;
+  const uint32_t* pfP = piece_first_dev(c, P, pfPb);
+  const uint32_t* pfR = piece_first_dev(c, R, pfRb);
+  const uint8_t* need_self = nullptr;
+  if (same && need_self_h) {
+    uint8_t* d = nsb.as<uint8_t>(P->nparent);
+    GSJ_CK(cudaMemcpyAsync(d, need_self_h, P->nparent, cudaMemcpyHostToDevice, s));
+    need_self = d;
+  }
+  if (!c->er_attr) {
+    GSJ_CK(cudaFuncSetAttribute(k_erode_main, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ER_SMEM));
+    GSJ_CK(cudaFuncSetAttribute(k_erode_tiles, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ER_SMEM));
+    c->er_attr = 1;
+  }
+  const double rmin = (ra > 0 && rb > 0) ? std::min(ra, rb) : (ra > 0 || rb > 0 ? 0.0 : -1.0);
+  RefineArgs rp{1e-12, 1e-7, 1e-11, 1, 0, 0};
+  PairsOut emit{c, sink, user, &st};
+  PrefilterFn pre;
+  if (ra > 0 || rb > 0)
+    pre = [&](uint2* pairs, uint64_t n) -> uint64_t {
+      uint32_t* keep = c->er_keep.as<uint32_t>(n);
+      uint32_t* off = c->er_off.as<uint32_t>(n);
+      k_er_prefilter<<<grid_for(n, 256), 256, 0, s>>>(P->d, R->d, pairs, n, ra, rb, keep); c->launches++;
+      const uint64_t k = scan_count(c, keep, off, n);
+      uint2* tmp = c->er_tmp.as<uint2>(k);
+      k_compact_pairs<<<grid_for(n, 256), 256, 0, s>>>(pairs, keep, off, n, tmp); c->launches++;
+      GSJ_CK(cudaMemcpyAsync(pairs, tmp, k * sizeof(uint2), cudaMemcpyDeviceToDevice, s));
+      GSJ_CK(cudaGetLastError());
+      return k;
+    };
+  Timer tm(s);
+  DeviceBatchFn pass2 = [&](const uint2* dp, const double* da, uint64_t n) {
+    tm.start();
+    uint32_t* keep = c->er_keep.as<uint32_t>(n);
+    uint32_t* off = c->er_off.as<uint32_t>(n);
+    k_er_filter<<<grid_for(n, 256), 256, 0, s>>>(dp, da, n, P->d, pfP, rmin, same, need_self, keep); c->launches++;
+    const uint64_t ne = scan_count(c, keep, off, n);
+    if (!ne) { st.compact_ms += tm.stop(); return; }
+    uint2* ep = c->er_pairs.as<uint2>(ne);
+    k_compact_pairs<<<grid_for(n, 256), 256, 0, s>>>(dp, keep, off, n, ep); c->launches++;
+    uint8_t* flag = c->er_flag.as<uint8_t>(ne);
+    uint32_t* heavy = c->er_heavy.as<uint32_t>(ne);
+    ErCtr* ctr = c->er_ctr.as<ErCtr>(2);
+    GSJ_CK(cudaMemsetAsync(ctr, 0, sizeof(ErCtr), s));
+    const int G = (int)std::min<uint64_t>((ne * 32 + 63) / 64, (uint64_t)c->sm_count * 32);
+    k_erode_main<<<G, ER_WARPS * 32, ER_SMEM, s>>>(P->d, R->d, pfP, pfR, ep, ne, ra, rb, flag, heavy, &ctr->ntile); c->launches++;
+    GSJ_CK(cudaGetLastError());
+    ErCtr h{};
+    GSJ_CK(cudaMemcpyAsync(&h, ctr, sizeof(ErCtr), cudaMemcpyDeviceToHost, s));
+    GSJ_CK(cudaStreamSynchronize(s));
+    const uint64_t nh = h.ntile;
+    st.heavy += nh;
+    if (nh) {   // overflowing pairs: quadrant tiles of their windows until the lists fit, then slabs
+      uint64_t ni = nh;
+      ETile* items = c->er_tiles.as<ETile>(ni);
+      k_tiles_init<<<grid_for(ni, 256), 256, 0, s>>>(heavy, ni, items); c->launches++;
+      for (int round = 0; ni; round++) {
+        if (round > 4 * ER_MAX_DEPTH) throw Error(GSJ_ERR_CUDA, "erosion tiling did not converge");
+        ETile* next = c->er_tiles2.as<ETile>(ni * 4);
+        ETile* slab = c->er_slab.as<ETile>(ni);
+        GSJ_CK(cudaMemsetAsync(ctr, 0, sizeof(ErCtr), s));
+        const int GT = (int)std::min<uint64_t>((ni * 32 + 63) / 64, (uint64_t)c->sm_count * 32);
+        k_erode_tiles<<<GT, ER_WARPS * 32, ER_SMEM, s>>>(P->d, R->d, pfP, pfR, ep, items, ni, ra, rb, flag, next, slab, ctr); c->launches++;
+        GSJ_CK(cudaGetLastError());
+        ErCtr hc{};
+        GSJ_CK(cudaMemcpyAsync(&hc, ctr, sizeof(ErCtr), cudaMemcpyDeviceToHost, s));
+        GSJ_CK(cudaStreamSynchronize(s));
+        uint64_t ns = hc.nslab;
+        for (int sround = 0; ns; sround++) {
+          if (sround >= 4) throw Error(GSJ_ERR_CUDA, "erosion slab tiles still overflow after 4 rounds");
+          const int capE = std::max<int>(hc.needE, ER_CAPE), capL = std::max<int>(std::max<int>(hc.needL, 17 * capE / 4), ER_CAPL);
+          const size_t per = 2 * (size_t)capE * sizeof(BEd) + 2 * (size_t)capL * sizeof(BEl);
+          uint64_t nwarps = std::max<uint64_t>(1, std::min<uint64_t>(ns, (1ull << 30) / per));
+          nwarps = (nwarps + 3) / 4 * 4;
+          unsigned char* scr = c->er_scr.as<unsigned char>(per * nwarps);
+          // ping-pong between er_again and er_tiles (this round's tiles are consumed by now)
+          ETile* again = (sround % 2 ? c->er_tiles : c->er_again).as<ETile>(ns);
+          GSJ_CK(cudaMemsetAsync(ctr, 0, sizeof(ErCtr), s));
+          k_erode_slab<<<(int)(nwarps / 4), 128, 0, s>>>(P->d, R->d, pfP, pfR, ep, slab, ns, ra, rb, flag, scr, capE, capL, again, ctr); c->launches++;
+          GSJ_CK(cudaGetLastError());
+          ErCtr h2{};
+          GSJ_CK(cudaMemcpyAsync(&h2, ctr, sizeof(ErCtr), cudaMemcpyDeviceToHost, s));
+          GSJ_CK(cudaStreamSynchronize(s));
+          slab = again; ns = h2.nslab; hc.needE = h2.needE; hc.needL = h2.needL;
+        }
+        std::swap(c->er_tiles.p, c->er_tiles2.p); std::swap(c->er_tiles.cap, c->er_tiles2.cap);
+        items = reinterpret_cast<ETile*>(c->er_tiles.p);
+        ni = hc.ntile;
+      }
+    }
+    st.refine_ms += tm.stop();
+    tm.start();
+    uint2* out = nullptr;
+    const uint64_t nu = fold_unique(c, ep, flag, ne, 1, nullptr, nullptr, &out);
+    st.compact_ms += tm.stop();
+    emit(out, nu);
+  };
+  join_device(c, P, R, rp, o, st, pre, pass2);
+  st.launches = c->launches - l0;
+  if (stp) *stp = st;
+}
+
+// ---- points in eroded polygons: thread per (point, piece) (k_pt_erode, buffer.cuh:1059-1132) ------------------------
+__device__ bool vertex_excl(double ex, double ey, double fx, double fy, double r, double wx, double wy, double eps) {
+  const double d2 = wx * wx + wy * wy;
+  if (d2 >= r * r) return false;
+  const double cr = ex * fy - ey * fx, dt = ex * fx + ey * fy;
+  if (cr > 0) {
+    const double ri = r - eps, s1 = wy * ex - wx * ey, s2 = wy * fx - wx * fy;
+    return d2 < ri * ri && !(s1 > eps && s2 > eps);
+  }
+  if (cr == 0 && dt >= 0) return false;
+  const double th = cr == 0 ? 3.14159265358979323846 : atan2(-cr, dt);
+  int m = (int)(th / FILLET_QUANTUM + 0.5);
+  if (m < 1) m = 1;
+  const double inc = th / m, ci = cos(inc), si = sin(inc);
+  const double nkx = -ey, nky = ex, nsx = -fy, nsy = fx;
+  if (nkx * wy - nky * wx > eps || nsx * wy - nsy * wx < -eps) return false;
+  const double chh = sqrt(0.5 * (1.0 + ci)), shh = sqrt(fmax(0.0, 0.5 * (1.0 - ci)));
+  const double ch = r * chh - eps;
+  if (d2 < ch * ch) return true;
+  double mx = nkx * chh + nky * shh, my = -nkx * shh + nky * chh;
+  for (int i = 0; i < m; i++) {
+    if (mx * wx + my * wy >= ch) return false;
+    const double t2 = mx * ci + my * si; my = -mx * si + my * ci; mx = t2;
+  }
+  return true;
+}
+// bit 1 = inside the piece, bit 2 = within r of its real boundary (OR-ed per (point, parent); kept iff == 1)
+__global__ void k_pt_erode(const double2* __restrict__ pts, DLayer R, const uint2* __restrict__ pairs, uint64_t np, double r_nom, uint8_t* bits) {
+  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= np) return;
+  const uint2 pr = pairs[i];
+  const uint32_t g = pr.y;
+  const double2 pt = pts[pr.x], o = R.origin[g], ext = R.ext[g];
+  const double r = r_nom / utm_k(o.x + 0.5 * ext.x, o.y + 0.5 * ext.y, pt.x, pt.y);
+  double kx, ky; m_per_deg(pt.y, kx, ky);
+  const double eps = 1e-9;
+  const double shx = o.x - pt.x, shy = o.y - pt.y, ox = shx * kx - 1.0;   // frame: meters relative to the point
+  auto vx = [&](uint64_t j, double& x, double& y) { const double2 q = R.xy[j]; x = (shx + q.x) * kx; y = (shy + q.y) * ky; };
+  bool par = false, ex = false;
+  for (uint32_t rr = R.gro[g]; rr < R.gro[g + 1] && !ex; rr++) {
+    const uint64_t s0 = R.rvo[rr], e = R.rvo[rr + 1];
+    if (e - s0 < 2) continue;
+    bool pv = false; double pux = 0, puy = 0;   // previous real edge direction (the ring closes)
+    {
+      const uint64_t j = e - 2;
+      if (!R.syn(j)) {
+        double a, b, c2, dd; vx(j, a, b); vx(j + 1, c2, dd);
+        const double L = hypot(c2 - a, dd - b);
+        if (L > 0) { pv = true; pux = (c2 - a) / L; puy = (dd - b) / L; }
+      }
+    }
+    double x0, y0; vx(s0, x0, y0);
+    for (uint64_t j = s0; j + 1 < e && !ex; j++) {
+      double x1, y1; vx(j + 1, x1, y1);
+      if (!((y0 > 0) == (y1 > 0) && y0 != 0 && y1 != 0)) {
+        const bool so = left_of(x0, y0, x1, y1, ox, 0.0), sp = left_of(x0, y0, x1, y1, 0.0, 0.0);
+        if (so != sp) {
+          const bool su = orient(ox, 0.0, 0.0, 0.0, x0, y0) > 0, sv = orient(ox, 0.0, 0.0, 0.0, x1, y1) > 0;
+          if (su != sv) par = !par;
+        }
+      }
+      const double L = hypot(x1 - x0, y1 - y0);
+      if (R.syn(j) || L == 0) { if (R.syn(j)) pv = false; x0 = x1; y0 = y1; continue; }
+      const double ux = (x1 - x0) / L, uy = (y1 - y0) / L;
+      if (r > 0) {
+        const double t = -x0 * ux - y0 * uy, s = -y0 * ux + x0 * uy;
+        if (fabs(s) < r - eps && t > -eps && t < L + eps) ex = true;
+        else if (pv && vertex_excl(pux, puy, ux, uy, r, -x0, -y0, eps)) ex = true;
+      }
+      pv = true; pux = ux; puy = uy;
+      x0 = x1; y0 = y1;
+    }
+  }
+  bits[i] = ex ? 2 : (par ? 1 : 0);
+}
+// (point, parent) keys of every candidate with its bits
+__global__ void k_pt_keys(const uint2* __restrict__ pairs, uint64_t n, const uint32_t* parR, unsigned long long* keys) {
+  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) keys[i] = ((unsigned long long)pairs[i].x << 32) | (parR ? parR[pairs[i].y] : pairs[i].y);
+}
+__global__ void k_or_fold(const unsigned long long* __restrict__ k, const uint8_t* __restrict__ v, const uint32_t* __restrict__ head,
+                          const uint32_t* __restrict__ hoff, uint64_t n, uint32_t* keep_seg, uint2* seg_pair) {
+  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n || !head[i]) return;
+  uint8_t o = 0;
+  for (uint64_t j = i; j < n && (j == i || !head[j]); j++) o |= v[j];
+  const uint32_t s = hoff[i];
+  keep_seg[s] = o == 1;
+  seg_pair[s] = make_uint2((uint32_t)(k[i] >> 32), (uint32_t)k[i]);
 }
 
 void points_buffer_host(gsj_ctx* c, const gsj_layer* pts, const gsj_layer* R, double d, int erode, const gsj_join_opts* op, gsj_pairs_sink sink,
                         void* user, gsj_join_stats* stp) {
   if (!pts->is_points || R->is_points) throw Error(GSJ_ERR_ARG, "a point layer and a polygon layer are needed");
-  if (erode) throw Error(GSJ_ERR_ARG, "points erode: not built yet");
   const gsj_join_opts o = opts_or_default(op);
   gsj_join_stats st{};
   const uint64_t l0 = c->launches;
@@ -449,9 +1077,10 @@ void points_buffer_host(gsj_ctx* c, const gsj_layer* pts, const gsj_layer* R, do
   Timer tm(s);
   const uint32_t n = pts->d.n;
   const float4* qbb = pts->d.bb;
-  if (d > 0) {
+  const double grow = erode ? d * 1.002 : d;   // erode: every piece whose boundary may be within r of the point
+  if (grow > 0) {
     float4* e = c->qbb.as<float4>(n);
-    k_expand_points<<<grid_for(n, 256), 256, 0, s>>>(pts->pts, n, d, e); c->launches++;
+    k_expand_points<<<grid_for(n, 256), 256, 0, s>>>(pts->pts, n, grow, e); c->launches++;
     GSJ_CK(cudaGetLastError());
     qbb = e;
   }
@@ -467,12 +1096,35 @@ void points_buffer_host(gsj_ctx* c, const gsj_layer* pts, const gsj_layer* R, do
     if (!np) continue;
     tm.start();
     uint8_t* hit = c->flag.as<uint8_t>(np);
-    k_pt_dwithin<<<grid_for(np, 128), 128, 0, s>>>(pts->pts, R->d, pairs, np, d, hit); c->launches++;
+    if (erode) { k_pt_erode<<<grid_for(np, 128), 128, 0, s>>>(pts->pts, R->d, pairs, np, d, hit); c->launches++; }
+    else { k_pt_dwithin<<<grid_for(np, 128), 128, 0, s>>>(pts->pts, R->d, pairs, np, d, hit); c->launches++; }
     GSJ_CK(cudaGetLastError());
     st.refine_ms += tm.stop();
     tm.start();
     uint2* out = nullptr;
-    const uint64_t nu = fold_unique(c, pairs, hit, np, 1, nullptr, R->d.parent, &out);
+    uint64_t nu = 0;
+    if (!erode) nu = fold_unique(c, pairs, hit, np, 1, nullptr, R->d.parent, &out);
+    else {   // OR the bits per (point, parent): inside some piece and near no real boundary (== 1)
+      unsigned long long* k1 = c->keys.as<unsigned long long>(np);
+      unsigned long long* k2 = c->keys2.as<unsigned long long>(np);
+      uint8_t* v2 = reinterpret_cast<uint8_t*>(c->misc3.as<uint32_t>(np / 4 + 1));
+      k_pt_keys<<<grid_for(np, 256), 256, 0, s>>>(pairs, np, R->d.parent, k1); c->launches++;
+      size_t tb = 0;
+      GSJ_CK(cub::DeviceRadixSort::SortPairs(nullptr, tb, k1, k2, hit, v2, (int64_t)np, 0, 64, s));
+      GSJ_CK(cub::DeviceRadixSort::SortPairs(c->tmp.get(tb), tb, k1, k2, hit, v2, (int64_t)np, 0, 64, s));
+      uint32_t* head = c->misc1.as<uint32_t>(np);
+      uint32_t* hoff = c->misc2.as<uint32_t>(np);
+      k_unique_heads<<<grid_for(np, 256), 256, 0, s>>>(k2, np, head); c->launches++;
+      const uint64_t nseg = scan_count(c, head, hoff, np);
+      uint32_t* keep = c->keep.as<uint32_t>(nseg);
+      uint2* segp = c->agg_flag.as<uint2>(nseg);
+      k_or_fold<<<grid_for(np, 256), 256, 0, s>>>(k2, v2, head, hoff, np, keep, segp); c->launches++;
+      uint32_t* off = c->idx.as<uint32_t>(nseg);
+      nu = scan_count(c, keep, off, nseg);
+      out = c->opairs.as<uint2>(nu);
+      k_compact_pairs<<<grid_for(nseg, 256), 256, 0, s>>>(segp, keep, off, nseg, out); c->launches++;
+      GSJ_CK(cudaGetLastError());
+    }
     st.compact_ms += tm.stop();
     emit(out, nu);
   }

@@ -6,6 +6,7 @@
 #include <cstdio>
 #include <stdexcept>
 #include <string>
+#include <functional>
 #include <vector>
 #include "../../include/gsj.h"
 #include "geom.cuh"
@@ -92,7 +93,8 @@ struct gsj_ctx {
   uint64_t node_visits = 0;   // LBVH nodes visited by traversals (roofline accounting)   // kernels launched by this context (reported per call in the stats)
   // scratch pools
   gsj::DevBuf counters, cand, flag, area, ev, evb, heavy, scratch, keep, opairs, oarea, oev, oevb, ocode, tmp, keys, keys2, idx,
-      idx2, agg_area, agg_ev, agg_evb, agg_flag, qbb, uf, misc1, misc2, misc3;
+      idx2, agg_area, agg_ev, agg_evb, agg_flag, qbb, uf, misc1, misc2, misc3,
+      er_pf, er_keep, er_off, er_pairs, er_flag, er_heavy, er_tiles, er_tiles2, er_slab, er_again, er_scr, er_ctr, er_tmp;
   gsj::PinnedBuf h_counters, h_pairs, h_area, h_code, h_where;
 };
 
@@ -116,6 +118,13 @@ struct RefineArgs {
   double tol_rel, eps_par, tol_abs;
   int want_area, want_relate, snap_half_ulp;
 };
+using PrefilterFn = std::function<uint64_t(uint2*, uint64_t)>;
+using DeviceBatchFn = std::function<void(const uint2*, const double*, uint64_t)>;
+void join_device(gsj_ctx* c, const gsj_layer* P, const gsj_layer* R, const RefineArgs& rp, const gsj_join_opts& o, gsj_join_stats& st,
+                 const PrefilterFn& pre, const DeviceBatchFn& on_batch);
+uint64_t candidates_for(gsj_ctx* c, const float4* qbb, const uint32_t* qorder, uint32_t q0, uint32_t nq, const DBvh& T, int upper, uint2** out);
+gsj_join_opts opts_or_default(const gsj_join_opts* o);
+
 // per-pair refinement (flag, area, ev, evb); returns the number of pairs that took the oversized path
 uint64_t refine(gsj_ctx* c, const gsj_layer* P, const gsj_layer* R, const uint2* pairs, uint64_t np, const RefineArgs& rp, int mode,
                 uint8_t* flag, double* area, double4* ev, uint32_t* evb);

@@ -137,8 +137,10 @@ struct JoinOut {   // device pointers of one finished batch
 };
 
 // Runs one join; calls on_batch(JoinOut) for every finished batch (device pointers, valid until the next batch).
+// pre (optional) may drop candidate pairs in place before refinement and returns the new count.
 template <class F>
-void run_join(gsj_ctx* c, const gsj_layer* P, const gsj_layer* R, const RefineArgs& rp, const gsj_join_opts& o, gsj_join_stats& st, F&& on_batch) {
+void run_join(gsj_ctx* c, const gsj_layer* P, const gsj_layer* R, const RefineArgs& rp, const gsj_join_opts& o, gsj_join_stats& st, F&& on_batch,
+              const PrefilterFn* pre = nullptr) {
   if (P->is_points || R->is_points) throw Error(GSJ_ERR_ARG, "polygon join needs two polygon layers");
   cudaStream_t s = c->stream;
   const bool agg = (P->d.parent || R->d.parent) && !o.no_agg;
@@ -154,6 +156,7 @@ void run_join(gsj_ctx* c, const gsj_layer* P, const gsj_layer* R, const RefineAr
     st.traverse_ms += tm.stop();
     st.candidates += np;
     st.batches++;
+    if (pre && *pre && np) np = (*pre)(pairs, np);
     if (!np) continue;
     tm.start();
     uint8_t* flag = c->flag.as<uint8_t>(np);
@@ -445,6 +448,12 @@ void cluster_host(gsj_ctx* c, const gsj_layer* P, uint32_t nparent, const gsj_jo
   st.launches = c->launches - l0;
   st.node_visits = c->node_visits - v0;
   if (stp) *stp = st;
+}
+
+// the intersects + area join with device-side results: pass 1 of the erosion join
+void join_device(gsj_ctx* c, const gsj_layer* P, const gsj_layer* R, const RefineArgs& rp, const gsj_join_opts& o, gsj_join_stats& st,
+                 const PrefilterFn& pre, const DeviceBatchFn& on_batch) {
+  run_join(c, P, R, rp, o, st, [&](const JoinOut& out) { if (out.n) on_batch(out.pairs, out.area, out.n); }, &pre);
 }
 
 void candidates_host(gsj_ctx* c, const gsj_layer* P, const gsj_layer* R, int upper, gsj_pairs_sink sink, void* user) {

@@ -36,6 +36,7 @@ def layers():
         "zonesB": ("gset", lambda: gen.voronoi(50, gen.LA_BOX, 1, vmin=4, vmax=4)),
         "parcels": ("gset", lambda: gen.layer_parcels(3000, SMALL_BOX, seed=5)),
         "points": ("pset", lambda: gen.points(5000, SMALL_BOX, 3)),
+        "parcels2": ("gset", lambda: gen.layer_parcels(2000, SMALL_BOX, seed=6)),
     }
 
 
@@ -57,6 +58,14 @@ CASES = {
     "pp_erode1": ("parcels", "parcels", ["--erode", "1"]),
     "pp_erode1_sub32": ("parcels", "parcels", ["--erode", "1", "--subdiv", "32"]),
     "pts_erode1": ("points", "parcels", ["--erode", "1"]),
+    "pq_area": ("parcels", "parcels2", ["--area"]),
+    "pq_relate": ("parcels", "parcels2", ["--relate"]),
+    "pq_erode1": ("parcels", "parcels2", ["--erode", "1"]),
+    "pq_erode1_3": ("parcels", "parcels2", ["--erode", "1,3"]),
+    "pq_erode5": ("parcels", "parcels2", ["--erode", "5"]),
+    "pq_erode1_sub32": ("parcels", "parcels2", ["--erode", "1", "--subdiv", "32"]),
+    "pq_dwithin5": ("parcels", "parcels2", ["--dwithin", "5"]),
+    "pts_erode3_sub32": ("points", "parcels", ["--erode", "3", "--subdiv-b", "32"]),
 }
 
 

@@ -169,3 +169,45 @@ def test_dedup_members():
     assert u.n == ps.n and list(midx[moff[5]:moff[6]]) == [5, 300, 302] and list(midx[moff[7]:moff[8]]) == [7, 301]
     um, moffm, midxm = gsj.dedup(dup, morton=True)
     assert um.n == ps.n and sorted(np.diff(moffm).tolist()) == sorted(np.diff(moff).tolist())
+
+
+def rowset(p):
+    return set(map(tuple, np.asarray(p).reshape(-1, 2).tolist()))
+
+
+def self_rows(p):
+    off = p[:, 0] != p[:, 1]
+    return rowset(np.concatenate([p, p[off][:, ::-1]]))
+
+
+def test_golden_erode(golden_layers, sub32):
+    """ST_Intersects(ST_Buffer(a, -1 m), ST_Buffer(b, -1 m)) and points in ST_Buffer(b, -1 m), whole and subdivided."""
+    P = O.OSet(golden_layers["parcels"])
+    none = np.zeros(golden_layers["parcels"].n, np.uint8)   # the harness's need_self without dedup: no self rows
+    p = O.erode(P, P, 1.0, 1.0, same=True, need_self=none)
+    assert self_rows(p) == rowset(np.load(f"{MG.HERE}/pp_erode1.npz")["pairs"])
+    S = O.OSet(sub32)
+    p = O.erode(S, S, 1.0, 1.0, same=True, need_self=none)
+    assert self_rows(p) == rowset(np.load(f"{MG.HERE}/pp_erode1_sub32.npz")["pairs"])
+    p = O.pt_erode(golden_layers["points"], P, 1.0)
+    assert rowset(p) == rowset(np.load(f"{MG.HERE}/pts_erode1.npz")["pairs"])
+
+
+def test_golden_two_layer_cases(golden_layers):
+    """Two overlapping parcel layers (different seeds): area, DE-9IM, eroded intersects with equal and unequal radii,
+    the subdivided erosion, dwithin, and points in subdivided eroded parcels."""
+    import gsj
+    P, Q = O.OSet(golden_layers["parcels"]), O.OSet(golden_layers["parcels2"])
+    p, a, c, _ = O.join(P, Q, O.params(1, 0))
+    check_pairs("pq_area", p, a, "area")
+    p, a, c, _ = O.join(P, Q, O.params(0, 1))
+    check_pairs("pq_relate", p, c, "relate")
+    for case, ra, rb in (("pq_erode1", 1.0, 1.0), ("pq_erode1_3", 1.0, 3.0), ("pq_erode5", 5.0, 5.0)):
+        assert rowset(O.erode(P, Q, ra, rb)) == rowset(np.load(f"{MG.HERE}/{case}.npz")["pairs"]), case
+    SP = O.OSet(gsj.subdivide(golden_layers["parcels"], 32))
+    SQ = O.OSet(gsj.subdivide(golden_layers["parcels2"], 32))
+    assert rowset(O.erode(SP, SQ, 1.0, 1.0)) == rowset(np.load(f"{MG.HERE}/pq_erode1_sub32.npz")["pairs"])
+    p, _ = O.dwithin(P, Q, 5.0)
+    assert rowset(p) == rowset(np.load(f"{MG.HERE}/pq_dwithin5.npz")["pairs"])
+    p = O.pt_erode(golden_layers["points"], SP, 3.0)
+    assert rowset(p) == rowset(np.load(f"{MG.HERE}/pts_erode3_sub32.npz")["pairs"])
