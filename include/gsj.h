@@ -34,6 +34,9 @@ const char* gsj_last_error(const gsj_ctx* ctx);
 /* The context's CUDA stream (a cudaStream_t): every kernel and copy of the context runs on it, in call order.
  * Lets a caller bracket calls with its own CUDA events. */
 void* gsj_ctx_stream(gsj_ctx* ctx);
+/* Name, compute capability and memory of a CUDA device, without a context (the daemon's STATUS, gpujoind.cu:486-494).
+ * GSJ_ERR_CUDA when no CUDA device can be used, GSJ_ERR_ARG for a device index out of range. */
+int gsj_device_query(int device, char* name, size_t namelen, int* cc_major, int* cc_minor, uint64_t* free_bytes, uint64_t* total_bytes);
 /* Free device memory and the number of SMs, for admission decisions (gpujoind.cu:133-137). */
 int gsj_ctx_mem_info(gsj_ctx* ctx, uint64_t* free_bytes, uint64_t* total_bytes, int* sm_count);
 
@@ -45,7 +48,7 @@ int gsj_layer_upload_polygons(gsj_ctx* ctx, uint64_t n, uint64_t nr, uint64_t nv
                               const double* xy, const uint32_t* parent, const uint8_t* syn, gsj_layer** out);
 /* Resident point layer + LBVH over the points' degenerate boxes: upload_points (engine.cuh:1068-1076). */
 int gsj_layer_upload_points(gsj_ctx* ctx, uint64_t n, const double* xy, gsj_layer** out);
-/* free_set / free_points / free_bvh (engine.cuh:91-97, 1077, 230). */
+/* free_set / free_points / free_bvh (engine.cuh:91-97, 1077, 230). ctx may be NULL (no stream to drain first). */
 void gsj_layer_free(gsj_ctx* ctx, gsj_layer* layer);
 
 typedef struct gsj_layer_info {

@@ -72,6 +72,22 @@ const char* gsj_last_error(const gsj_ctx* c) { return c ? c->err.c_str() : "no c
 
 void* gsj_ctx_stream(gsj_ctx* c) { return c ? (void*)c->stream : nullptr; }
 
+int gsj_device_query(int device, char* name, size_t namelen, int* cc_major, int* cc_minor, uint64_t* free_bytes, uint64_t* total_bytes) {
+  int nd = 0;
+  if (cudaGetDeviceCount(&nd) != cudaSuccess) { (void)cudaGetLastError(); return GSJ_ERR_CUDA; }
+  if (device < 0 || device >= nd) return GSJ_ERR_ARG;
+  cudaDeviceProp p;
+  if (cudaSetDevice(device) != cudaSuccess || cudaGetDeviceProperties(&p, device) != cudaSuccess) { (void)cudaGetLastError(); return GSJ_ERR_CUDA; }
+  if (name && namelen) { std::strncpy(name, p.name, namelen - 1); name[namelen - 1] = 0; }
+  if (cc_major) *cc_major = p.major;
+  if (cc_minor) *cc_minor = p.minor;
+  size_t f = 0, t = 0;
+  if (cudaMemGetInfo(&f, &t) != cudaSuccess) { (void)cudaGetLastError(); return GSJ_ERR_CUDA; }
+  if (free_bytes) *free_bytes = f;
+  if (total_bytes) *total_bytes = t;
+  return GSJ_OK;
+}
+
 int gsj_ctx_mem_info(gsj_ctx* c, uint64_t* fr, uint64_t* tot, int* sms) {
   if (!c) return GSJ_ERR_ARG;
   return guard(c, [&] {
@@ -109,6 +125,7 @@ int gsj_layer_upload_points(gsj_ctx* c, uint64_t n, const double* xy, gsj_layer*
 void gsj_layer_free(gsj_ctx* c, gsj_layer* L) {
   if (!L) return;
   if (c) { cudaSetDevice(c->device); if (c->stream) cudaStreamSynchronize(c->stream); }
+  else cudaSetDevice(L->device);
   gsj::layer_free(L);
   delete L;
 }

@@ -1,0 +1,896 @@
+// gsjd: serves resident layers over the gpujoind wire protocol (gsp_protocol.h) with the gsj engine.
+//
+// Behaviour follows daemon/gpujoind.cu of landstats-us/postgis-cuda: the same ops, argument checks, row rules,
+// frame format and stats keys, so its Postgres extension works unchanged. Differences, by design:
+//  - layers come from files (binary COPY / .gset / .pset, resolved inside --data-dir) instead of SQL over libpq;
+//    LOAD_QUERY and LOAD's row filter need PostgreSQL and answer with an error;
+//  - GPU work runs on a pool of engine contexts (--workers, each its own CUDA stream and scratch) sharing the
+//    resident layers, so small requests overlap on the GPU instead of queueing behind one device lock
+//    (g_gpu, gpujoind.cu:35); admission is first come, first served.
+#include <arpa/inet.h>
+#include <netinet/in.h>
+#include <netinet/tcp.h>
+#include <omp.h>
+#include <poll.h>
+#include <sys/socket.h>
+#include <sys/stat.h>
+#include <sys/un.h>
+#include <unistd.h>
+
+#include <atomic>
+#include <cerrno>
+#include <chrono>
+#include <climits>
+#include <cmath>
+#include <condition_variable>
+#include <csignal>
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <ctime>
+#include <fstream>
+#include <limits>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <stdexcept>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "../../../include/gsj.h"
+#include "../../../include/gsjd.h"
+#include "../../../include/gsp_protocol.h"
+#include "load.h"
+#include "rows.h"
+
+namespace gsjd {
+namespace {
+
+using Clock = std::chrono::steady_clock;
+double secs_since(Clock::time_point t) { return std::chrono::duration<double>(Clock::now() - t).count(); }
+
+struct Config {
+  std::string socket = "/tmp/gpujoind.sock", tcp, token, data_dir = ".";
+  int device = 0, workers = 2, threads = 16;
+};
+Config g_cfg;
+std::atomic<bool> g_stop{false};
+
+void logf(const char* fmt, ...) {
+  char ts[32];
+  const time_t now = time(nullptr);
+  struct tm tmv;
+  localtime_r(&now, &tmv);
+  strftime(ts, sizeof ts, "%Y-%m-%d %H:%M:%S", &tmv);
+  va_list ap;
+  va_start(ap, fmt);
+  fprintf(stderr, "[%s] ", ts);
+  vfprintf(stderr, fmt, ap);
+  fputc('\n', stderr);
+  va_end(ap);
+}
+
+// ---- JSON text -------------------------------------------------------------------------------------------------
+std::string jquote(const std::string& s) {
+  std::string o = "\"";
+  for (unsigned char c : s) {
+    if (c == '"' || c == '\\') { o += '\\'; o += (char)c; }
+    else if (c < 0x20) { char b[8]; snprintf(b, sizeof b, "\\u%04x", c); o += b; }
+    else o += (char)c;
+  }
+  return o + "\"";
+}
+std::string jnum(double x) {
+  if (!std::isfinite(x)) return "null";
+  char b[64];
+  snprintf(b, sizeof b, "%.6g", x);
+  return b;
+}
+class Json {
+ public:
+  Json& key(const char* k) { s_ += first_ ? "" : ","; first_ = false; s_ += jquote(k) + ":"; return *this; }
+  Json& str(const char* k, const std::string& v) { return key(k).raw(jquote(v)); }
+  Json& num(const char* k, double v) { return key(k).raw(jnum(v)); }
+  Json& u64(const char* k, uint64_t v) { return key(k).raw(std::to_string(v)); }
+  Json& boolean(const char* k, bool v) { return key(k).raw(v ? "true" : "false"); }
+  Json& raw(const std::string& v) { s_ += v; return *this; }
+  std::string done() const { return s_ + "}"; }
+
+ private:
+  std::string s_ = "{";
+  bool first_ = true;
+};
+
+// ---- engine contexts ---------------------------------------------------------------------------------------------
+// A fixed pool of contexts on one device, created on first use (the daemon starts without touching the GPU).
+// Waiters are served in arrival order.
+class GpuPool {
+ public:
+  gsj_ctx* acquire() {
+    std::unique_lock<std::mutex> lk(m_);
+    const uint64_t ticket = next_++;
+    cv_.wait(lk, [&] { return ticket == serving_ && (!free_.empty() || created_ < g_cfg.workers); });
+    serving_++;
+    gsj_ctx* c = nullptr;
+    if (!free_.empty()) { c = free_.back(); free_.pop_back(); }
+    else {
+      const int rc = gsj_ctx_create(g_cfg.device, &c);
+      if (rc) {
+        cv_.notify_all();
+        throw std::runtime_error("no usable CUDA device " + std::to_string(g_cfg.device) + " (gsj_ctx_create: " + std::to_string(rc) + ")");
+      }
+      created_++;
+    }
+    busy_++;
+    cv_.notify_all();
+    return c;
+  }
+  void release(gsj_ctx* c) {
+    std::lock_guard<std::mutex> lk(m_);
+    free_.push_back(c);
+    busy_--;
+    cv_.notify_all();
+  }
+  void counts(int* busy, uint64_t* queued) {
+    std::lock_guard<std::mutex> lk(m_);
+    *busy = busy_;
+    *queued = next_ - serving_;
+  }
+
+ private:
+  std::mutex m_;
+  std::condition_variable cv_;
+  std::vector<gsj_ctx*> free_;
+  int created_ = 0, busy_ = 0;
+  uint64_t next_ = 0, serving_ = 0;
+};
+GpuPool g_pool;
+
+class Lease {
+ public:
+  Lease() : c_(g_pool.acquire()) {}
+  ~Lease() { g_pool.release(c_); }
+  gsj_ctx* get() const { return c_; }
+  Lease(const Lease&) = delete;
+  Lease& operator=(const Lease&) = delete;
+
+ private:
+  gsj_ctx* c_;
+};
+
+void check(gsj_ctx* c, int rc, const char* what) {
+  if (rc) throw std::runtime_error(std::string(what) + ": " + gsj_last_error(c));
+}
+
+// ---- layers -------------------------------------------------------------------------------------------------------
+struct Layer {
+  std::string name, kind, source;
+  int subdiv = 0;
+  bool deduped = false;
+  IdTable ids;
+  uint64_t rows = 0, skipped = 0, n_distinct = 0, gpu_geoms = 0, verts = 0, gpu_bytes = 0;
+  std::vector<uint64_t> moff;
+  std::vector<uint32_t> midx;
+  gsj_layer* h = nullptr;
+  double copy_s = 0, prep_s = 0, upload_s = 0;
+
+  Members members() const { return deduped ? Members{moff.data(), midx.data()} : Members{}; }
+  bool points() const { return kind == "point"; }
+  ~Layer() { if (h) gsj_layer_free(nullptr, h); }
+  std::string json() const {   // Layer::json, gpujoind.cu:81-86
+    return Json().str("layer", name).str("kind", kind).str("source", source).u64("rows", rows).u64("skipped", skipped)
+        .u64("distinct", n_distinct).u64("gpu_geoms", gpu_geoms).u64("vertices", verts).u64("subdivide", (uint64_t)subdiv)
+        .boolean("dedup", deduped).num("gpu_mb", gpu_bytes / 1048576.0).num("copy_s", copy_s).num("prepare_s", prep_s)
+        .num("upload_s", upload_s).done();
+  }
+};
+
+std::mutex g_reg;
+std::map<std::string, std::shared_ptr<Layer>> g_layers;
+
+std::shared_ptr<Layer> get_layer(const std::string& n) {
+  std::lock_guard<std::mutex> g(g_reg);
+  auto it = g_layers.find(n);
+  if (it == g_layers.end()) throw std::runtime_error("no such layer: " + n);
+  return it->second;
+}
+
+// LOAD's table argument: a file inside the data directory.
+std::string resolve_path(const std::string& p) {
+  if (p.empty()) throw std::runtime_error("LOAD needs a file path as its table argument");
+  const std::string full = p[0] == '/' ? p : g_cfg.data_dir + "/" + p;
+  char rp[PATH_MAX], rd[PATH_MAX];
+  if (!realpath(full.c_str(), rp)) throw std::runtime_error("cannot open " + p + ": " + strerror(errno));
+  if (!realpath(g_cfg.data_dir.c_str(), rd)) throw std::runtime_error("bad --data-dir");
+  const std::string a = rp, d = rd;
+  if (a.compare(0, d.size(), d) != 0 || (a.size() > d.size() && a[d.size()] != '/' && d != "/"))
+    throw std::runtime_error("LOAD reads files inside the data directory only: " + p);
+  return a;
+}
+
+template <class T> struct HostArray {   // library-allocated host arrays (gsj_dedup / gsj_subdivide outputs)
+  T* p = nullptr;
+  ~HostArray() { if (p) gsj_host_free(p); }
+};
+
+std::string build_layer(const std::string& name, const std::string& path, int subdiv, bool dedup) {
+  auto t0 = Clock::now();
+  LoadedLayer ld;
+  const std::string err = load_layer_file(path, ld);
+  if (!err.empty()) throw std::runtime_error("load failed: " + err);
+  auto L = std::make_shared<Layer>();
+  L->name = name; L->subdiv = subdiv; L->source = "file " + path; L->copy_s = secs_since(t0);
+  L->rows = ld.ids.size();
+  L->skipped = ld.skipped_null + ld.skipped_type + ld.skipped_empty;
+  L->ids = std::move(ld.ids);
+  logf("load %s: %llu rows in %.2fs (skipped null=%llu type=%llu empty=%llu)", name.c_str(), (unsigned long long)L->rows, L->copy_s,
+       (unsigned long long)ld.skipped_null, (unsigned long long)ld.skipped_type, (unsigned long long)ld.skipped_empty);
+  t0 = Clock::now();
+  if (ld.is_points) {
+    L->kind = "point"; L->n_distinct = L->gpu_geoms = L->verts = L->rows;
+    if (L->rows == 0) throw std::runtime_error("layer has no rows");
+    Lease lease;
+    auto t1 = Clock::now();
+    check(lease.get(), gsj_layer_upload_points(lease.get(), L->rows, ld.xy.data(), &L->h), "upload");
+    L->upload_s = secs_since(t1);
+  } else {
+    L->kind = "polygon";
+    const uint64_t n = ld.gro.size() - 1;
+    if (n == 0) throw std::runtime_error("layer has no polygonal rows");
+    uint64_t bn = n, bnr = ld.rvo.size() - 1, bnv = ld.xy.size() / 2;
+    const uint64_t* gro = ld.gro.data();
+    const uint64_t* rvo = ld.rvo.data();
+    const double* xy = ld.xy.data();
+    HostArray<uint64_t> dgro, drvo, dmoff, sgro, srvo;
+    HostArray<double> dxy, sxy;
+    HostArray<uint32_t> dmidx, spar;
+    HostArray<uint8_t> ssyn;
+    if (dedup) {   // identical geometries once, rows expand to members (dedup_set, first-occurrence order)
+      uint64_t un, unr, unv;
+      if (gsj_dedup(bn, bnr, bnv, gro, rvo, xy, 0, &un, &unr, &unv, &dgro.p, &drvo.p, &dxy.p, &dmoff.p, &dmidx.p))
+        throw std::runtime_error("dedup failed");
+      L->deduped = true;
+      L->moff.assign(dmoff.p, dmoff.p + un + 1);
+      L->midx.assign(dmidx.p, dmidx.p + n);
+      bn = un; bnr = unr; bnv = unv; gro = dgro.p; rvo = drvo.p; xy = dxy.p;
+    }
+    L->n_distinct = bn;
+    if (subdiv > 0) {
+      uint64_t pn, pnr, pnv;
+      if (gsj_subdivide(bn, bnr, bnv, gro, rvo, xy, subdiv, &pn, &pnr, &pnv, &sgro.p, &srvo.p, &sxy.p, &spar.p, &ssyn.p))
+        throw std::runtime_error("subdivide failed");
+      bn = pn; bnr = pnr; bnv = pnv; gro = sgro.p; rvo = srvo.p; xy = sxy.p;
+    }
+    L->gpu_geoms = bn; L->verts = bnv;
+    L->prep_s = secs_since(t0);
+    Lease lease;
+    uint64_t fr = 0, tot = 0;
+    check(lease.get(), gsj_ctx_mem_info(lease.get(), &fr, &tot, nullptr), "memory query");
+    const uint64_t need = bnv * 16 + bnr * 8 + bn * 120 + bnv / 8;   // vertices, rings, per-geometry arrays + LBVH
+    if (need + (2ull << 30) > fr)
+      throw std::runtime_error("not enough GPU memory: need ~" + std::to_string(need >> 20) + " MB, free " + std::to_string(fr >> 20) + " MB");
+    auto t1 = Clock::now();
+    check(lease.get(), gsj_layer_upload_polygons(lease.get(), bn, bnr, bnv, gro, rvo, xy, subdiv > 0 ? spar.p : nullptr,
+                                                 subdiv > 0 ? ssyn.p : nullptr, &L->h), "upload");
+    L->upload_s = secs_since(t1);
+  }
+  gsj_layer_info info;
+  gsj_layer_get_info(L->h, &info);
+  L->gpu_bytes = info.device_bytes;
+  const std::string js = L->json();
+  logf("load %s: ready %s", name.c_str(), js.c_str());
+  std::shared_ptr<Layer> old;
+  {
+    std::lock_guard<std::mutex> g(g_reg);
+    auto& slot = g_layers[name];
+    old = slot;
+    slot = L;
+  }
+  return js;
+}
+
+// ---- connection ---------------------------------------------------------------------------------------------------
+struct Conn {
+  int fd;
+  volatile int broken = 0;   // the client went away: the engine stops between batches (JoinOpts::cancel)
+  bool streaming = false;    // a result stream started: errors go out as GSP_FRAME_ERR
+  bool read_full(void* p, size_t n) {
+    char* c = static_cast<char*>(p);
+    while (n) {
+      const ssize_t r = ::read(fd, c, n);
+      if (r <= 0) { if (r < 0 && errno == EINTR) continue; return false; }
+      c += r; n -= (size_t)r;
+    }
+    return true;
+  }
+  bool write_full(const void* p, size_t n) {
+    const char* c = static_cast<const char*>(p);
+    while (n && !broken) {
+      const ssize_t r = ::send(fd, c, n, MSG_NOSIGNAL);
+      if (r <= 0) { if (r < 0 && errno == EINTR) continue; broken = 1; return false; }
+      c += r; n -= (size_t)r;
+    }
+    return !broken;
+  }
+  bool u32(uint32_t v) { return write_full(&v, 4); }
+  bool str(const std::string& s) { return u32((uint32_t)s.size()) && write_full(s.data(), s.size()); }
+  void ok_json(const std::string& j) { u32(GSP_OK); str(j); }
+  void error(const std::string& m) { u32(GSP_ERR); str(m); }
+  void end_stream(const std::string& stats) { u32(0); str(stats); }
+};
+
+// Encode rows of n items in parallel into independent runs of complete frames, send them in order
+// (send_parallel, gpujoind.cu:192-206). enc(i, FrameWriter&) writes the rows of item i.
+template <class Enc> uint64_t send_rows(Conn& c, uint64_t n, Enc&& enc) {
+  if (!n || c.broken) return 0;
+  const int T = std::max(1, g_cfg.threads);
+  const uint64_t nch = std::min<uint64_t>(n, (uint64_t)T * 4);
+  std::vector<FrameWriter> fw(nch);
+#pragma omp parallel for num_threads(T) schedule(dynamic, 1)
+  for (int64_t k = 0; k < (int64_t)nch; k++) {
+    const uint64_t i0 = n * k / nch, i1 = n * (k + 1) / nch;
+    fw[k].out.reserve((i1 - i0) * 64);
+    fw[k].begin();
+    for (uint64_t i = i0; i < i1; i++) enc(i, fw[k]);
+    fw[k].finish();
+  }
+  uint64_t rows = 0;
+  for (auto& f : fw) {
+    if (!c.write_full(f.out.data(), f.out.size())) break;
+    rows += f.rows;
+  }
+  return rows;
+}
+
+constexpr double kNaN = std::numeric_limits<double>::quiet_NaN();
+// relate(point, polygon) for a point inside / on the boundary (DE9IM_PT_INTERIOR / _BOUNDARY, engine.cuh:337-338)
+constexpr uint32_t kPtInterior = 1u | (3u << 12) | (2u << 14) | (3u << 16);   // 0FFFFF212
+constexpr uint32_t kPtBoundary = (1u << 2) | (3u << 12) | (2u << 14) | (3u << 16);   // F0FFFF212
+
+bool self_pairs_arg(const std::string& s) {
+  if (s != "all" && s != "distinct") throw std::runtime_error("self_pairs must be 'all' or 'distinct'");
+  return s == "distinct";
+}
+
+// The engine call failed: the client going away ends the request quietly, anything else is an error.
+void engine_status(Conn& c, gsj_ctx* ctx, int rc, const char* what) {
+  if (!rc) return;
+  if (c.broken && (rc == GSJ_ERR_SINK || rc == GSJ_ERR_CANCELLED)) return;
+  throw std::runtime_error(std::string(what) + ": " + gsj_last_error(ctx));
+}
+
+std::string with_stats_only(const std::string& stats, bool want_area, double area_sum) {
+  return stats.substr(0, stats.size() - 1) + ",\"stats_only\":true" + (want_area ? ",\"area_sum\":" + jnum(area_sum) : std::string()) + "}";
+}
+
+// ---- JOIN (op_join, gpujoind.cu:210-290) ----------------------------------------------------------------------------
+struct JoinRun {
+  Conn* c;
+  const Layer *A, *B;   // engine order: A probe (points when one side is points), B build
+  const Layer *LA, *LB; // output order
+  bool same, distinct, want_area, stats_only, swapped;
+  uint64_t total = 0;
+  double area_sum = 0, host_s = 0;
+};
+
+int join_sink(void* u, const uint32_t* p, const double* ar, const uint32_t*, uint64_t n) {
+  JoinRun& J = *static_cast<JoinRun*>(u);
+  const auto th = Clock::now();
+  const Members MA = J.A->members(), MB = J.B->members();
+  if (J.stats_only) {
+    uint64_t t = 0;
+    double as = 0;
+#pragma omp parallel for num_threads(g_cfg.threads) reduction(+ : t, as)
+    for (int64_t i = 0; i < (int64_t)n; i++) {
+      const uint64_t k = pair_row_count(p[2 * i], p[2 * i + 1], MA, MB, J.same, J.distinct);
+      t += k;
+      if (ar) as += ar[i] * (double)k;
+    }
+    J.total += t; J.area_sum += as; J.host_s += secs_since(th);
+    return 0;
+  }
+  const Layer& A = *J.A;
+  const Layer& B = *J.B;
+  J.total += send_rows(*J.c, n, [&](uint64_t i, FrameWriter& f) {
+    const double area = ar ? ar[i] : kNaN;
+    pair_rows(p[2 * i], p[2 * i + 1], MA, MB, J.same, J.distinct, [&](uint32_t ra, uint32_t rb, bool) {
+      const Layer& OB = J.same ? A : B;
+      f.id(A.ids.data(ra), A.ids.len(ra)); f.id(OB.ids.data(rb), OB.ids.len(rb)); f.f64(area); f.row_done();
+    });
+  });
+  J.host_s += secs_since(th);
+  return J.c->broken ? 1 : 0;
+}
+
+int join_points_sink(void* u, const uint32_t* p, const uint8_t*, uint64_t n) {
+  JoinRun& J = *static_cast<JoinRun*>(u);
+  const auto th = Clock::now();
+  const Members MB = J.B->members();
+  if (J.stats_only) {
+    for (uint64_t i = 0; i < n; i++) J.total += MB.count(p[2 * i + 1]);
+    J.host_s += secs_since(th);
+    return 0;
+  }
+  J.total += send_rows(*J.c, n, [&](uint64_t i, FrameWriter& f) {
+    MB.each(p[2 * i + 1], [&](uint32_t rb) {
+      uint32_t ra = p[2 * i];
+      if (J.swapped) std::swap(ra, rb);
+      f.id(J.LA->ids.data(ra), J.LA->ids.len(ra)); f.id(J.LB->ids.data(rb), J.LB->ids.len(rb));
+      f.f64(J.want_area ? 0.0 : kNaN); f.row_done();
+    });
+  });
+  J.host_s += secs_since(th);
+  return J.c->broken ? 1 : 0;
+}
+
+void op_join(Conn& c, const std::vector<std::string>& a) {
+  if (a.size() < 4) throw std::runtime_error("JOIN needs layer_a, layer_b, want_area, self_pairs[, mode]");
+  const bool stats_only = a.size() > 4 && a[4] == "stats";
+  auto A = get_layer(a[0]), B = get_layer(a[1]);
+  const bool want_area = a[2] == "1" || a[2] == "t" || a[2] == "true";
+  const bool distinct = self_pairs_arg(a[3]);
+  const bool same = A.get() == B.get();
+  if (A->points() && B->points()) throw std::runtime_error("point x point joins are not supported");
+  bool swapped = false;
+  if (!A->points() && B->points()) { std::swap(A, B); swapped = true; }   // run as point x polygon
+  Lease lease;
+  gsj_ctx* ctx = lease.get();
+  c.u32(GSP_OK);
+  c.streaming = true;
+  gsj_join_opts o;
+  gsj_join_opts_default(&o);
+  o.cancel = &c.broken;
+  const auto t0 = Clock::now();
+  JoinRun J{&c, A.get(), B.get(), swapped ? B.get() : A.get(), swapped ? A.get() : B.get(), same, distinct, want_area, stats_only, swapped};
+  gsj_join_stats st{};
+  std::string stats;
+  if (A->points()) {
+    engine_status(c, ctx, gsj_join_points(ctx, A->h, B->h, &o, join_points_sink, &J, &st), "join");
+    stats = Json().str("kind", "point_in_polygon").u64("candidates", st.candidates).u64("gpu_hits", st.hits).u64("rows", J.total)
+        .num("traverse_ms", st.traverse_ms).num("refine_ms", st.refine_ms).num("host_encode_send_s", J.host_s).num("total_s", secs_since(t0)).done();
+  } else {
+    gsj_refine_params rp;
+    gsj_refine_params_default(&rp);
+    rp.want_area = want_area ? 1 : 0;
+    o.upper = same;   // self-join: each unordered pair once, mirrored by the row rules
+    engine_status(c, ctx, gsj_join(ctx, A->h, B->h, &rp, &o, join_sink, &J, &st), "join");
+    stats = Json().str("kind", "polygon_polygon").u64("candidates", st.candidates).u64("gpu_hits", st.hits).u64("rows", J.total)
+        .u64("heavy", st.heavy).num("traverse_ms", st.traverse_ms).num("refine_ms", st.refine_ms).num("compact_ms", st.compact_ms)
+        .num("d2h_ms", st.copy_ms).num("host_encode_send_s", J.host_s).num("total_s", secs_since(t0)).done();
+  }
+  if (stats_only) stats = with_stats_only(stats, want_area, J.area_sum);
+  if (!c.broken) c.end_stream(stats);
+  logf("join %s x %s area=%d: %s%s", a[0].c_str(), a[1].c_str(), (int)want_area, stats.c_str(), c.broken ? " (client went away)" : "");
+}
+
+// ---- CLUSTER (op_cluster, gpujoind.cu:293-320) ---------------------------------------------------------------------
+void op_cluster(Conn& c, const std::vector<std::string>& a) {
+  if (a.empty()) throw std::runtime_error("CLUSTER needs layer");
+  auto L = get_layer(a[0]);
+  if (L->points()) throw std::runtime_error("cluster needs a polygon layer");
+  Lease lease;
+  gsj_ctx* ctx = lease.get();
+  const auto t0 = Clock::now();
+  gsj_join_opts o;
+  gsj_join_opts_default(&o);
+  o.cancel = &c.broken;
+  std::vector<uint32_t> root(L->n_distinct);
+  gsj_join_stats st{};
+  check(ctx, gsj_cluster(ctx, L->h, (uint32_t)L->n_distinct, &o, root.data(), &st), "cluster");
+  const double uf_s = secs_since(t0);
+  std::vector<uint32_t> label(L->rows);
+  const uint32_t k = gsjd_cluster_labels((uint32_t)L->n_distinct, root.data(), L->rows, L->deduped ? L->moff.data() : nullptr,
+                                         L->deduped ? L->midx.data() : nullptr, label.data());
+  c.u32(GSP_OK);
+  c.streaming = true;
+  const uint64_t total = send_rows(c, L->rows, [&](uint64_t r, FrameWriter& f) {
+    f.id(L->ids.data(r), L->ids.len(r)); f.u32(label[r]); f.row_done();
+  });
+  const std::string stats = Json().str("kind", "cluster_intersecting").u64("rows", total).u64("clusters", k).u64("candidates", st.candidates)
+      .u64("edges", st.hits).num("traverse_ms", st.traverse_ms).num("refine_ms", st.refine_ms)
+      .num("union_find_ms", std::max(0.0, uf_s * 1e3 - st.traverse_ms - st.refine_ms - st.compact_ms)).num("total_s", secs_since(t0)).done();
+  if (!c.broken) c.end_stream(stats);
+  logf("cluster %s: %s", a[0].c_str(), stats.c_str());
+}
+
+// ---- RELATE (op_relate, gpujoind.cu:323-388) ------------------------------------------------------------------------
+struct RelateRun {
+  Conn* c;
+  const Layer *A, *B;
+  bool same, distinct, swapped;
+  std::string pat;
+  uint64_t total = 0;
+  double host_s = 0;
+};
+
+void put_relate(FrameWriter& f, const RelateRun& R, const Layer& LA, uint32_t ra, const Layer& LB, uint32_t rb, uint32_t code) {
+  if (!R.pat.empty() && !gsj_de9im_match(code, R.pat.c_str())) return;
+  char m[9];
+  gsj_de9im_str(code, m);
+  f.id(LA.ids.data(ra), LA.ids.len(ra)); f.id(LB.ids.data(rb), LB.ids.len(rb)); f.raw(m, 9); f.row_done();
+}
+
+int relate_sink(void* u, const uint32_t* p, const double*, const uint32_t* code, uint64_t n) {
+  RelateRun& R = *static_cast<RelateRun*>(u);
+  const auto th = Clock::now();
+  const Members MA = R.A->members(), MB = R.B->members();
+  const Layer& A = *R.A;
+  const Layer& OB = R.same ? *R.A : *R.B;
+  R.total += send_rows(*R.c, n, [&](uint64_t i, FrameWriter& f) {
+    const uint32_t cd = code[i], ct = gsj_de9im_transpose(cd);
+    pair_rows(p[2 * i], p[2 * i + 1], MA, MB, R.same, R.distinct, [&](uint32_t ra, uint32_t rb, bool tr) {
+      put_relate(f, R, A, ra, OB, rb, tr ? ct : cd);
+    });
+  });
+  R.host_s += secs_since(th);
+  return R.c->broken ? 1 : 0;
+}
+
+int relate_points_sink(void* u, const uint32_t* p, const uint8_t* wh, uint64_t n) {
+  RelateRun& R = *static_cast<RelateRun*>(u);
+  const auto th = Clock::now();
+  const Members MB = R.B->members();
+  R.total += send_rows(*R.c, n, [&](uint64_t i, FrameWriter& f) {
+    const uint32_t code = wh[i] == 2 ? kPtBoundary : kPtInterior;   // relate(point, polygon)
+    MB.each(p[2 * i + 1], [&](uint32_t rb) {
+      if (R.swapped) put_relate(f, R, *R.B, rb, *R.A, p[2 * i], gsj_de9im_transpose(code));
+      else put_relate(f, R, *R.A, p[2 * i], *R.B, rb, code);
+    });
+  });
+  R.host_s += secs_since(th);
+  return R.c->broken ? 1 : 0;
+}
+
+void op_relate(Conn& c, const std::vector<std::string>& a) {
+  if (a.size() < 4) throw std::runtime_error("RELATE needs layer_a, layer_b, pattern, self_pairs");
+  auto A = get_layer(a[0]), B = get_layer(a[1]);
+  const std::string pat = a[2];
+  if (!pat.empty()) {
+    if (pat.size() != 9) throw std::runtime_error("DE-9IM pattern must have 9 characters");
+    for (char ch : pat)
+      if (!strchr("TtFf*012", ch) || ch == 0) throw std::runtime_error("bad DE-9IM pattern character '" + std::string(1, ch) + "'");
+  }
+  const bool distinct = self_pairs_arg(a[3]);
+  const bool same = A.get() == B.get();
+  if (A->points() && B->points()) throw std::runtime_error("point x point relate is not supported");
+  bool swapped = false;
+  if (!A->points() && B->points()) { std::swap(A, B); swapped = true; }
+  Lease lease;
+  gsj_ctx* ctx = lease.get();
+  c.u32(GSP_OK);
+  c.streaming = true;
+  gsj_join_opts o;
+  gsj_join_opts_default(&o);
+  o.cancel = &c.broken;
+  const auto t0 = Clock::now();
+  RelateRun R{&c, A.get(), B.get(), same, distinct, swapped, pat};
+  gsj_join_stats st{};
+  if (A->points()) {
+    engine_status(c, ctx, gsj_join_points(ctx, A->h, B->h, &o, relate_points_sink, &R, &st), "relate");
+  } else {
+    gsj_refine_params rp;
+    gsj_refine_params_default(&rp);
+    rp.want_area = 0;
+    rp.want_relate = 1;
+    o.upper = same;
+    engine_status(c, ctx, gsj_join(ctx, A->h, B->h, &rp, &o, relate_sink, &R, &st), "relate");
+  }
+  const std::string stats = Json().str("kind", "relate").str("pattern", pat).u64("candidates", st.candidates).u64("gpu_hits", st.hits)
+      .u64("rows", R.total).num("host_encode_send_s", R.host_s).num("total_s", secs_since(t0)).done();
+  if (!c.broken) c.end_stream(stats);
+  logf("relate %s x %s: %s%s", a[0].c_str(), a[1].c_str(), stats.c_str(), c.broken ? " (client went away)" : "");
+}
+
+// ---- DWITHIN (op_dwithin, gpujoind.cu:391-484) ----------------------------------------------------------------------
+double to_double(const std::string& s) {
+  char* e;
+  const double v = strtod(s.c_str(), &e);
+  if (s.empty() || *e || !std::isfinite(v)) throw std::runtime_error("not a number: " + s);
+  return v;
+}
+
+struct PairsRun {
+  Conn* c;
+  const Layer *A, *B, *LA, *LB;
+  bool same, distinct, stats_only, swapped;
+  uint64_t total = 0;
+  double host_s = 0;
+};
+
+int pairs_sink(void* u, const uint32_t* p, uint64_t n) {
+  PairsRun& P = *static_cast<PairsRun*>(u);
+  const auto th = Clock::now();
+  const Members MA = P.A->members(), MB = P.B->members();
+  if (P.A->points()) {   // (point, polygon parent) pairs
+    if (P.stats_only) {
+      for (uint64_t i = 0; i < n; i++) P.total += MB.count(p[2 * i + 1]);
+    } else {
+      P.total += send_rows(*P.c, n, [&](uint64_t i, FrameWriter& f) {
+        MB.each(p[2 * i + 1], [&](uint32_t rb) {
+          uint32_t ra = p[2 * i];
+          if (P.swapped) std::swap(ra, rb);
+          f.id(P.LA->ids.data(ra), P.LA->ids.len(ra)); f.id(P.LB->ids.data(rb), P.LB->ids.len(rb)); f.f64(kNaN); f.row_done();
+        });
+      });
+    }
+  } else if (P.stats_only) {
+    uint64_t t = 0;
+#pragma omp parallel for num_threads(g_cfg.threads) reduction(+ : t)
+    for (int64_t i = 0; i < (int64_t)n; i++) t += pair_row_count(p[2 * i], p[2 * i + 1], MA, MB, P.same, P.distinct);
+    P.total += t;
+  } else {
+    const Layer& A = *P.A;
+    const Layer& OB = P.same ? *P.A : *P.B;
+    P.total += send_rows(*P.c, n, [&](uint64_t i, FrameWriter& f) {
+      pair_rows(p[2 * i], p[2 * i + 1], MA, MB, P.same, P.distinct, [&](uint32_t ra, uint32_t rb, bool) {
+        f.id(A.ids.data(ra), A.ids.len(ra)); f.id(OB.ids.data(rb), OB.ids.len(rb)); f.f64(kNaN); f.row_done();
+      });
+    });
+  }
+  P.host_s += secs_since(th);
+  return P.c->broken ? 1 : 0;
+}
+
+void op_dwithin(Conn& c, const std::vector<std::string>& a) {
+  if (a.size() < 6) throw std::runtime_error("DWITHIN needs layer_a, layer_b, mode, dist_a, dist_b, self_pairs[, stats]");
+  const bool stats_only = a.size() > 6 && a[6] == "stats";
+  auto A = get_layer(a[0]), B = get_layer(a[1]);
+  const std::string mode = a[2];
+  const double da = to_double(a[3]), db = to_double(a[4]);
+  const bool distinct = self_pairs_arg(a[5]);
+  bool erode = false;
+  double d = 0, ra = 0, rb = 0;
+  if (mode == "dwithin") {
+    if (da < 0) throw std::runtime_error("distance must be >= 0");
+    d = da;
+  } else if (mode == "buffer") {
+    if (da <= 0 && db <= 0 && (da < 0 || db < 0)) { erode = true; ra = -da; rb = -db; }
+    else if (da >= 0 && db >= 0) d = da + db;
+    else throw std::runtime_error("buffers of opposite sign are not supported");
+  } else {
+    throw std::runtime_error("mode must be 'dwithin' or 'buffer'");
+  }
+  if (A->points() && B->points()) throw std::runtime_error("point x point distance joins are not supported");
+  const bool same = A.get() == B.get();
+  bool swapped = false;
+  if (!A->points() && B->points()) { std::swap(A, B); std::swap(ra, rb); swapped = true; }
+  if (A->points() && erode && ra > 0) throw std::runtime_error("a point layer cannot have a negative buffer");
+  Lease lease;
+  gsj_ctx* ctx = lease.get();
+  c.u32(GSP_OK);
+  c.streaming = true;
+  gsj_join_opts o;
+  gsj_join_opts_default(&o);
+  o.cancel = &c.broken;
+  const auto t0 = Clock::now();
+  PairsRun P{&c, A.get(), B.get(), swapped ? B.get() : A.get(), swapped ? A.get() : B.get(), same, distinct, stats_only, swapped};
+  gsj_join_stats st{};
+  if (A->points()) {
+    const int rc = erode ? gsj_points_erode(ctx, A->h, B->h, rb, &o, pairs_sink, &P, &st) : gsj_points_dwithin(ctx, A->h, B->h, d, &o, pairs_sink, &P, &st);
+    engine_status(c, ctx, rc, "dwithin");
+  } else {
+    o.upper = same;
+    if (erode) {
+      std::vector<uint8_t> need;   // a geometry's pair with itself matters only for groups of identical rows
+      if (same && distinct) {
+        need.assign(A->n_distinct, 0);
+        if (A->deduped) for (uint64_t g = 0; g < A->n_distinct; g++) need[g] = A->moff[g + 1] - A->moff[g] > 1;
+      }
+      engine_status(c, ctx, gsj_erode(ctx, A->h, B->h, ra, rb, same, need.empty() ? nullptr : need.data(), &o, pairs_sink, &P, &st), "dwithin");
+    } else {
+      engine_status(c, ctx, gsj_dwithin(ctx, A->h, B->h, d, same, &o, pairs_sink, &P, &st), "dwithin");
+    }
+  }
+  const std::string stats = Json().str("kind", erode ? "buffer_intersects" : "dwithin").num("distance_m", d).num("erode_a_m", swapped ? rb : ra)
+      .num("erode_b_m", swapped ? ra : rb).u64("candidates", st.candidates).u64("tested", st.candidates).u64("gpu_hits", st.hits)
+      .u64("rows", P.total).u64("heavy", st.heavy).num("traverse_ms", st.traverse_ms).num("refine_ms", st.refine_ms)
+      .num("compact_ms", st.compact_ms).num("d2h_ms", st.copy_ms).num("host_encode_send_s", P.host_s).num("total_s", secs_since(t0))
+      .boolean("stats_only", stats_only).done();
+  if (!c.broken) c.end_stream(stats);
+  logf("dwithin %s x %s %s %s %s: %s%s", a[0].c_str(), a[1].c_str(), mode.c_str(), a[3].c_str(), a[4].c_str(), stats.c_str(),
+       c.broken ? " (client went away)" : "");
+}
+
+// ---- JSON ops -----------------------------------------------------------------------------------------------------
+std::string layer_names() {
+  std::lock_guard<std::mutex> r(g_reg);
+  std::string ls = "[";
+  bool first = true;
+  for (auto& kv : g_layers) { if (!first) ls += ","; first = false; ls += jquote(kv.first); }
+  return ls + "]";
+}
+
+std::string op_status() {   // gpujoind.cu:486-494 (+ the worker pool)
+  char name[256] = {0};
+  int ma = 0, mi = 0;
+  uint64_t fr = 0, tot = 0;
+  const int rc = gsj_device_query(g_cfg.device, name, sizeof name, &ma, &mi, &fr, &tot);
+  if (rc) throw std::runtime_error("no usable CUDA device " + std::to_string(g_cfg.device));
+  int busy = 0;
+  uint64_t queued = 0;
+  g_pool.counts(&busy, &queued);
+  return Json().str("device", name).str("cc", std::to_string(ma) + "." + std::to_string(mi)).num("mem_total_mb", tot / 1048576.0)
+      .num("mem_free_mb", fr / 1048576.0).key("layers").raw(layer_names()).u64("workers", (uint64_t)g_cfg.workers)
+      .u64("busy", (uint64_t)busy).u64("queued", queued).done();
+}
+
+std::string op_list() {
+  std::lock_guard<std::mutex> r(g_reg);
+  std::string s = "[";
+  bool first = true;
+  for (auto& kv : g_layers) { if (!first) s += ","; first = false; s += kv.second->json(); }
+  return s + "]";
+}
+
+int to_int(const std::string& s, int dflt) {
+  if (s.empty()) return dflt;
+  char* e;
+  const long v = strtol(s.c_str(), &e, 10);
+  if (*e) throw std::runtime_error("not an integer: " + s);
+  return (int)v;
+}
+bool to_bool(const std::string& s, bool dflt) {
+  if (s.empty()) return dflt;
+  return s == "1" || s == "t" || s == "true" || s == "on";
+}
+
+bool token_ok(const std::string& tok) {   // constant time in the token's length (gpujoind.cu:527-533)
+  unsigned diff = tok.size() != g_cfg.token.size();
+  for (size_t i = 0; i < g_cfg.token.size(); i++)
+    diff |= (unsigned)(uint8_t)g_cfg.token[i] ^ (unsigned)(uint8_t)(i < tok.size() ? tok[i] : 0);
+  return diff == 0;
+}
+
+void handle(int fd) {
+  Conn c{fd};
+  try {
+    uint32_t hdr[3];
+    if (!c.read_full(hdr, 12) || hdr[0] != GSP_MAGIC || hdr[2] > GSP_MAX_ARGS) { close(fd); return; }
+    std::vector<std::string> args(hdr[2]);
+    for (auto& s : args) {
+      uint32_t l;
+      if (!c.read_full(&l, 4) || l > GSP_MAX_ARG_BYTES) { close(fd); return; }
+      s.resize(l);
+      if (l && !c.read_full(&s[0], l)) { close(fd); return; }
+    }
+    if (!token_ok(args.empty() ? std::string() : args[0])) {
+      logf("rejected request: bad token");
+      c.error("authentication failed");
+      close(fd);
+      return;
+    }
+    if (!args.empty()) args.erase(args.begin());
+    switch (hdr[1]) {
+      case GSP_OP_LOAD: {
+        if (args.size() < 7) throw std::runtime_error("LOAD needs 7 args");
+        // args: layer, table (a file), id_col, geom_col (the file's two columns), filter, subdivide, dedup
+        if (!args[4].empty()) throw std::runtime_error("a row filter needs PostgreSQL: filter the rows when writing the COPY file");
+        c.ok_json(build_layer(args[0], resolve_path(args[1]), to_int(args[5], 0), to_bool(args[6], true)));
+        break;
+      }
+      case GSP_OP_LOAD_QUERY:
+        throw std::runtime_error("LOAD_QUERY runs SQL over libpq, which this daemon does not link: write the query's rows with "
+                                 "COPY (SELECT id::text, geom ...) TO 'file' (FORMAT binary) and LOAD the file");
+      case GSP_OP_DROP: {
+        if (args.empty()) throw std::runtime_error("DROP needs layer");
+        std::shared_ptr<Layer> old;
+        {
+          std::lock_guard<std::mutex> g(g_reg);
+          auto it = g_layers.find(args[0]);
+          if (it != g_layers.end()) { old = it->second; g_layers.erase(it); }
+        }
+        c.ok_json(old ? "true" : "false");
+        break;
+      }
+      case GSP_OP_LIST: c.ok_json(op_list()); break;
+      case GSP_OP_STATUS: c.ok_json(op_status()); break;
+      case GSP_OP_JOIN: op_join(c, args); break;
+      case GSP_OP_CLUSTER: op_cluster(c, args); break;
+      case GSP_OP_RELATE: op_relate(c, args); break;
+      case GSP_OP_DWITHIN: op_dwithin(c, args); break;
+      default: c.error("unknown op");
+    }
+  } catch (const std::exception& e) {
+    logf("error: %s", e.what());
+    if (c.streaming) { c.u32(GSP_FRAME_ERR); c.str(e.what()); }
+    else c.error(e.what());
+  }
+  close(fd);
+}
+
+// ---- listeners ----------------------------------------------------------------------------------------------------
+int listen_unix(const std::string& path) {
+  const int fd = socket(AF_UNIX, SOCK_STREAM, 0);
+  sockaddr_un a{};
+  a.sun_family = AF_UNIX;
+  if (path.size() >= sizeof(a.sun_path)) { fprintf(stderr, "socket path too long\n"); return -1; }
+  strncpy(a.sun_path, path.c_str(), sizeof(a.sun_path) - 1);
+  unlink(path.c_str());
+  if (bind(fd, (sockaddr*)&a, sizeof a) || listen(fd, 64)) { perror(("unix socket " + path).c_str()); close(fd); return -1; }
+  chmod(path.c_str(), 0666);
+  return fd;
+}
+int listen_tcp(const std::string& hp) {
+  const auto pos = hp.rfind(':');
+  if (pos == std::string::npos) { fprintf(stderr, "--tcp wants HOST:PORT\n"); return -1; }
+  const std::string host = hp.substr(0, pos);
+  const int port = atoi(hp.c_str() + pos + 1);
+  const int fd = socket(AF_INET, SOCK_STREAM, 0), one = 1;
+  setsockopt(fd, SOL_SOCKET, SO_REUSEADDR, &one, sizeof one);
+  sockaddr_in a{};
+  a.sin_family = AF_INET;
+  a.sin_port = htons((uint16_t)port);
+  if (inet_pton(AF_INET, host.c_str(), &a.sin_addr) != 1) { fprintf(stderr, "bad tcp address %s\n", hp.c_str()); close(fd); return -1; }
+  if (bind(fd, (sockaddr*)&a, sizeof a) || listen(fd, 64)) { perror(("tcp " + hp).c_str()); close(fd); return -1; }
+  return fd;
+}
+
+void on_signal(int) { g_stop = true; }
+
+const char* kUsage =
+    "usage: gsjd [--socket PATH] [--tcp HOST:PORT] [--token-file FILE] [--data-dir DIR] [--device N] [--workers N]\n"
+    "            [--threads N] [--conninfo STR (accepted, unused: layers load from files)]\n";
+
+}  // namespace
+}  // namespace gsjd
+
+extern "C" int gsjd_main(int argc, char** argv) {
+  using namespace gsjd;
+  for (int i = 1; i < argc; i++) {
+    const std::string a = argv[i];
+    const bool has = i + 1 < argc;
+    if (a == "--socket" && has) g_cfg.socket = argv[++i];
+    else if (a == "--tcp" && has) g_cfg.tcp = argv[++i];
+    else if (a == "--data-dir" && has) g_cfg.data_dir = argv[++i];
+    else if (a == "--device" && has) g_cfg.device = atoi(argv[++i]);
+    else if (a == "--workers" && has) g_cfg.workers = std::max(1, atoi(argv[++i]));
+    else if (a == "--threads" && has) g_cfg.threads = std::max(1, atoi(argv[++i]));
+    else if (a == "--conninfo" && has) ++i;
+    else if (a == "--token-file" && has) {
+      std::ifstream tf(argv[++i]);
+      std::getline(tf, g_cfg.token);
+      if (g_cfg.token.empty()) { fprintf(stderr, "empty token file\n"); return 1; }
+    } else {
+      fputs(kUsage, stderr);
+      return 1;
+    }
+  }
+  if (!g_cfg.tcp.empty() && g_cfg.token.empty()) { fprintf(stderr, "--tcp requires --token-file\n"); return 1; }
+  signal(SIGPIPE, SIG_IGN);
+  struct sigaction sa{};
+  sa.sa_handler = on_signal;   // no SA_RESTART: poll() returns and the loop sees the flag
+  sigaction(SIGTERM, &sa, nullptr);
+  sigaction(SIGINT, &sa, nullptr);
+  std::vector<pollfd> fds;
+  const int u = listen_unix(g_cfg.socket);
+  if (u < 0) return 1;
+  fds.push_back({u, POLLIN, 0});
+  logf("gsjd listening on unix:%s (device %d, %d workers, data dir %s)", g_cfg.socket.c_str(), g_cfg.device, g_cfg.workers, g_cfg.data_dir.c_str());
+  if (!g_cfg.tcp.empty()) {
+    const int t = listen_tcp(g_cfg.tcp);
+    if (t < 0) return 1;
+    fds.push_back({t, POLLIN, 0});
+    logf("listening on tcp:%s", g_cfg.tcp.c_str());
+  }
+  while (!g_stop) {
+    if (poll(fds.data(), fds.size(), 500) < 0) {
+      if (errno == EINTR) continue;
+      perror("poll");
+      return 1;
+    }
+    for (auto& f : fds)
+      if (f.revents & POLLIN) {
+        const int cfd = accept(f.fd, nullptr, nullptr);
+        if (cfd < 0) continue;
+        const int one = 1;
+        setsockopt(cfd, IPPROTO_TCP, TCP_NODELAY, &one, sizeof one);
+        std::thread(handle, cfd).detach();
+      }
+  }
+  for (auto& f : fds) close(f.fd);
+  unlink(g_cfg.socket.c_str());
+  logf("gsjd stopped");
+  return 0;
+}

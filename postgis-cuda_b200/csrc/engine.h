@@ -89,8 +89,8 @@ struct gsj_ctx {
   cudaStream_t stream = nullptr;
   std::string err;
   int refine_attr = 0, dw_attr = 0, er_attr = 0;
-  uint64_t launches = 0;
-  uint64_t node_visits = 0;   // LBVH nodes visited by traversals (roofline accounting)   // kernels launched by this context (reported per call in the stats)
+  uint64_t launches = 0;      // kernels launched by this context (reported per call in the stats)
+  uint64_t node_visits = 0;   // LBVH nodes visited by traversals (roofline accounting)
   // scratch pools
   gsj::DevBuf counters, cand, flag, area, ev, evb, heavy, scratch, keep, opairs, oarea, oev, oevb, ocode, tmp, keys, keys2, idx,
       idx2, agg_area, agg_ev, agg_evb, agg_flag, qbb, uf, misc1, misc2, misc3,
