@@ -122,6 +122,13 @@ def allreduce_sum(x: float, ws: int) -> float:
     return float(t.item())
 
 
+def aggregate(ms_local: float, units_local: float, ws: int):
+    """Whole-job rate over replicas: units of all ranks / the slowest rank's device time. (value, max ms)."""
+    tot_ms = allreduce_max(ms_local, ws)
+    units = allreduce_sum(units_local, ws)
+    return units / (tot_ms / 1000.0), tot_ms
+
+
 def barrier(ws):
     if ws > 1:
         import torch.distributed as dist
@@ -177,13 +184,94 @@ def cpu_oracle_rate(ps, target_s=15.0):
     return n / dt, dict(pairs=n, seconds=dt, parcels=sub.n, box_deg=w, threads=os.cpu_count())
 
 
+SERVE_RATE, SERVE_REQUESTS, SERVE_WARMUP = 50.0, 500, 50
+SERVE_SIZES = (1e2, 1e5)   # query geometries per request, log-uniform
+
+
+def serving_schedule(rng, qpoly, qpts):
+    """Poisson arrivals at SERVE_RATE; ops: intersects+area 50%, relate 20%, dwithin 5 m 20%, point in polygon 10%."""
+    lines, t = [], 0.0
+    for _ in range(SERVE_REQUESTS):
+        t += rng.exponential(1.0 / SERVE_RATE)
+        u = rng.random()
+        if u < 0.5:
+            lines.append(f"{t:.6f}\tJOIN\t{rng.choice(qpoly)}\tresident\t1\tall")
+        elif u < 0.7:
+            lines.append(f"{t:.6f}\tRELATE\t{rng.choice(qpoly)}\tresident\t\tall")
+        elif u < 0.9:
+            lines.append(f"{t:.6f}\tDWITHIN\t{rng.choice(qpoly)}\tresident\tdwithin\t5\t0\tall")
+        else:
+            lines.append(f"{t:.6f}\tJOIN\t{rng.choice(qpts)}\tresident\t0\tall")
+    return "\n".join(lines) + "\n"
+
+
+def serving_leg(ps, n_points=1_000_000, workers=4):
+    """gsjd serving a Poisson request stream against the resident layer, filtered and plain refinement."""
+    import shutil
+    import tempfile
+    from gsj import client as C
+    from gsj import daemon as D
+    from gsj import gen
+    from gsj._build import lib_path
+    d = tempfile.mkdtemp(prefix="gsjd_bench_")
+    try:
+        t0 = time.time()
+        gen.write_gset(os.path.join(d, "resident.gset"), ps)
+        rng = np.random.default_rng(42)
+        density = ps.n / ((BOX[2] - BOX[0]) * (BOX[3] - BOX[1]))
+        qpoly, qpts, qsizes = [], [], []
+        for i in range(32):
+            n = int(np.exp(rng.uniform(np.log(SERVE_SIZES[0]), np.log(SERVE_SIZES[1]))))
+            side = min(BOX[2] - BOX[0], (n / density) ** 0.5)
+            x0 = rng.uniform(BOX[0], BOX[2] - side)
+            y0 = rng.uniform(BOX[1], BOX[3] - side)
+            box = (x0, y0, x0 + side, y0 + side)
+            if i < 24:
+                gen.write_gset(os.path.join(d, f"q{i}.gset"), gen.layer_parcels(max(n, 4), box, seed=1000 + i))
+                qpoly.append(f"q{i}")
+            else:
+                gen.write_pset(os.path.join(d, f"t{i}.pset"), gen.points(n, box, 1000 + i))
+                qpts.append(f"t{i}")
+            qsizes.append(n)
+        sched = os.path.join(d, "schedule.tsv")
+        open(sched, "w").write(serving_schedule(rng, qpoly, qpts))
+        prep_s = time.time() - t0
+        out = {}
+        for mode in ("filtered", "plain"):
+            sock = os.path.join(d, f"gsjd_{mode}.sock")
+            log = open(os.path.join(d, f"gsjd_{mode}.log"), "w")
+            p = D.start(sock, d, workers=workers, threads=max(4, (os.cpu_count() or 8) // 2), log=log, extra=["--refine", mode])
+            try:
+                cl = C.Client(sock)
+                cl.load("resident", "resident.gset", dedup=False)
+                for q in qpoly:
+                    cl.load(q, q + ".gset", dedup=False)
+                for q in qpts:
+                    cl.load(q, q + ".pset")
+                r = subprocess.run([lib_path("gsjd_loadgen"), "--socket", sock, "--schedule", sched, "--warmup", str(SERVE_WARMUP)],
+                                   capture_output=True, text=True, timeout=900)
+                res = json.loads(r.stdout.strip().splitlines()[-1])
+                res["rows_per_s"] = res["rows"] / res["span_s"]
+                out[mode] = res
+            finally:
+                D.stop(p)
+                log.close()
+        out["config"] = {"resident_parcels": int(ps.n), "rate_per_s": SERVE_RATE, "requests": SERVE_REQUESTS, "warmup_requests": SERVE_WARMUP,
+                         "query_sizes": "log-uniform 1e2-1e5", "mix": "join+area 50%, relate 20%, dwithin 5 m 20%, pip 10%",
+                         "workers": workers, "prep_s": round(prep_s, 1)}
+        return out
+    finally:
+        shutil.rmtree(d, ignore_errors=True)
+
+
 def run_reference(args, rank, ws):
     """--impl reference: the CPU FP64 port of the reference's predicates, timed on the host cores."""
     from gsj import gen
     if rank != 0:
         return
     ps = gen.layer_parcels(args.seeds, BOX, seed=0)
-    S, sub, w = cpu_sample(ps, target_s=max(4.0, min(15.0, 90.0 / max(1, args.steps + args.warmup))))
+    target = args.cpu_sample_s or max(4.0, min(15.0, 90.0 / max(1, args.steps + args.warmup)))
+    S, sub, w = cpu_sample(ps, target_s=target)
     runs = [cpu_time(S) for _ in range(args.warmup + args.steps)][args.warmup:]
     n = runs[0][0]
     secs = float(np.sum([r[1] for r in runs]))
@@ -206,6 +294,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--seeds", type=int, default=N_SEEDS)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-sample-s", type=float, default=0.0, help="CPU seconds per reference-arm step (0: sized from --steps)")
+    ap.add_argument("--no-serve", action="store_true", help="skip the serving-latency leg (gsjd under a Poisson request stream)")
     args = ap.parse_args()
     rank, local, ws = dist_setup()
     if args.impl == "reference":
@@ -274,13 +364,9 @@ def main():
     d2h = int(len(r.pairs) * 12)
 
     f = res["filtered"]
-    tot_ms = allreduce_max(float(np.sum(f["ms"])), ws)
-    all_pairs = allreduce_sum(float(f["pairs"]), ws)
-    value = all_pairs / (tot_ms / 1000.0)
-    plain_ms = allreduce_max(float(np.sum(res["plain"]["ms"])), ws)
-    plain_value = allreduce_sum(float(res["plain"]["pairs"]), ws) / (plain_ms / 1000.0)
-    e2e_tot = allreduce_max(float(np.sum(e2e_ms)), ws)
-    e2e_value = allreduce_sum(float(e2e_pairs), ws) / (e2e_tot / 1000.0)
+    value, tot_ms = aggregate(float(np.sum(f["ms"])), float(f["pairs"]), ws)
+    plain_value, plain_ms = aggregate(float(np.sum(res["plain"]["ms"])), float(res["plain"]["pairs"]), ws)
+    e2e_value, e2e_tot = aggregate(float(np.sum(e2e_ms)), float(e2e_pairs), ws)
     pk = peaks()
     # roofline of the dominant kernel (refinement): algorithmic bytes = both geometries' vertices per candidate pair
     cand = eng.candidates(L, L, upper=True)
@@ -307,6 +393,9 @@ def main():
                "sample": f"CPU FP64 oracle, relate self-join of {info['parcels']} parcels in a {info['box_deg']:.3f} deg corner sub-box "
                          f"({info['pairs']} pairs, {info['seconds']:.1f} s)"}
     lat = sorted(f["ms"])
+    serving = None
+    if rank == 0 and not args.no_serve:
+        serving = serving_leg(ps)
     line = {
         "metric": METRIC, "value": value, "unit": "pairs/s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": tot_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
@@ -314,7 +403,10 @@ def main():
         "config": {"workload": WORKLOAD, "parcels": int(L.info["n"]), "vertices": int(L.info["nv"]), "candidates": int(st[0]["candidates"]),
                    "pairs_per_step": int(st[0]["hits"]), "parallelism": f"replicas x{ws} (own layer per rank)",
                    "l2": "inputs > L2 (2.2 GB resident layer)", "gen_s": round(t_gen, 2)},
-        "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
+        "latency_ms": ({"p50": serving["filtered"]["p50_ms"], "p99": serving["filtered"]["p99_ms"],
+                        "what": "gsjd serving, arrival to end of result stream"} if serving else None),
+        "step_latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
+        "serving": serving,
         "plain_fp64": {"value": plain_value, "ms_per_step": plain_ms / args.steps,
                        "latency_ms": {"p50": float(np.percentile(res["plain"]["ms"], 50)), "p99": float(np.percentile(res["plain"]["ms"], 99))},
                        "speedup_filtered": value / plain_value},

@@ -5,8 +5,9 @@
 //  - layers come from files (binary COPY / .gset / .pset, resolved inside --data-dir) instead of SQL over libpq;
 //    LOAD_QUERY and LOAD's row filter need PostgreSQL and answer with an error;
 //  - GPU work runs on a pool of engine contexts (--workers, each its own CUDA stream and scratch) sharing the
-//    resident layers, so small requests overlap on the GPU instead of queueing behind one device lock
-//    (g_gpu, gpujoind.cu:35); admission is first come, first served.
+//    resident layers, so requests that arrive while others run are admitted and overlap on the GPU instead of
+//    queueing behind one device lock (g_gpu, gpujoind.cu:35). Admission is first come, first served, as a context
+//    and the request's scratch-memory estimate (within --mem-budget-gb) become free.
 #include <arpa/inet.h>
 #include <netinet/in.h>
 #include <netinet/tcp.h>
@@ -54,6 +55,8 @@ double secs_since(Clock::time_point t) { return std::chrono::duration<double>(Cl
 struct Config {
   std::string socket = "/tmp/gpujoind.sock", tcp, token, data_dir = ".";
   int device = 0, workers = 2, threads = 16;
+  int refine_mode = GSJ_REFINE_FILTERED;
+  double mem_budget_gb = 0;   // scratch budget shared by running requests (0: half of the free memory at first use)
 };
 Config g_cfg;
 std::atomic<bool> g_stop{false};
@@ -103,15 +106,18 @@ class Json {
   bool first_ = true;
 };
 
-// ---- engine contexts ---------------------------------------------------------------------------------------------
+// ---- engine contexts and admission ------------------------------------------------------------------------------
 // A fixed pool of contexts on one device, created on first use (the daemon starts without touching the GPU).
-// Waiters are served in arrival order.
+// A request is admitted in arrival order once a context is free and its scratch estimate fits in the budget
+// beside the running requests (a request larger than the whole budget runs alone).
 class GpuPool {
  public:
-  gsj_ctx* acquire() {
+  gsj_ctx* acquire(uint64_t est) {
     std::unique_lock<std::mutex> lk(m_);
     const uint64_t ticket = next_++;
-    cv_.wait(lk, [&] { return ticket == serving_ && (!free_.empty() || created_ < g_cfg.workers); });
+    cv_.wait(lk, [&] {
+      return ticket == serving_ && (!free_.empty() || created_ < g_cfg.workers) && (busy_ == 0 || budget_ == 0 || used_ + est <= budget_);
+    });
     serving_++;
     gsj_ctx* c = nullptr;
     if (!free_.empty()) { c = free_.back(); free_.pop_back(); }
@@ -122,21 +128,31 @@ class GpuPool {
         throw std::runtime_error("no usable CUDA device " + std::to_string(g_cfg.device) + " (gsj_ctx_create: " + std::to_string(rc) + ")");
       }
       created_++;
+      if (!budget_set_) {
+        uint64_t fr = 0, tot = 0;
+        gsj_ctx_mem_info(c, &fr, &tot, nullptr);
+        budget_ = g_cfg.mem_budget_gb > 0 ? (uint64_t)(g_cfg.mem_budget_gb * 1073741824.0) : fr / 2;
+        budget_set_ = true;
+      }
     }
     busy_++;
+    used_ += est;
     cv_.notify_all();
     return c;
   }
-  void release(gsj_ctx* c) {
+  void release(gsj_ctx* c, uint64_t est) {
     std::lock_guard<std::mutex> lk(m_);
     free_.push_back(c);
     busy_--;
+    used_ -= est;
     cv_.notify_all();
   }
-  void counts(int* busy, uint64_t* queued) {
+  void counts(int* busy, uint64_t* queued, uint64_t* used, uint64_t* budget) {
     std::lock_guard<std::mutex> lk(m_);
     *busy = busy_;
     *queued = next_ - serving_;
+    *used = used_;
+    *budget = budget_;
   }
 
  private:
@@ -144,19 +160,21 @@ class GpuPool {
   std::condition_variable cv_;
   std::vector<gsj_ctx*> free_;
   int created_ = 0, busy_ = 0;
-  uint64_t next_ = 0, serving_ = 0;
+  uint64_t next_ = 0, serving_ = 0, used_ = 0, budget_ = 0;
+  bool budget_set_ = false;
 };
 GpuPool g_pool;
 
 class Lease {
  public:
-  Lease() : c_(g_pool.acquire()) {}
-  ~Lease() { g_pool.release(c_); }
+  explicit Lease(uint64_t est = 0) : est_(est), c_(g_pool.acquire(est)) {}
+  ~Lease() { g_pool.release(c_, est_); }
   gsj_ctx* get() const { return c_; }
   Lease(const Lease&) = delete;
   Lease& operator=(const Lease&) = delete;
 
  private:
+  uint64_t est_;
   gsj_ctx* c_;
 };
 
@@ -186,6 +204,14 @@ struct Layer {
         .num("upload_s", upload_s).done();
   }
 };
+
+// Scratch estimate of a join of probe layer P against build layer R: candidate pairs (one 8-byte pair, the
+// refinement outputs and the compaction buffers, ~96 bytes each) at ~24 candidates per probe geometry, plus the
+// per-call fixed buffers. Generous on purpose: it only orders admission.
+uint64_t scratch_estimate(const Layer& P, const Layer& R) {
+  (void)R;
+  return (64ull << 20) + P.gpu_geoms * 24ull * 96ull;
+}
 
 std::mutex g_reg;
 std::map<std::string, std::shared_ptr<Layer>> g_layers;
@@ -435,13 +461,14 @@ void op_join(Conn& c, const std::vector<std::string>& a) {
   if (A->points() && B->points()) throw std::runtime_error("point x point joins are not supported");
   bool swapped = false;
   if (!A->points() && B->points()) { std::swap(A, B); swapped = true; }   // run as point x polygon
-  Lease lease;
+  Lease lease(scratch_estimate(*A, *B));
   gsj_ctx* ctx = lease.get();
   c.u32(GSP_OK);
   c.streaming = true;
   gsj_join_opts o;
   gsj_join_opts_default(&o);
   o.cancel = &c.broken;
+  o.refine_mode = g_cfg.refine_mode;
   const auto t0 = Clock::now();
   JoinRun J{&c, A.get(), B.get(), swapped ? B.get() : A.get(), swapped ? A.get() : B.get(), same, distinct, want_area, stats_only, swapped};
   gsj_join_stats st{};
@@ -470,12 +497,13 @@ void op_cluster(Conn& c, const std::vector<std::string>& a) {
   if (a.empty()) throw std::runtime_error("CLUSTER needs layer");
   auto L = get_layer(a[0]);
   if (L->points()) throw std::runtime_error("cluster needs a polygon layer");
-  Lease lease;
+  Lease lease(scratch_estimate(*L, *L));
   gsj_ctx* ctx = lease.get();
   const auto t0 = Clock::now();
   gsj_join_opts o;
   gsj_join_opts_default(&o);
   o.cancel = &c.broken;
+  o.refine_mode = g_cfg.refine_mode;
   std::vector<uint32_t> root(L->n_distinct);
   gsj_join_stats st{};
   check(ctx, gsj_cluster(ctx, L->h, (uint32_t)L->n_distinct, &o, root.data(), &st), "cluster");
@@ -557,13 +585,14 @@ void op_relate(Conn& c, const std::vector<std::string>& a) {
   if (A->points() && B->points()) throw std::runtime_error("point x point relate is not supported");
   bool swapped = false;
   if (!A->points() && B->points()) { std::swap(A, B); swapped = true; }
-  Lease lease;
+  Lease lease(scratch_estimate(*A, *B));
   gsj_ctx* ctx = lease.get();
   c.u32(GSP_OK);
   c.streaming = true;
   gsj_join_opts o;
   gsj_join_opts_default(&o);
   o.cancel = &c.broken;
+  o.refine_mode = g_cfg.refine_mode;
   const auto t0 = Clock::now();
   RelateRun R{&c, A.get(), B.get(), same, distinct, swapped, pat};
   gsj_join_stats st{};
@@ -657,13 +686,14 @@ void op_dwithin(Conn& c, const std::vector<std::string>& a) {
   bool swapped = false;
   if (!A->points() && B->points()) { std::swap(A, B); std::swap(ra, rb); swapped = true; }
   if (A->points() && erode && ra > 0) throw std::runtime_error("a point layer cannot have a negative buffer");
-  Lease lease;
+  Lease lease(scratch_estimate(*A, *B));
   gsj_ctx* ctx = lease.get();
   c.u32(GSP_OK);
   c.streaming = true;
   gsj_join_opts o;
   gsj_join_opts_default(&o);
   o.cancel = &c.broken;
+  o.refine_mode = g_cfg.refine_mode;
   const auto t0 = Clock::now();
   PairsRun P{&c, A.get(), B.get(), swapped ? B.get() : A.get(), swapped ? A.get() : B.get(), same, distinct, stats_only, swapped};
   gsj_join_stats st{};
@@ -709,11 +739,12 @@ std::string op_status() {   // gpujoind.cu:486-494 (+ the worker pool)
   const int rc = gsj_device_query(g_cfg.device, name, sizeof name, &ma, &mi, &fr, &tot);
   if (rc) throw std::runtime_error("no usable CUDA device " + std::to_string(g_cfg.device));
   int busy = 0;
-  uint64_t queued = 0;
-  g_pool.counts(&busy, &queued);
+  uint64_t queued = 0, used = 0, budget = 0;
+  g_pool.counts(&busy, &queued, &used, &budget);
   return Json().str("device", name).str("cc", std::to_string(ma) + "." + std::to_string(mi)).num("mem_total_mb", tot / 1048576.0)
       .num("mem_free_mb", fr / 1048576.0).key("layers").raw(layer_names()).u64("workers", (uint64_t)g_cfg.workers)
-      .u64("busy", (uint64_t)busy).u64("queued", queued).done();
+      .u64("busy", (uint64_t)busy).u64("queued", queued).num("scratch_used_mb", used / 1048576.0).num("scratch_budget_mb", budget / 1048576.0)
+      .str("refine", g_cfg.refine_mode == GSJ_REFINE_PLAIN ? "plain" : "filtered").done();
 }
 
 std::string op_list() {
@@ -831,7 +862,8 @@ void on_signal(int) { g_stop = true; }
 
 const char* kUsage =
     "usage: gsjd [--socket PATH] [--tcp HOST:PORT] [--token-file FILE] [--data-dir DIR] [--device N] [--workers N]\n"
-    "            [--threads N] [--conninfo STR (accepted, unused: layers load from files)]\n";
+    "            [--threads N] [--mem-budget-gb G] [--refine plain|filtered]\n"
+    "            [--conninfo STR (accepted, unused: layers load from files)]\n";
 
 }  // namespace
 }  // namespace gsjd
@@ -847,6 +879,12 @@ extern "C" int gsjd_main(int argc, char** argv) {
     else if (a == "--device" && has) g_cfg.device = atoi(argv[++i]);
     else if (a == "--workers" && has) g_cfg.workers = std::max(1, atoi(argv[++i]));
     else if (a == "--threads" && has) g_cfg.threads = std::max(1, atoi(argv[++i]));
+    else if (a == "--mem-budget-gb" && has) g_cfg.mem_budget_gb = atof(argv[++i]);
+    else if (a == "--refine" && has) {
+      const std::string m = argv[++i];
+      if (m != "plain" && m != "filtered") { fputs("--refine plain|filtered\n", stderr); return 1; }
+      g_cfg.refine_mode = m == "plain" ? GSJ_REFINE_PLAIN : GSJ_REFINE_FILTERED;
+    }
     else if (a == "--conninfo" && has) ++i;
     else if (a == "--token-file" && has) {
       std::ifstream tf(argv[++i]);
