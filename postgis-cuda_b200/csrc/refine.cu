@@ -31,10 +31,83 @@ constexpr size_t RB_SMEM_F = (size_t)RB_WARPS * 2 * LIST_BYTES_F;
 
 struct PairGeo { Box ov; double tol, eps_par, snap, cx, cy; };
 
-// Green's-theorem contribution of edge p->q within the other polygon + relate lengths (engine.cuh:416-515)
-template <bool F>
-__device__ double edge_contrib(double px, double py, double qx, double qy, const EList& L, int cnt, bool in_c, const PairGeo& G, bool real,
-                               double* l_in, double* l_on, uint32_t* bits, uint32_t cut) {
+// Candidate edge pairs of the filtered variant: every (i, j) of A's and B's local edges whose boxes come within
+// 2 tol of each other - a superset of the pairs any box test of the pair routine keeps (those use tol or no pad).
+// Built by one lane-balanced sweep over the na x nb grid (ballot compaction keeps (i, j) order); per-edge
+// ranges: A edge i owns cp[sa[i] .. sa[i+1]), B edge j owns pj[(j ? sb[j-1] : 0) .. sb[j]) (entries in i order).
+constexpr int CPCAP = 1024;
+struct FlatBuf { uint32_t* cp; uint16_t* pj; uint32_t* sa; uint32_t* sb; };
+constexpr size_t FLAT_BYTES = CPCAP * sizeof(uint32_t) + CPCAP * sizeof(uint16_t) + 2 * (CAP_F + 1) * sizeof(uint32_t);
+
+__device__ __forceinline__ void warp_exscan(uint32_t* a, int n, int lane) {   // in place over a[0 .. n)
+  uint32_t run = 0;
+  for (int base = 0; base < n; base += 32) {
+    const int t = base + lane;
+    const uint32_t v = t < n ? a[t] : 0u;
+    uint32_t x = v;
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= o) x += y;
+    }
+    if (t < n) a[t] = run + x - v;
+    run += __shfl_sync(0xffffffffu, x, 31);
+  }
+  __syncwarp();
+}
+
+// returns the number of candidate pairs (> CPCAP: the lists were not kept)
+__device__ int flat_candidates(const EList& LA, int na, const EList& LB, int nb, double pad, const FlatBuf& fb, int lane) {
+  for (int t = lane; t <= na; t += 32) fb.sa[t] = 0;
+  for (int t = lane; t <= nb; t += 32) fb.sb[t] = 0;
+  __syncwarp();
+  if (na == 0 || nb == 0) return 0;
+  const unsigned lt = (1u << lane) - 1;
+  const int total = na * nb;
+  const int qi = 32 / nb, qj = 32 % nb;
+  int i = lane / nb, j = lane % nb, cnt = 0;
+  for (int base = 0; base < total; base += 32) {
+    bool keep = false;
+    if (base + lane < total) {
+      const double px = LA.x0[i], py = LA.y0[i], qx = LA.x1[i], qy = LA.y1[i];
+      const double ax0 = (px < qx ? px : qx) - pad, ax1 = (px < qx ? qx : px) + pad;
+      const double ay0 = (py < qy ? py : qy) - pad, ay1 = (py < qy ? qy : py) + pad;
+      keep = !out_cmp(LB.x0[j], LB.y0[j], LB.x1[j], LB.y1[j], ax0, ay0, ax1, ay1);
+    }
+    const unsigned m = __ballot_sync(0xffffffffu, keep);
+    const int pos = cnt + __popc(m & lt);
+    if (keep && pos < CPCAP) {
+      fb.cp[pos] = (uint32_t)i | ((uint32_t)j << 16);
+      atomicAdd(&fb.sa[i], 1u);
+      atomicAdd(&fb.sb[j], 1u);
+    }
+    cnt += __popc(m);
+    i += qi; j += qj;
+    if (j >= nb) { j -= nb; i++; }
+  }
+  if (cnt > CPCAP) return cnt;
+  __syncwarp();
+  warp_exscan(fb.sa, na + 1, lane);
+  warp_exscan(fb.sb, nb + 1, lane);
+  // stable scatter by j: entries of one B edge keep their (increasing i) order
+  for (int base = 0; base < cnt; base += 32) {
+    const int e = base + lane;
+    const bool v = e < cnt;
+    const uint32_t jj = v ? (fb.cp[e] >> 16) : 0xFFFFFu;
+    const unsigned peers = __match_any_sync(0xffffffffu, jj);
+    if (v) fb.pj[fb.sb[jj] + __popc(peers & lt)] = (uint16_t)e;
+    __syncwarp();
+    if (v && (peers & lt) == 0) fb.sb[jj] += __popc(peers);
+    __syncwarp();
+  }
+  return cnt;
+}
+
+// Green's-theorem contribution of edge p->q within the other polygon + relate lengths (engine.cuh:416-515).
+// each_k(visit) calls visit(k) for the other polygon's local edges k in increasing order: all of them, or only
+// those of a candidate list that holds every k passing the box test below (the same visits, the same results).
+template <bool F, class EachK>
+__device__ double edge_contrib_k(double px, double py, double qx, double qy, const EList& L, int cnt, bool in_c, const PairGeo& G, bool real,
+                                 double* l_in, double* l_on, uint32_t* bits, uint32_t cut, EachK&& each_k) {
   const double dx = qx - px, dy = qy - py;
   const double len2 = dx * dx + dy * dy;
   if (len2 == 0) return 0.0;
@@ -77,7 +150,7 @@ __device__ double edge_contrib(double px, double py, double qx, double qy, const
     }
     return false;
   };
-  for (int k = 0; k < cnt; k++) visit(k);
+  each_k(visit);
   for (int a = 1; a < ns; a++) { double v = ts[a]; int b = a - 1; while (b >= 0 && ts[b] > v) { ts[b + 1] = ts[b]; b--; } ts[b + 1] = v; }
   double acc = 0.0;
   for (int k = 0; k + 1 < ns; k++) {
@@ -125,6 +198,14 @@ __device__ double edge_contrib(double px, double py, double qx, double qy, const
   return acc;
 }
 
+template <bool F>
+__device__ __forceinline__ double edge_contrib(double px, double py, double qx, double qy, const EList& L, int cnt, bool in_c, const PairGeo& G,
+                                               bool real, double* l_in, double* l_on, uint32_t* bits, uint32_t cut) {
+  return edge_contrib_k<F>(px, py, qx, qy, L, cnt, in_c, G, real, l_in, l_on, bits, cut, [&](auto&& visit) {
+    for (int k = 0; k < cnt; k++) visit(k);
+  });
+}
+
 __device__ __forceinline__ double pair_snap(double2 oa, double2 ea) {   // engine.cuh:524-527
   double m = fmax(fmax(fabs(oa.x), fabs(oa.x + ea.x)), fmax(fabs(oa.y), fabs(oa.y + ea.y)));
   return 0.5 * (nextafter(m, INFINITY) - m);
@@ -133,7 +214,7 @@ __device__ __forceinline__ double pair_snap(double2 oa, double2 ea) {   // engin
 // One pair, whole warp. Returns false when a local list exceeded cap (nothing written).
 template <bool F>
 __device__ bool refine_pair_t(const DLayer& P, const DLayer& R, uint32_t a, uint32_t b, const RefineArgs& rp, EList LA, EList LB, int cap,
-                              int lane, uint8_t& o_flag, double& o_area, double4& o_ev, uint32_t& o_evb) {
+                              int lane, uint8_t& o_flag, double& o_area, double4& o_ev, uint32_t& o_evb, const FlatBuf* fb = nullptr) {
   const double2 oa = P.origin[a], ob = R.origin[b], ea = P.ext[a], eb = R.ext[b];
   const double sx = ob.x - oa.x, sy = ob.y - oa.y;
   const double pad = 4.0 * fmax(rp.tol_abs, (double)rp.tol_rel * fmax(fmax(ea.x, ea.y), fmax(eb.x, eb.y)));
@@ -147,6 +228,13 @@ __device__ bool refine_pair_t(const DLayer& P, const DLayer& R, uint32_t a, uint
   const int nb = collect<F>(B, G.ov, LB, cap, lane);
   if (na > cap || nb > cap) return false;
   __syncwarp();
+  int ncp = -1;   // candidate edge pairs (filtered variant); -1: sweep every edge pair
+  if constexpr (F) {
+    if (fb) {
+      ncp = flat_candidates(LA, na, LB, nb, 2.0 * G.tol, *fb, lane);
+      if (ncp > CPCAP) ncp = -1;
+    }
+  }
   // boundary contact
   bool hit = false, hit_any = false;
   auto seg_loop = [&](int i) {
@@ -165,7 +253,26 @@ __device__ bool refine_pair_t(const DLayer& P, const DLayer& R, uint32_t a, uint
     };
     for (int j = 0; j < nb; j++) if (test(j)) break;
   };
-  for (int i = lane; i < na && !hit; i += 32) seg_loop(i);
+  if (ncp >= 0) {
+    // one candidate per lane; the warp stops at the first real contact (hit_any is then implied)
+    for (int base = 0; base < ncp; base += 32) {
+      const int e = base + lane;
+      if (e < ncp) {
+        const uint32_t c = fb->cp[e];
+        const int i = (int)(c & 0xFFFFu), j = (int)(c >> 16);
+        const double px0 = LA.x0[i], py0 = LA.y0[i], px1 = LA.x1[i], py1 = LA.y1[i];
+        const double qx0 = LB.x0[j], qy0 = LB.y0[j], qx1 = LB.x1[j], qy1 = LB.y1[j];
+        const double ax0 = px0 < px1 ? px0 : px1, ax1 = px0 < px1 ? px1 : px0, ay0 = py0 < py1 ? py0 : py1, ay1 = py0 < py1 ? py1 : py0;
+        if (!out_cmp(qx0, qy0, qx1, qy1, ax0, ay0, ax1, ay1) && seg_isect(px0, py0, px1, py1, qx0, qy0, qx1, qy1)) {
+          hit_any = true;
+          if (!((LA.fl[i] | LB.fl[j]) & 1u)) hit = true;
+        }
+      }
+      if (__any_sync(0xffffffffu, hit)) { hit = true; break; }
+    }
+  } else {
+    for (int i = lane; i < na && !hit; i += 32) seg_loop(i);
+  }
   hit = __any_sync(0xffffffffu, hit);
   hit_any = __any_sync(0xffffffffu, hit_any || hit);
   const bool rtouch = hit;
@@ -215,13 +322,30 @@ __device__ bool refine_pair_t(const DLayer& P, const DLayer& R, uint32_t a, uint
     double s2 = 0.0, ai = 0, ao = 0, bi = 0, bo = 0;
     uint32_t bits = rtouch ? REL_TOUCH : 0;
     const bool rel = rp.want_relate != 0;
-    for (int i = lane; i < na; i += 32) {
-      const uint32_t f = LA.fl[i];
-      s2 += edge_contrib<F>(LA.x0[i], LA.y0[i], LA.x1[i], LA.y1[i], LB, nb, inB_c, G, !(f & 1u), rel ? &ai : nullptr, &ao, &bits, f);
-    }
-    for (int i = lane; i < nb; i += 32) {
-      const uint32_t f = LB.fl[i];
-      s2 += edge_contrib<F>(LB.x0[i], LB.y0[i], LB.x1[i], LB.y1[i], LA, na, inA_c, G, !(f & 1u), rel ? &bi : nullptr, &bo, &bits, f);
+    if (ncp >= 0) {   // visit only each edge's candidates, in the same increasing order
+      const uint32_t* cp = fb->cp;
+      const uint16_t* pj = fb->pj;
+      for (int i = lane; i < na; i += 32) {
+        const uint32_t f = LA.fl[i];
+        const int r0 = (int)fb->sa[i], r1 = (int)fb->sa[i + 1];
+        s2 += edge_contrib_k<F>(LA.x0[i], LA.y0[i], LA.x1[i], LA.y1[i], LB, nb, inB_c, G, !(f & 1u), rel ? &ai : nullptr, &ao, &bits, f,
+                                [&](auto&& visit) { for (int e = r0; e < r1; e++) visit((int)(cp[e] >> 16)); });
+      }
+      for (int j = lane; j < nb; j += 32) {
+        const uint32_t f = LB.fl[j];
+        const int r0 = j ? (int)fb->sb[j - 1] : 0, r1 = (int)fb->sb[j];
+        s2 += edge_contrib_k<F>(LB.x0[j], LB.y0[j], LB.x1[j], LB.y1[j], LA, na, inA_c, G, !(f & 1u), rel ? &bi : nullptr, &bo, &bits, f,
+                                [&](auto&& visit) { for (int e = r0; e < r1; e++) visit((int)(cp[pj[e]] & 0xFFFFu)); });
+      }
+    } else {
+      for (int i = lane; i < na; i += 32) {
+        const uint32_t f = LA.fl[i];
+        s2 += edge_contrib<F>(LA.x0[i], LA.y0[i], LA.x1[i], LA.y1[i], LB, nb, inB_c, G, !(f & 1u), rel ? &ai : nullptr, &ao, &bits, f);
+      }
+      for (int i = lane; i < nb; i += 32) {
+        const uint32_t f = LB.fl[i];
+        s2 += edge_contrib<F>(LB.x0[i], LB.y0[i], LB.x1[i], LB.y1[i], LA, na, inA_c, G, !(f & 1u), rel ? &bi : nullptr, &bo, &bits, f);
+      }
     }
     s2 = warp_sum(s2); ai = warp_sum(ai); ao = warp_sum(ao); bi = warp_sum(bi); bo = warp_sum(bo);
     ar = 0.5 * s2;
@@ -242,7 +366,7 @@ __device__ bool refine_pair(const DLayer& P, const DLayer& R, uint32_t a, uint32
 
 template <bool F> struct Cfg;
 template <> struct Cfg<false> { static constexpr int cap = CAP; static constexpr size_t list = LIST_BYTES, smem = RB_SMEM, edge = EDGE_BYTES; static constexpr int minb = 3; };
-template <> struct Cfg<true> { static constexpr int cap = CAP_F; static constexpr size_t list = LIST_BYTES_F, smem = RB_SMEM_F, edge = EDGE_BYTES_F; static constexpr int minb = 4; };
+template <> struct Cfg<true> { static constexpr int cap = CAP_F; static constexpr size_t list = LIST_BYTES_F, smem = RB_SMEM_F + RB_WARPS * FLAT_BYTES, edge = EDGE_BYTES_F; static constexpr int minb = 3; };
 
 template <bool F>
 __device__ __forceinline__ EList carve_t(unsigned char* base, int cap) { return F ? carve_f(base, cap) : carve(base, cap); }
@@ -255,11 +379,21 @@ __global__ void __launch_bounds__(RB_WARPS * 32, Cfg<F>::minb) k_refine(DLayer P
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   EList LA = carve_t<F>(smem + (size_t)wib * 2 * Cfg<F>::list, Cfg<F>::cap);
   EList LB = carve_t<F>(smem + (size_t)wib * 2 * Cfg<F>::list + Cfg<F>::list, Cfg<F>::cap);
+  FlatBuf fbuf;
+  const FlatBuf* fb = nullptr;
+  if constexpr (F) {   // after the lists of all warps: cp (u32), sa, sb (u32), pj (u16)
+    unsigned char* fbase = smem + (size_t)RB_WARPS * 2 * Cfg<F>::list + (size_t)wib * FLAT_BYTES;
+    fbuf.cp = reinterpret_cast<uint32_t*>(fbase);
+    fbuf.sa = fbuf.cp + CPCAP;
+    fbuf.sb = fbuf.sa + (CAP_F + 1);
+    fbuf.pj = reinterpret_cast<uint16_t*>(fbuf.sb + (CAP_F + 1));
+    fb = &fbuf;
+  }
   const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
   for (uint64_t p = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; p < np; p += nw) {
     const uint2 pr = pairs[p];
     uint8_t f; double ar; double4 e4; uint32_t b4;
-    const bool ok = refine_pair_t<F>(P, R, pr.x, pr.y, rp, LA, LB, Cfg<F>::cap, lane, f, ar, e4, b4);
+    const bool ok = refine_pair_t<F>(P, R, pr.x, pr.y, rp, LA, LB, Cfg<F>::cap, lane, f, ar, e4, b4, fb);
     if (lane == 0) {
       if (!ok) { heavy[atomicAdd(nheavy, 1ull)] = (uint32_t)p; flag[p] = 0; }
       else {
