@@ -166,29 +166,27 @@ __device__ double edge_contrib_k(double px, double py, double qx, double qy, con
         net += sgn; if (first < 0) first = o;
         if (!(L.fl[oidx[o]] & 1u)) { net_real += sgn; n_real++; }
       }
-    int vin = -1;
-    auto inside_m = [&]() {
-      if (vin < 0) vin = (in_ov && inside_from_c<F>(L, cnt, G.cx, G.cy, in_c, mx, my)) ? 1 : 0;
-      return vin;
-    };
-    if (l_in && real) {
+    // the inside test of the midpoint, evaluated once and only where a branch below reads it
+    const bool lens = l_in && real;
+    const bool need = first < 0 || (net != 1 && net != -1) || (lens && net_real == 0 && !(n_real == 0 && (net == 1 || net == -1)));
+    const int vin = (need && in_ov && inside_from_c<F>(L, cnt, G.cx, G.cy, in_c, mx, my)) ? 1 : 0;
+    if (lens) {
       const double seg = sqrt(len2) * (t1 - t0);
       if (net_real != 0) { *l_on += seg; *bits |= (net_real > 0 ? REL_COIN_SAME : REL_COIN_OPP) | REL_TOUCH; }
       else if (n_real == 0 && (net == 1 || net == -1)) *l_in += 0.5 * seg;
-      else if (inside_m()) *l_in += seg;
+      else if (vin) *l_in += seg;
     }
     double w;
-    if (first < 0) w = inside_m() ? 1.0 : 0.0;
+    if (first < 0) w = vin ? 1.0 : 0.0;
     else if (net == 1 || net == -1) w = 0.5;
-    else if (net == 0) w = inside_m() ? 1.0 : 0.0;
+    else if (net == 0) w = vin ? 1.0 : 0.0;
     else {
       const int fo = oidx[first];
       const bool sb = left_of(L.x0[fo], L.y0[fo], L.x1[fo], L.y1[fo], mx, my);
       const bool m_left = osame[first] ? sb : !sb;
-      const int v = inside_m();
-      int other = m_left ? v - net : v + net;
+      int other = m_left ? vin - net : vin + net;
       other = other < 0 ? 0 : (other > 1 ? 1 : other);
-      w = 0.5 * (v + other);
+      w = 0.5 * (vin + other);
     }
     if (w != 0.0) {
       const double ax = px + dx * t0 - G.cx, ay = py + dy * t0 - G.cy, bx = px + dx * t1 - G.cx, by = py + dy * t1 - G.cy;
@@ -212,7 +210,9 @@ __device__ __forceinline__ double pair_snap(double2 oa, double2 ea) {   // engin
 }
 
 // One pair, whole warp. Returns false when a local list exceeded cap (nothing written).
-template <bool F>
+// FLAT (filtered kernel only): the candidate-list path; a pair whose list would exceed CPCAP is handed back
+// (false) like an oversized pair, and the scratch kernel runs it with the full sweeps.
+template <bool F, bool FLAT = false>
 __device__ bool refine_pair_t(const DLayer& P, const DLayer& R, uint32_t a, uint32_t b, const RefineArgs& rp, EList LA, EList LB, int cap,
                               int lane, uint8_t& o_flag, double& o_area, double4& o_ev, uint32_t& o_evb, const FlatBuf* fb = nullptr) {
   const double2 oa = P.origin[a], ob = R.origin[b], ea = P.ext[a], eb = R.ext[b];
@@ -224,16 +224,17 @@ __device__ bool refine_pair_t(const DLayer& P, const DLayer& R, uint32_t a, uint
   G.tol = fmax(rp.tol_abs, (double)rp.tol_rel * fmax(G.ov.x1 - G.ov.x0, G.ov.y1 - G.ov.y0));
   G.eps_par = rp.eps_par;
   G.snap = rp.snap_half_ulp ? pair_snap(oa, ea) : 0.0;
-  const int na = collect<F>(A, G.ov, LA, cap, lane);
-  const int nb = collect<F>(B, G.ov, LB, cap, lane);
+  int na = 0, nb = 0;
+  for (int side = 0; side < 2; side++) {   // one inlined copy of the gather
+    const int n = collect<F>(side ? B : A, G.ov, side ? LB : LA, cap, lane);
+    if (side) nb = n; else na = n;
+  }
   if (na > cap || nb > cap) return false;
   __syncwarp();
-  int ncp = -1;   // candidate edge pairs (filtered variant); -1: sweep every edge pair
-  if constexpr (F) {
-    if (fb) {
-      ncp = flat_candidates(LA, na, LB, nb, 2.0 * G.tol, *fb, lane);
-      if (ncp > CPCAP) ncp = -1;
-    }
+  int ncp = -1;   // candidate edge pairs (FLAT); -1: sweep every edge pair
+  if constexpr (FLAT) {
+    ncp = flat_candidates(LA, na, LB, nb, 2.0 * G.tol, *fb, lane);
+    if (ncp > CPCAP) return false;
   }
   // boundary contact
   bool hit = false, hit_any = false;
@@ -253,7 +254,7 @@ __device__ bool refine_pair_t(const DLayer& P, const DLayer& R, uint32_t a, uint
     };
     for (int j = 0; j < nb; j++) if (test(j)) break;
   };
-  if (ncp >= 0) {
+  if constexpr (FLAT) {
     // one candidate per lane; the warp stops at the first real contact (hit_any is then implied)
     for (int base = 0; base < ncp; base += 32) {
       const int e = base + lane;
@@ -279,7 +280,11 @@ __device__ bool refine_pair_t(const DLayer& P, const DLayer& R, uint32_t a, uint
   G.cx = (double)(G.ov.x0 + 0.381966 * (G.ov.x1 - G.ov.x0));
   G.cy = (double)(G.ov.y0 + 0.414213 * (G.ov.y1 - G.ov.y0));
   bool inB_c = false, inA_c = false;
-  if (!hit || rp.want_area || rp.want_relate) { inB_c = pip_full_warp(B, G.cx, G.cy, lane); inA_c = pip_full_warp(A, G.cx, G.cy, lane); }
+  if (!hit || rp.want_area || rp.want_relate)
+    for (int side = 0; side < 2; side++) {
+      const bool in = pip_full_warp(side ? A : B, G.cx, G.cy, lane);
+      if (side) inA_c = in; else inB_c = in;
+    }
   bool contain_any = false;
   if (!hit) {
     // no real boundary contact: intersects iff a real-edge vertex of one lies inside the other (engine.cuh:577-594)
@@ -322,20 +327,25 @@ __device__ bool refine_pair_t(const DLayer& P, const DLayer& R, uint32_t a, uint
     double s2 = 0.0, ai = 0, ao = 0, bi = 0, bo = 0;
     uint32_t bits = rtouch ? REL_TOUCH : 0;
     const bool rel = rp.want_relate != 0;
-    if (ncp >= 0) {   // visit only each edge's candidates, in the same increasing order
+    if constexpr (FLAT) {   // visit only each edge's candidates, in the same increasing order; one call site for both passes
       const uint32_t* cp = fb->cp;
       const uint16_t* pj = fb->pj;
-      for (int i = lane; i < na; i += 32) {
-        const uint32_t f = LA.fl[i];
-        const int r0 = (int)fb->sa[i], r1 = (int)fb->sa[i + 1];
-        s2 += edge_contrib_k<F>(LA.x0[i], LA.y0[i], LA.x1[i], LA.y1[i], LB, nb, inB_c, G, !(f & 1u), rel ? &ai : nullptr, &ao, &bits, f,
-                                [&](auto&& visit) { for (int e = r0; e < r1; e++) visit((int)(cp[e] >> 16)); });
-      }
-      for (int j = lane; j < nb; j += 32) {
-        const uint32_t f = LB.fl[j];
-        const int r0 = j ? (int)fb->sb[j - 1] : 0, r1 = (int)fb->sb[j];
-        s2 += edge_contrib_k<F>(LB.x0[j], LB.y0[j], LB.x1[j], LB.y1[j], LA, na, inA_c, G, !(f & 1u), rel ? &bi : nullptr, &bo, &bits, f,
-                                [&](auto&& visit) { for (int e = r0; e < r1; e++) visit((int)(cp[pj[e]] & 0xFFFFu)); });
+      for (int pass = 0; pass < 2; pass++) {
+        const EList& LS = pass ? LB : LA;
+        const EList& LO = pass ? LA : LB;
+        const int nself = pass ? nb : na, nother = pass ? na : nb;
+        const bool inc = pass ? inA_c : inB_c;
+        double lin = 0.0, lon = 0.0;   // this pass's lengths (each starts from 0, so the sums are the same)
+        for (int i = lane; i < nself; i += 32) {
+          const uint32_t f = LS.fl[i];
+          const int r0 = pass ? (i ? (int)fb->sb[i - 1] : 0) : (int)fb->sa[i];
+          const int r1 = pass ? (int)fb->sb[i] : (int)fb->sa[i + 1];
+          s2 += edge_contrib_k<F>(LS.x0[i], LS.y0[i], LS.x1[i], LS.y1[i], LO, nother, inc, G, !(f & 1u), rel ? &lin : nullptr, &lon, &bits, f,
+                                  [&](auto&& visit) {
+                                    for (int e = r0; e < r1; e++) visit(pass ? (int)(cp[pj[e]] & 0xFFFFu) : (int)(cp[e] >> 16));
+                                  });
+        }
+        if (pass) { bi = lin; bo = lon; } else { ai = lin; ao = lon; }
       }
     } else {
       for (int i = lane; i < na; i += 32) {
@@ -393,7 +403,7 @@ __global__ void __launch_bounds__(RB_WARPS * 32, Cfg<F>::minb) k_refine(DLayer P
   for (uint64_t p = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; p < np; p += nw) {
     const uint2 pr = pairs[p];
     uint8_t f; double ar; double4 e4; uint32_t b4;
-    const bool ok = refine_pair_t<F>(P, R, pr.x, pr.y, rp, LA, LB, Cfg<F>::cap, lane, f, ar, e4, b4, fb);
+    const bool ok = refine_pair_t<F, F>(P, R, pr.x, pr.y, rp, LA, LB, Cfg<F>::cap, lane, f, ar, e4, b4, fb);
     if (lane == 0) {
       if (!ok) { heavy[atomicAdd(nheavy, 1ull)] = (uint32_t)p; flag[p] = 0; }
       else {
