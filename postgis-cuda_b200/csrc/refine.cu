@@ -36,8 +36,14 @@ struct PairGeo { Box ov; double tol, eps_par, snap, cx, cy; };
 // Built by one lane-balanced sweep over the na x nb grid (ballot compaction keeps (i, j) order); per-edge
 // ranges: A edge i owns cp[sa[i] .. sa[i+1]), B edge j owns pj[(j ? sb[j-1] : 0) .. sb[j]) (entries in i order).
 constexpr int CPCAP = 1024;
-struct FlatBuf { uint32_t* cp; uint16_t* pj; uint32_t* sa; uint32_t* sb; };
-constexpr size_t FLAT_BYTES = CPCAP * sizeof(uint32_t) + CPCAP * sizeof(uint16_t) + 2 * (CAP_F + 1) * sizeof(uint32_t);
+// Large grids are searched by buckets instead: NBK slabs along the overlap box's longer side, B's edges listed per
+// slab (bl, boff), each lane scanning only its A edge's slabs and reporting a pair once, in the first slab both
+// edges reach; the lane sorts its few candidates (at most LCAP) so the list keeps (i, j) order.
+constexpr int NBK = 16, BLCAP = 512, LCAP = 32;
+constexpr int GRID_MAX = 2048;   // na x nb up to this: the grid sweep
+struct FlatBuf { uint32_t* cp; uint16_t* pj; uint32_t* sa; uint32_t* sb; uint32_t* bl; uint32_t* boff; int cap, blcap; };   // cap: entries of cp / pj
+constexpr size_t FLAT_BYTES = (CPCAP * sizeof(uint32_t) + CPCAP * sizeof(uint16_t) + 2 * (CAP_F + 1) * sizeof(uint32_t) + BLCAP * sizeof(uint32_t) +
+                               (NBK + 1) * sizeof(uint32_t) + 15) & ~(size_t)15;
 
 __device__ __forceinline__ void warp_exscan(uint32_t* a, int n, int lane) {   // in place over a[0 .. n)
   uint32_t run = 0;
@@ -55,16 +61,109 @@ __device__ __forceinline__ void warp_exscan(uint32_t* a, int n, int lane) {   //
   __syncwarp();
 }
 
-// returns the number of candidate pairs (> CPCAP: the lists were not kept)
-__device__ int flat_candidates(const EList& LA, int na, const EList& LB, int nb, double pad, const FlatBuf& fb, int lane) {
+// Bucketed search (large grids): fills cp in (i, j) order with the per-edge counts in sa / sb and returns the
+// number of candidates, or -1 when a bucket list or a lane's candidate buffer would overflow.
+__device__ int bucket_candidates(const EList& LA, int na, const EList& LB, int nb, double pad, const Box& ov, const FlatBuf& fb, int lane) {
+  const bool ax = (ov.x1 - ov.x0) >= (ov.y1 - ov.y0);
+  const double o0 = ax ? ov.x0 : ov.y0, len = ax ? ov.x1 - ov.x0 : ov.y1 - ov.y0;
+  const double inv = len > 0 ? NBK / len : 0.0;
+  auto bk = [&](double v) {   // monotone in v
+    const double t = (v - o0) * inv;
+    return t < 1.0 ? 0 : (t >= (double)(NBK - 1) ? NBK - 1 : (int)t);
+  };
+  const unsigned lt = (1u << lane) - 1;
+  if (lane <= NBK) fb.boff[lane] = 0;
+  __syncwarp();
+  for (int j = lane; j < nb; j += 32) {   // slab span of each B edge (kept in pj until the scatter)
+    const double c0 = ax ? LB.x0[j] : LB.y0[j], c1 = ax ? LB.x1[j] : LB.y1[j];
+    const int s0 = bk(c0 < c1 ? c0 : c1), s1 = bk(c0 < c1 ? c1 : c0);
+    fb.pj[j] = (uint16_t)(s0 | (s1 << 8));
+    for (int b2 = s0; b2 <= s1; b2++) atomicAdd(&fb.boff[b2], 1u);
+  }
+  __syncwarp();
+  warp_exscan(fb.boff, NBK + 1, lane);
+  if ((int)fb.boff[NBK] > fb.blcap) return -1;
+  for (int b2 = 0; b2 < NBK; b2++) {   // stable lists: B edges of slab b2 in increasing j
+    int run = 0;
+    for (int j0 = 0; j0 < nb; j0 += 32) {
+      const int j = j0 + lane;
+      int s0 = 0;
+      bool cov = false;
+      if (j < nb) { const uint32_t sp = fb.pj[j]; s0 = (int)(sp & 0xFFu); cov = s0 <= b2 && b2 <= (int)(sp >> 8); }
+      const unsigned m = __ballot_sync(0xffffffffu, cov);
+      if (cov) fb.bl[fb.boff[b2] + run + __popc(m & lt)] = (uint32_t)j | ((uint32_t)s0 << 16);
+      run += __popc(m);
+    }
+  }
+  __syncwarp();
+  int cnt = 0;
+  for (int t0 = 0; t0 < na; t0 += 32) {
+    const int i = t0 + lane;
+    int ni = 0;
+    uint16_t lc[LCAP];
+    if (i < na) {
+      const double px = LA.x0[i], py = LA.y0[i], qx = LA.x1[i], qy = LA.y1[i];
+      const double ax0 = (px < qx ? px : qx) - pad, ax1 = (px < qx ? qx : px) + pad;
+      const double ay0 = (py < qy ? py : qy) - pad, ay1 = (py < qy ? qy : py) + pad;
+      const int s0 = bk(ax ? ax0 : ay0), s1 = bk(ax ? ax1 : ay1);
+      for (int b2 = s0; b2 <= s1; b2++)
+        for (uint32_t e = fb.boff[b2]; e < fb.boff[b2 + 1]; e++) {
+          const uint32_t v = fb.bl[e];
+          const int j = (int)(v & 0xFFFFu), sj = (int)(v >> 16);
+          if ((sj > s0 ? sj : s0) != b2) continue;   // the pair belongs to the first slab both edges reach
+          if (out_cmp(LB.x0[j], LB.y0[j], LB.x1[j], LB.y1[j], ax0, ay0, ax1, ay1)) continue;
+          if (ni < LCAP) lc[ni] = (uint16_t)j;
+          ni++;
+        }
+      if (ni <= LCAP)
+        for (int u = 1; u < ni; u++) {
+          const uint16_t v = lc[u];
+          int w = u - 1;
+          while (w >= 0 && lc[w] > v) { lc[w + 1] = lc[w]; w--; }
+          lc[w + 1] = v;
+        }
+    }
+    if (__any_sync(0xffffffffu, ni > LCAP)) return -1;
+    int x = ni;
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= o) x += y;
+    }
+    const int off = cnt + x - ni;
+    if (i < na) {
+      fb.sa[i] = (uint32_t)ni;
+      for (int k = 0; k < ni; k++) {
+        if (off + k < fb.cap) fb.cp[off + k] = (uint32_t)i | ((uint32_t)lc[k] << 16);
+        atomicAdd(&fb.sb[lc[k]], 1u);
+      }
+    }
+    cnt += __shfl_sync(0xffffffffu, x, 31);
+  }
+  __syncwarp();
+  return cnt;
+}
+
+// returns the number of candidate pairs (> fb.cap: the lists were not kept)
+__device__ int flat_candidates(const EList& LA, int na, const EList& LB, int nb, double pad, const Box& ov, const FlatBuf& fb, int lane) {
   for (int t = lane; t <= na; t += 32) fb.sa[t] = 0;
   for (int t = lane; t <= nb; t += 32) fb.sb[t] = 0;
   __syncwarp();
   if (na == 0 || nb == 0) return 0;
   const unsigned lt = (1u << lane) - 1;
   const int total = na * nb;
+  int cnt = -1;
+  if (total > GRID_MAX) {
+    cnt = bucket_candidates(LA, na, LB, nb, pad, ov, fb, lane);
+    if (cnt < 0) {   // overflowed: count afresh with the grid
+      for (int t = lane; t <= na; t += 32) fb.sa[t] = 0;
+      for (int t = lane; t <= nb; t += 32) fb.sb[t] = 0;
+      __syncwarp();
+    }
+  }
+  if (cnt < 0) {
   const int qi = 32 / nb, qj = 32 % nb;
-  int i = lane / nb, j = lane % nb, cnt = 0;
+  int i = lane / nb, j = lane % nb;
+  cnt = 0;
   for (int base = 0; base < total; base += 32) {
     bool keep = false;
     if (base + lane < total) {
@@ -75,7 +174,7 @@ __device__ int flat_candidates(const EList& LA, int na, const EList& LB, int nb,
     }
     const unsigned m = __ballot_sync(0xffffffffu, keep);
     const int pos = cnt + __popc(m & lt);
-    if (keep && pos < CPCAP) {
+    if (keep && pos < fb.cap) {
       fb.cp[pos] = (uint32_t)i | ((uint32_t)j << 16);
       atomicAdd(&fb.sa[i], 1u);
       atomicAdd(&fb.sb[j], 1u);
@@ -84,7 +183,8 @@ __device__ int flat_candidates(const EList& LA, int na, const EList& LB, int nb,
     i += qi; j += qj;
     if (j >= nb) { j -= nb; i++; }
   }
-  if (cnt > CPCAP) return cnt;
+  }
+  if (cnt > fb.cap) return cnt;
   __syncwarp();
   warp_exscan(fb.sa, na + 1, lane);
   warp_exscan(fb.sb, nb + 1, lane);
@@ -233,8 +333,8 @@ __device__ bool refine_pair_t(const DLayer& P, const DLayer& R, uint32_t a, uint
   __syncwarp();
   int ncp = -1;   // candidate edge pairs (FLAT); -1: sweep every edge pair
   if constexpr (FLAT) {
-    ncp = flat_candidates(LA, na, LB, nb, 2.0 * G.tol, *fb, lane);
-    if (ncp > CPCAP) return false;
+    ncp = flat_candidates(LA, na, LB, nb, 2.0 * G.tol, G.ov, *fb, lane);
+    if (ncp > fb->cap) return false;
   }
   // boundary contact
   bool hit = false, hit_any = false;
@@ -396,7 +496,11 @@ __global__ void __launch_bounds__(RB_WARPS * 32, Cfg<F>::minb) k_refine(DLayer P
     fbuf.cp = reinterpret_cast<uint32_t*>(fbase);
     fbuf.sa = fbuf.cp + CPCAP;
     fbuf.sb = fbuf.sa + (CAP_F + 1);
-    fbuf.pj = reinterpret_cast<uint16_t*>(fbuf.sb + (CAP_F + 1));
+    fbuf.bl = fbuf.sb + (CAP_F + 1);
+    fbuf.boff = fbuf.bl + BLCAP;
+    fbuf.pj = reinterpret_cast<uint16_t*>(fbuf.boff + (NBK + 1));
+    fbuf.cap = CPCAP;
+    fbuf.blcap = BLCAP;
     fb = &fbuf;
   }
   const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
@@ -416,20 +520,43 @@ __global__ void __launch_bounds__(RB_WARPS * 32, Cfg<F>::minb) k_refine(DLayer P
   }
 }
 
-// oversized pairs: the same pair routine with per-warp edge lists in global scratch
+// oversized pairs: the same pair routine with per-warp edge lists in global scratch. The filtered variant also
+// keeps its candidate list there (cph entries); a pair with more candidates runs the full sweeps instead.
+template <bool F>
+__host__ __device__ constexpr size_t scratch_per_warp(int cap, int cph) {
+  return ((2 * (size_t)cap * Cfg<F>::edge + (F ? (size_t)cph * 6 + 2 * ((size_t)cap + 1) * 4 + ((size_t)(2 * cap + 64) + NBK + 1) * 4 : 0)) + 15) &
+         ~(size_t)15;
+}
 template <bool F>
 __global__ void __launch_bounds__(128) k_refine_scratch(DLayer P, DLayer R, const uint2* __restrict__ pairs, const uint32_t* __restrict__ heavy,
                                                        uint64_t nh, RefineArgs rp, uint8_t* flag, double* area, double4* ev, uint32_t* evb,
-                                                       unsigned char* scratch, int cap, int* err) {
+                                                       unsigned char* scratch, int cap, int cph, int* err) {
   const int lane = threadIdx.x & 31;
   const uint64_t w = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
-  unsigned char* base = scratch + w * 2 * (size_t)cap * Cfg<F>::edge;
+  unsigned char* base = scratch + w * scratch_per_warp<F>(cap, cph);
   EList LA = carve_t<F>(base, cap), LB = carve_t<F>(base + (size_t)cap * Cfg<F>::edge, cap);
+  FlatBuf fb;
+  if constexpr (F) {   // cp (u32), sa, sb (u32), pj (u16) after the lists
+    fb.cp = reinterpret_cast<uint32_t*>(base + 2 * (size_t)cap * Cfg<F>::edge);
+    fb.sa = fb.cp + cph;
+    fb.sb = fb.sa + (cap + 1);
+    fb.bl = fb.sb + (cap + 1);
+    fb.boff = fb.bl + (2 * cap + 64);
+    fb.pj = reinterpret_cast<uint16_t*>(fb.boff + (NBK + 1));
+    fb.cap = cph;
+    fb.blcap = 2 * cap + 64;
+  }
   for (uint64_t h = w; h < nh; h += nw) {
     const uint32_t p = heavy[h];
     const uint2 pr = pairs[p];
     uint8_t f; double ar; double4 e4; uint32_t b4;
-    const bool ok = refine_pair_t<F>(P, R, pr.x, pr.y, rp, LA, LB, cap, lane, f, ar, e4, b4);
+    bool ok;
+    if constexpr (F) {   // candidate entries pack both edge indices in 16 bits each
+      ok = cap <= 0xFFFF && refine_pair_t<F, true>(P, R, pr.x, pr.y, rp, LA, LB, cap, lane, f, ar, e4, b4, &fb);
+      if (!ok) ok = refine_pair_t<F, false>(P, R, pr.x, pr.y, rp, LA, LB, cap, lane, f, ar, e4, b4);
+    } else {
+      ok = refine_pair_t<F, false>(P, R, pr.x, pr.y, rp, LA, LB, cap, lane, f, ar, e4, b4);
+    }
     if (lane == 0) {
       if (!ok) *err = 1;
       else {
@@ -464,13 +591,14 @@ static uint64_t refine_t(gsj_ctx* c, const gsj_layer* P, const gsj_layer* R, con
   if (nh) {
     // list capacity rounded to 8 edges keeps every double array of the slab 8-byte aligned
     const int cap = (int)((std::max<uint32_t>(std::max(P->max_geom_edges, R->max_geom_edges), 1u) + 7u) & ~7u);
-    const size_t per = 2 * (size_t)cap * Cfg<F>::edge;
+    const int cph = std::min(8 * cap, 1 << 16);   // candidate entries (indices stay below 2^16)
+    const size_t per = scratch_per_warp<F>(cap, cph);
     uint64_t nwarps = std::min<uint64_t>(nh, std::max<uint64_t>(1, (1ull << 30) / per));
     nwarps = std::min<uint64_t>(nwarps, (uint64_t)c->sm_count * 32);
     nwarps = (nwarps + 3) / 4 * 4;
     unsigned char* scr = c->scratch.as<unsigned char>(per * nwarps);
     GSJ_CK(cudaMemsetAsync(err, 0, 4, s));
-    k_refine_scratch<F><<<(int)(nwarps / 4), 128, 0, s>>>(P->d, R->d, pairs, heavy, nh, rp, flag, area, ev, evb, scr, cap, err); c->launches++;
+    k_refine_scratch<F><<<(int)(nwarps / 4), 128, 0, s>>>(P->d, R->d, pairs, heavy, nh, rp, flag, area, ev, evb, scr, cap, cph, err); c->launches++;
     GSJ_CK(cudaGetLastError());
     GSJ_CK(cudaMemcpyAsync(h, ctr, 16, cudaMemcpyDeviceToHost, s));
     GSJ_CK(cudaStreamSynchronize(s));
