@@ -39,11 +39,11 @@ constexpr int CPCAP = 1024;
 // Large grids are searched by buckets instead: NBK slabs along the overlap box's longer side, B's edges listed per
 // slab (bl, boff), each lane scanning only its A edge's slabs and reporting a pair once, in the first slab both
 // edges reach; the lane sorts its few candidates (at most LCAP) so the list keeps (i, j) order.
-constexpr int NBK = 16, BLCAP = 512, LCAP = 32;
-constexpr int GRID_MAX = 2048;   // na x nb up to this: the grid sweep
+// Only the oversized pairs of the scratch kernel use the buckets: for the shared-memory bins the grid is faster.
+constexpr int NBK = 16, LCAP = 32;
+constexpr int GRID_MAX = 2048;   // scratch kernel: na x nb up to this: the grid sweep
 struct FlatBuf { uint32_t* cp; uint16_t* pj; uint32_t* sa; uint32_t* sb; uint32_t* bl; uint32_t* boff; int cap, blcap; };   // cap: entries of cp / pj
-constexpr size_t FLAT_BYTES = (CPCAP * sizeof(uint32_t) + CPCAP * sizeof(uint16_t) + 2 * (CAP_F + 1) * sizeof(uint32_t) + BLCAP * sizeof(uint32_t) +
-                               (NBK + 1) * sizeof(uint32_t) + 15) & ~(size_t)15;
+constexpr size_t FLAT_BYTES = CPCAP * sizeof(uint32_t) + CPCAP * sizeof(uint16_t) + 2 * (CAP_F + 1) * sizeof(uint32_t);
 
 __device__ __forceinline__ void warp_exscan(uint32_t* a, int n, int lane) {   // in place over a[0 .. n)
   uint32_t run = 0;
@@ -144,6 +144,7 @@ __device__ int bucket_candidates(const EList& LA, int na, const EList& LB, int n
 }
 
 // returns the number of candidate pairs (> fb.cap: the lists were not kept)
+template <bool BUCKETS>
 __device__ int flat_candidates(const EList& LA, int na, const EList& LB, int nb, double pad, const Box& ov, const FlatBuf& fb, int lane) {
   for (int t = lane; t <= na; t += 32) fb.sa[t] = 0;
   for (int t = lane; t <= nb; t += 32) fb.sb[t] = 0;
@@ -152,7 +153,7 @@ __device__ int flat_candidates(const EList& LA, int na, const EList& LB, int nb,
   const unsigned lt = (1u << lane) - 1;
   const int total = na * nb;
   int cnt = -1;
-  if (total > GRID_MAX) {
+  if (BUCKETS && total > GRID_MAX) {
     cnt = bucket_candidates(LA, na, LB, nb, pad, ov, fb, lane);
     if (cnt < 0) {   // overflowed: count afresh with the grid
       for (int t = lane; t <= na; t += 32) fb.sa[t] = 0;
@@ -312,7 +313,7 @@ __device__ __forceinline__ double pair_snap(double2 oa, double2 ea) {   // engin
 // One pair, whole warp. Returns false when a local list exceeded cap (nothing written).
 // FLAT (filtered kernel only): the candidate-list path; a pair whose list would exceed CPCAP is handed back
 // (false) like an oversized pair, and the scratch kernel runs it with the full sweeps.
-template <bool F, bool FLAT = false>
+template <bool F, bool FLAT = false, bool BUCKETS = false>
 __device__ bool refine_pair_t(const DLayer& P, const DLayer& R, uint32_t a, uint32_t b, const RefineArgs& rp, EList LA, EList LB, int cap,
                               int lane, uint8_t& o_flag, double& o_area, double4& o_ev, uint32_t& o_evb, const FlatBuf* fb = nullptr) {
   const double2 oa = P.origin[a], ob = R.origin[b], ea = P.ext[a], eb = R.ext[b];
@@ -333,7 +334,7 @@ __device__ bool refine_pair_t(const DLayer& P, const DLayer& R, uint32_t a, uint
   __syncwarp();
   int ncp = -1;   // candidate edge pairs (FLAT); -1: sweep every edge pair
   if constexpr (FLAT) {
-    ncp = flat_candidates(LA, na, LB, nb, 2.0 * G.tol, G.ov, *fb, lane);
+    ncp = flat_candidates<BUCKETS>(LA, na, LB, nb, 2.0 * G.tol, G.ov, *fb, lane);
     if (ncp > fb->cap) return false;
   }
   // boundary contact
@@ -496,11 +497,10 @@ __global__ void __launch_bounds__(RB_WARPS * 32, Cfg<F>::minb) k_refine(DLayer P
     fbuf.cp = reinterpret_cast<uint32_t*>(fbase);
     fbuf.sa = fbuf.cp + CPCAP;
     fbuf.sb = fbuf.sa + (CAP_F + 1);
-    fbuf.bl = fbuf.sb + (CAP_F + 1);
-    fbuf.boff = fbuf.bl + BLCAP;
-    fbuf.pj = reinterpret_cast<uint16_t*>(fbuf.boff + (NBK + 1));
+    fbuf.pj = reinterpret_cast<uint16_t*>(fbuf.sb + (CAP_F + 1));
+    fbuf.bl = fbuf.boff = nullptr;
     fbuf.cap = CPCAP;
-    fbuf.blcap = BLCAP;
+    fbuf.blcap = 0;
     fb = &fbuf;
   }
   const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
@@ -552,7 +552,7 @@ __global__ void __launch_bounds__(128) k_refine_scratch(DLayer P, DLayer R, cons
     uint8_t f; double ar; double4 e4; uint32_t b4;
     bool ok;
     if constexpr (F) {   // candidate entries pack both edge indices in 16 bits each
-      ok = cap <= 0xFFFF && refine_pair_t<F, true>(P, R, pr.x, pr.y, rp, LA, LB, cap, lane, f, ar, e4, b4, &fb);
+      ok = cap <= 0xFFFF && refine_pair_t<F, true, true>(P, R, pr.x, pr.y, rp, LA, LB, cap, lane, f, ar, e4, b4, &fb);
       if (!ok) ok = refine_pair_t<F, false>(P, R, pr.x, pr.y, rp, LA, LB, cap, lane, f, ar, e4, b4);
     } else {
       ok = refine_pair_t<F, false>(P, R, pr.x, pr.y, rp, LA, LB, cap, lane, f, ar, e4, b4);
