@@ -35,7 +35,7 @@ struct PairGeo { Box ov; double tol, eps_par, snap, cx, cy; };
 // 2 tol of each other - a superset of the pairs any box test of the pair routine keeps (those use tol or no pad).
 // Built by one lane-balanced sweep over the na x nb grid (ballot compaction keeps (i, j) order); per-edge
 // ranges: A edge i owns cp[sa[i] .. sa[i+1]), B edge j owns pj[(j ? sb[j-1] : 0) .. sb[j]) (entries in i order).
-constexpr int CPCAP = 1024;
+constexpr int CPCAP = 512;
 // Large grids are searched by buckets instead: NBK slabs along the overlap box's longer side, B's edges listed per
 // slab (bl, boff), each lane scanning only its A edge's slabs and reporting a pair once, in the first slab both
 // edges reach; the lane sorts its few candidates (at most LCAP) so the list keeps (i, j) order.
@@ -477,7 +477,7 @@ __device__ bool refine_pair(const DLayer& P, const DLayer& R, uint32_t a, uint32
 
 template <bool F> struct Cfg;
 template <> struct Cfg<false> { static constexpr int cap = CAP; static constexpr size_t list = LIST_BYTES, smem = RB_SMEM, edge = EDGE_BYTES; static constexpr int minb = 3; };
-template <> struct Cfg<true> { static constexpr int cap = CAP_F; static constexpr size_t list = LIST_BYTES_F, smem = RB_SMEM_F + RB_WARPS * FLAT_BYTES, edge = EDGE_BYTES_F; static constexpr int minb = 3; };
+template <> struct Cfg<true> { static constexpr int cap = CAP_F; static constexpr size_t list = LIST_BYTES_F, smem = RB_SMEM_F + RB_WARPS * FLAT_BYTES, edge = EDGE_BYTES_F; static constexpr int minb = 4; };
 
 template <bool F>
 __device__ __forceinline__ EList carve_t(unsigned char* base, int cap) { return F ? carve_f(base, cap) : carve(base, cap); }
