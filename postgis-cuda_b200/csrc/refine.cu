@@ -485,7 +485,7 @@ __device__ __forceinline__ EList carve_t(unsigned char* base, int cap) { return 
 template <bool F>
 __global__ void __launch_bounds__(RB_WARPS * 32, Cfg<F>::minb) k_refine(DLayer P, DLayer R, const uint2* __restrict__ pairs, uint64_t np,
                                                                         RefineArgs rp, uint8_t* flag, double* area, double4* ev, uint32_t* evb,
-                                                                        uint32_t* heavy, unsigned long long* nheavy) {
+                                                                        uint32_t* heavy, unsigned long long* nheavy, unsigned long long* next) {
   extern __shared__ __align__(16) unsigned char smem[];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   EList LA = carve_t<F>(smem + (size_t)wib * 2 * Cfg<F>::list, Cfg<F>::cap);
@@ -503,8 +503,7 @@ __global__ void __launch_bounds__(RB_WARPS * 32, Cfg<F>::minb) k_refine(DLayer P
     fbuf.blcap = 0;
     fb = &fbuf;
   }
-  const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
-  for (uint64_t p = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; p < np; p += nw) {
+  auto one = [&](uint64_t p) {
     const uint2 pr = pairs[p];
     uint8_t f; double ar; double4 e4; uint32_t b4;
     const bool ok = refine_pair_t<F, F>(P, R, pr.x, pr.y, rp, LA, LB, Cfg<F>::cap, lane, f, ar, e4, b4, fb);
@@ -517,6 +516,21 @@ __global__ void __launch_bounds__(RB_WARPS * 32, Cfg<F>::minb) k_refine(DLayer P
       }
     }
     __syncwarp();
+  };
+  if constexpr (F) {
+    // persistent grid (one wave): warps take runs of consecutive pairs (shared probe geometry) from a counter
+    constexpr uint64_t RUN = 4;
+    for (;;) {
+      unsigned long long p0 = 0;
+      if (lane == 0) p0 = atomicAdd(next, (unsigned long long)RUN);
+      p0 = __shfl_sync(0xffffffffu, p0, 0);
+      if (p0 >= np) break;
+      const uint64_t p1 = p0 + RUN < np ? p0 + RUN : np;
+      for (uint64_t p = p0; p < p1; p++) one(p);
+    }
+  } else {
+    const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    for (uint64_t p = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; p < np; p += nw) one(p);
   }
 }
 
@@ -579,10 +593,10 @@ static uint64_t refine_t(gsj_ctx* c, const gsj_layer* P, const gsj_layer* R, con
   }
   unsigned long long* ctr = c->counters.as<unsigned long long>(8);
   int* err = reinterpret_cast<int*>(ctr + 1);
-  GSJ_CK(cudaMemsetAsync(ctr, 0, 16, s));
+  GSJ_CK(cudaMemsetAsync(ctr, 0, 24, s));   // heavy count, error word, pair counter
   uint32_t* heavy = c->heavy.as<uint32_t>(np);
-  const int blocks = (int)std::min<uint64_t>((np + RB_WARPS - 1) / RB_WARPS, (uint64_t)c->sm_count * 8);
-  k_refine<F><<<blocks, RB_WARPS * 32, Cfg<F>::smem, s>>>(P->d, R->d, pairs, np, rp, flag, area, ev, evb, heavy, ctr); c->launches++;
+  const int blocks = (int)std::min<uint64_t>((np + RB_WARPS - 1) / RB_WARPS, (uint64_t)c->sm_count * (F ? Cfg<F>::minb : 8));
+  k_refine<F><<<blocks, RB_WARPS * 32, Cfg<F>::smem, s>>>(P->d, R->d, pairs, np, rp, flag, area, ev, evb, heavy, ctr, ctr + 2); c->launches++;
   GSJ_CK(cudaGetLastError());
   unsigned long long* h = c->h_counters.as<unsigned long long>(2);
   GSJ_CK(cudaMemcpyAsync(h, ctr, 16, cudaMemcpyDeviceToHost, s));
