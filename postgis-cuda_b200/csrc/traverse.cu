@@ -11,9 +11,10 @@ __device__ __forceinline__ bool box_hit(const float4& c, const float4& b) {
   return !(c.x > b.z || c.z < b.x || c.y > b.w || c.w < b.y);
 }
 
-// Two neighbouring probes per thread (adjacent in Morton order), walked in lockstep: each step issues both node
-// loads before testing either, so every lane keeps two independent load chains in flight.
-constexpr int QPT = 2;
+// QPT neighbouring probes per thread (adjacent in Morton order), walked in lockstep: each step issues all their node
+// loads before testing any, so every lane keeps QPT independent load chains in flight (the walk is latency-bound:
+// one dependent load per step otherwise).
+constexpr int QPT = 4;
 __global__ void __launch_bounds__(128) k_traverse(const float4* __restrict__ qbb, const uint32_t* __restrict__ qorder, uint32_t q0, uint32_t nq,
                                                   DBvh T, int upper, uint2* __restrict__ out, unsigned long long cap,
                                                   unsigned long long* counter, int* err, unsigned long long* visits) {
