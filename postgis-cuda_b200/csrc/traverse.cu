@@ -1,4 +1,4 @@
-// Candidate search: LBVH traversal, one thread per probe box, probes taken in Morton order so the lanes of a warp
+// Candidate search: LBVH traversal, QPT probe boxes per thread, probes taken in Morton order so the lanes of a warp
 // walk neighbouring parts of the tree (the reference's k_traverse, engine/engine.cuh:233-259, runs a count pass
 // and a write pass; here one pass appends with one atomic per warp step).
 #include "engine.h"
