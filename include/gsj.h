@@ -29,6 +29,10 @@ typedef struct gsj_layer gsj_layer;
 
 /* Context on a CUDA device (replaces the daemon's process-global device state, daemon/gpujoind.cu:589-621). */
 int gsj_ctx_create(int device, gsj_ctx** out);
+/* The same, with the context's stream at the device's highest (high_priority != 0) or lowest priority: the kernels
+ * of a high-priority context get SMs first as blocks of other contexts' kernels retire (serving: small requests
+ * ahead of large ones). */
+int gsj_ctx_create_prio(int device, int high_priority, gsj_ctx** out);
 void gsj_ctx_destroy(gsj_ctx* ctx);
 const char* gsj_last_error(const gsj_ctx* ctx);
 /* The context's CUDA stream (a cudaStream_t): every kernel and copy of the context runs on it, in call order.

@@ -43,7 +43,7 @@ template <class F> static int guard(gsj_ctx* c, F&& f) {
 
 extern "C" {
 
-int gsj_ctx_create(int device, gsj_ctx** out) {
+static int ctx_create(int device, int high_priority, gsj_ctx** out) {
   if (!out) return GSJ_ERR_ARG;
   *out = nullptr;
   gsj_ctx* c = new gsj_ctx();
@@ -54,17 +54,32 @@ int gsj_ctx_create(int device, gsj_ctx** out) {
     if (device < 0 || device >= nd) throw Error(GSJ_ERR_ARG, "no such CUDA device");
     GSJ_CK(cudaSetDevice(device));
     GSJ_CK(cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, device));
-    GSJ_CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    int lo = 0, hi = 0;
+    GSJ_CK(cudaDeviceGetStreamPriorityRange(&lo, &hi));   // hi is the numerically smallest, most urgent
+    GSJ_CK(cudaStreamCreateWithPriority(&c->stream, cudaStreamNonBlocking, high_priority ? hi : lo));
+    // stream-ordered scratch: keep freed pool memory cached in the process (growth never goes back to the driver)
+    cudaMemPool_t pool;
+    GSJ_CK(cudaDeviceGetDefaultMemPool(&pool, device));
+    uint64_t keep = UINT64_MAX;
+    GSJ_CK(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
+    c->each_buf([&](gsj::DevBuf& b) { b.s = c->stream; });
   });
   if (rc) { delete c; return rc; }
   *out = c;
   return GSJ_OK;
 }
 
+int gsj_ctx_create(int device, gsj_ctx** out) { return ctx_create(device, 0, out); }
+int gsj_ctx_create_prio(int device, int high_priority, gsj_ctx** out) { return ctx_create(device, high_priority, out); }
+
 void gsj_ctx_destroy(gsj_ctx* c) {
   if (!c) return;
   cudaSetDevice(c->device);
-  if (c->stream) { cudaStreamSynchronize(c->stream); cudaStreamDestroy(c->stream); }
+  if (c->stream) {
+    c->each_buf([](gsj::DevBuf& b) { b.release(); });   // stream-ordered frees before the stream goes
+    cudaStreamSynchronize(c->stream);
+    cudaStreamDestroy(c->stream);
+  }
   delete c;
 }
 

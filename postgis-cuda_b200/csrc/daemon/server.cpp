@@ -4,10 +4,11 @@
 // frame format and stats keys, so its Postgres extension works unchanged. Differences, by design:
 //  - layers come from files (binary COPY / .gset / .pset, resolved inside --data-dir) instead of SQL over libpq;
 //    LOAD_QUERY and LOAD's row filter need PostgreSQL and answer with an error;
-//  - GPU work runs on a pool of engine contexts (--workers, each its own CUDA stream and scratch) sharing the
+//  - GPU work runs on pools of engine contexts (--workers, each its own CUDA stream and scratch) sharing the
 //    resident layers, so requests that arrive while others run are admitted and overlap on the GPU instead of
-//    queueing behind one device lock (g_gpu, gpujoind.cu:35). Admission is first come, first served, as a context
-//    and the request's scratch-memory estimate (within --mem-budget-gb) become free.
+//    queueing behind one device lock (g_gpu, gpujoind.cu:35). Small requests use high-priority streams. Admission
+//    is first come, first served per pool, as a context and the request's scratch-memory estimate (within
+//    --mem-budget-gb) become free.
 #include <arpa/inet.h>
 #include <netinet/in.h>
 #include <netinet/tcp.h>
@@ -107,22 +108,26 @@ class Json {
 };
 
 // ---- engine contexts and admission ------------------------------------------------------------------------------
-// A fixed pool of contexts on one device, created on first use (the daemon starts without touching the GPU).
-// A request is admitted in arrival order once a context is free and its scratch estimate fits in the budget
+// Two pools of contexts on one device, created on first use (the daemon starts without touching the GPU): small
+// requests (probe layers of at most kSmallGeoms geometries) run on high-priority streams, so their kernels get SMs
+// ahead of a large request's as its blocks retire; large requests run on normal-priority streams. In each pool a
+// request is admitted in arrival order once a context is free and its scratch estimate fits in the pool's budget
 // beside the running requests (a request larger than the whole budget runs alone).
+constexpr uint64_t kSmallGeoms = 16384;
 class GpuPool {
  public:
+  GpuPool(int high, int share) : high_(high), share_(share) {}
   gsj_ctx* acquire(uint64_t est) {
     std::unique_lock<std::mutex> lk(m_);
     const uint64_t ticket = next_++;
     cv_.wait(lk, [&] {
-      return ticket == serving_ && (!free_.empty() || created_ < g_cfg.workers) && (busy_ == 0 || budget_ == 0 || used_ + est <= budget_);
+      return ticket == serving_ && (!free_.empty() || created_ < size()) && (busy_ == 0 || budget_ == 0 || used_ + est <= budget_);
     });
     serving_++;
     gsj_ctx* c = nullptr;
     if (!free_.empty()) { c = free_.back(); free_.pop_back(); }
     else {
-      const int rc = gsj_ctx_create(g_cfg.device, &c);
+      const int rc = gsj_ctx_create_prio(g_cfg.device, high_, &c);
       if (rc) {
         cv_.notify_all();
         throw std::runtime_error("no usable CUDA device " + std::to_string(g_cfg.device) + " (gsj_ctx_create: " + std::to_string(rc) + ")");
@@ -131,7 +136,8 @@ class GpuPool {
       if (!budget_set_) {
         uint64_t fr = 0, tot = 0;
         gsj_ctx_mem_info(c, &fr, &tot, nullptr);
-        budget_ = g_cfg.mem_budget_gb > 0 ? (uint64_t)(g_cfg.mem_budget_gb * 1073741824.0) : fr / 2;
+        const uint64_t all = g_cfg.mem_budget_gb > 0 ? (uint64_t)(g_cfg.mem_budget_gb * 1073741824.0) : fr / 2;
+        budget_ = all / 2;
         budget_set_ = true;
       }
     }
@@ -149,13 +155,15 @@ class GpuPool {
   }
   void counts(int* busy, uint64_t* queued, uint64_t* used, uint64_t* budget) {
     std::lock_guard<std::mutex> lk(m_);
-    *busy = busy_;
-    *queued = next_ - serving_;
-    *used = used_;
-    *budget = budget_;
+    *busy += busy_;
+    *queued += next_ - serving_;
+    *used += used_;
+    *budget += budget_;
   }
 
  private:
+  int size() const { return std::max(1, share_ == 0 ? g_cfg.workers / 2 : g_cfg.workers - g_cfg.workers / 2); }
+  int high_, share_;
   std::mutex m_;
   std::condition_variable cv_;
   std::vector<gsj_ctx*> free_;
@@ -163,18 +171,21 @@ class GpuPool {
   uint64_t next_ = 0, serving_ = 0, used_ = 0, budget_ = 0;
   bool budget_set_ = false;
 };
-GpuPool g_pool;
+GpuPool g_pool_small(1, 0), g_pool_large(0, 1);
 
 class Lease {
  public:
-  explicit Lease(uint64_t est = 0) : est_(est), c_(g_pool.acquire(est)) {}
-  ~Lease() { g_pool.release(c_, est_); }
+  // small: the request's probe layer has at most kSmallGeoms geometries
+  explicit Lease(uint64_t est = 0, bool small = false)
+      : est_(est), pool_(small ? g_pool_small : g_pool_large), c_(pool_.acquire(est)) {}
+  ~Lease() { pool_.release(c_, est_); }
   gsj_ctx* get() const { return c_; }
   Lease(const Lease&) = delete;
   Lease& operator=(const Lease&) = delete;
 
  private:
   uint64_t est_;
+  GpuPool& pool_;
   gsj_ctx* c_;
 };
 
@@ -461,7 +472,7 @@ void op_join(Conn& c, const std::vector<std::string>& a) {
   if (A->points() && B->points()) throw std::runtime_error("point x point joins are not supported");
   bool swapped = false;
   if (!A->points() && B->points()) { std::swap(A, B); swapped = true; }   // run as point x polygon
-  Lease lease(scratch_estimate(*A, *B));
+  Lease lease(scratch_estimate(*A, *B), A->gpu_geoms <= kSmallGeoms);
   gsj_ctx* ctx = lease.get();
   c.u32(GSP_OK);
   c.streaming = true;
@@ -585,7 +596,7 @@ void op_relate(Conn& c, const std::vector<std::string>& a) {
   if (A->points() && B->points()) throw std::runtime_error("point x point relate is not supported");
   bool swapped = false;
   if (!A->points() && B->points()) { std::swap(A, B); swapped = true; }
-  Lease lease(scratch_estimate(*A, *B));
+  Lease lease(scratch_estimate(*A, *B), A->gpu_geoms <= kSmallGeoms);
   gsj_ctx* ctx = lease.get();
   c.u32(GSP_OK);
   c.streaming = true;
@@ -686,7 +697,7 @@ void op_dwithin(Conn& c, const std::vector<std::string>& a) {
   bool swapped = false;
   if (!A->points() && B->points()) { std::swap(A, B); std::swap(ra, rb); swapped = true; }
   if (A->points() && erode && ra > 0) throw std::runtime_error("a point layer cannot have a negative buffer");
-  Lease lease(scratch_estimate(*A, *B));
+  Lease lease(scratch_estimate(*A, *B), A->gpu_geoms <= kSmallGeoms);
   gsj_ctx* ctx = lease.get();
   c.u32(GSP_OK);
   c.streaming = true;
@@ -740,7 +751,8 @@ std::string op_status() {   // gpujoind.cu:486-494 (+ the worker pool)
   if (rc) throw std::runtime_error("no usable CUDA device " + std::to_string(g_cfg.device));
   int busy = 0;
   uint64_t queued = 0, used = 0, budget = 0;
-  g_pool.counts(&busy, &queued, &used, &budget);
+  g_pool_small.counts(&busy, &queued, &used, &budget);
+  g_pool_large.counts(&busy, &queued, &used, &budget);
   return Json().str("device", name).str("cc", std::to_string(ma) + "." + std::to_string(mi)).num("mem_total_mb", tot / 1048576.0)
       .num("mem_free_mb", fr / 1048576.0).key("layers").raw(layer_names()).u64("workers", (uint64_t)g_cfg.workers)
       .u64("busy", (uint64_t)busy).u64("queued", queued).num("scratch_used_mb", used / 1048576.0).num("scratch_budget_mb", budget / 1048576.0)

@@ -26,21 +26,25 @@ struct Error : std::runtime_error {
                          std::string(#x) + ": " + cudaGetErrorString(e_) + " (" __FILE__ ":" + std::to_string(__LINE__) + ")"); \
   } while (0)
 
-// grow-only device scratch: the pools live in the context, so steady-state requests allocate nothing
+// grow-only device scratch: the pools live in the context, so steady-state requests allocate nothing. Bound to
+// the context's stream, growth is stream-ordered (cudaMallocAsync / cudaFreeAsync): it never synchronises the
+// device, so one request's growth does not stall the requests running on other contexts.
 struct DevBuf {
   void* p = nullptr; size_t cap = 0;
+  cudaStream_t s = nullptr;
   void* get(size_t n) {
     if (n > cap) {
-      if (p) cudaFree(p);
+      if (p) { if (s) cudaFreeAsync(p, s); else cudaFree(p); }
       p = nullptr; cap = 0;
       size_t want = n + n / 4 + 256;
-      GSJ_CK(cudaMalloc(&p, want));
+      if (s) GSJ_CK(cudaMallocAsync(&p, want, s));
+      else GSJ_CK(cudaMalloc(&p, want));
       cap = want;
     }
     return p;
   }
   template <class T> T* as(size_t count) { return reinterpret_cast<T*>(get(count * sizeof(T) + 16)); }
-  void release() { if (p) cudaFree(p); p = nullptr; cap = 0; }
+  void release() { if (p) { if (s) cudaFreeAsync(p, s); else cudaFree(p); } p = nullptr; cap = 0; }
   ~DevBuf() { release(); }
 };
 struct PinnedBuf {
@@ -95,6 +99,10 @@ struct gsj_ctx {
   gsj::DevBuf counters, cand, flag, area, ev, evb, heavy, scratch, keep, opairs, oarea, oev, oevb, ocode, tmp, keys, keys2, idx,
       idx2, agg_area, agg_ev, agg_evb, agg_flag, qbb, uf, misc1, misc2, misc3,
       er_pf, er_keep, er_off, er_pairs, er_flag, er_heavy, er_tiles, er_tiles2, er_slab, er_again, er_scr, er_ctr, er_tmp;
+  // every scratch pool, e.g. to bind them to the stream or release them before the stream goes
+  template <class Fn> void each_buf(Fn&& fn) {
+    for (gsj::DevBuf* b : {&counters, &cand, &flag, &area, &ev, &evb, &heavy, &scratch, &keep, &opairs, &oarea, &oev, &oevb, &ocode, &tmp, &keys, &keys2, &idx, &idx2, &agg_area, &agg_ev, &agg_evb, &agg_flag, &qbb, &uf, &misc1, &misc2, &misc3, &er_pf, &er_keep, &er_off, &er_pairs, &er_flag, &er_heavy, &er_tiles, &er_tiles2, &er_slab, &er_again, &er_scr, &er_ctr, &er_tmp}) fn(*b);
+  }
   gsj::PinnedBuf h_counters, h_pairs, h_area, h_code, h_where;
 };
 

@@ -36,6 +36,7 @@ struct PairGeo { Box ov; double tol, eps_par, snap, cx, cy; };
 // Built by one lane-balanced sweep over the na x nb grid (ballot compaction keeps (i, j) order); per-edge
 // ranges: A edge i owns cp[sa[i] .. sa[i+1]), B edge j owns pj[(j ? sb[j-1] : 0) .. sb[j]) (entries in i order).
 constexpr int CPCAP = 512;
+constexpr int REFINE_RUN = 4, REFINE_RUNS = 32;   // filtered kernel: pairs per fetch, fetches per warp
 // Large grids are searched by buckets instead: NBK slabs along the overlap box's longer side, B's edges listed per
 // slab (bl, boff), each lane scanning only its A edge's slabs and reporting a pair once, in the first slab both
 // edges reach; the lane sorts its few candidates (at most LCAP) so the list keeps (i, j) order.
@@ -518,14 +519,15 @@ __global__ void __launch_bounds__(RB_WARPS * 32, Cfg<F>::minb) k_refine(DLayer P
     __syncwarp();
   };
   if constexpr (F) {
-    // persistent grid (one wave): warps take runs of consecutive pairs (shared probe geometry) from a counter
-    constexpr uint64_t RUN = 4;
-    for (;;) {
+    // warps take runs of consecutive pairs (shared probe geometry) from a counter, at most REFINE_RUNS runs each:
+    // the grid is sized to cover every pair that way, and bounded block lifetimes let the kernels of other
+    // streams (higher-priority requests) take SMs as blocks retire
+    for (int k = 0; k < REFINE_RUNS; k++) {
       unsigned long long p0 = 0;
-      if (lane == 0) p0 = atomicAdd(next, (unsigned long long)RUN);
+      if (lane == 0) p0 = atomicAdd(next, (unsigned long long)REFINE_RUN);
       p0 = __shfl_sync(0xffffffffu, p0, 0);
       if (p0 >= np) break;
-      const uint64_t p1 = p0 + RUN < np ? p0 + RUN : np;
+      const uint64_t p1 = p0 + REFINE_RUN < np ? p0 + REFINE_RUN : np;
       for (uint64_t p = p0; p < p1; p++) one(p);
     }
   } else {
@@ -595,7 +597,15 @@ static uint64_t refine_t(gsj_ctx* c, const gsj_layer* P, const gsj_layer* R, con
   int* err = reinterpret_cast<int*>(ctr + 1);
   GSJ_CK(cudaMemsetAsync(ctr, 0, 24, s));   // heavy count, error word, pair counter
   uint32_t* heavy = c->heavy.as<uint32_t>(np);
-  const int blocks = (int)std::min<uint64_t>((np + RB_WARPS - 1) / RB_WARPS, (uint64_t)c->sm_count * (F ? Cfg<F>::minb : 8));
+  int blocks;
+  if constexpr (F) {   // enough warps to cover every pair with REFINE_RUNS fetches each, spread over all SMs
+    const uint64_t per_block = (uint64_t)RB_WARPS * REFINE_RUNS * REFINE_RUN;
+    const uint64_t cover = (np + per_block - 1) / per_block;
+    const uint64_t spread = std::min<uint64_t>((np + RB_WARPS * REFINE_RUN - 1) / (RB_WARPS * REFINE_RUN), (uint64_t)c->sm_count * Cfg<F>::minb);
+    blocks = (int)std::max<uint64_t>(cover, spread);
+  } else {
+    blocks = (int)std::min<uint64_t>((np + RB_WARPS - 1) / RB_WARPS, (uint64_t)c->sm_count * 8);
+  }
   k_refine<F><<<blocks, RB_WARPS * 32, Cfg<F>::smem, s>>>(P->d, R->d, pairs, np, rp, flag, area, ev, evb, heavy, ctr, ctr + 2); c->launches++;
   GSJ_CK(cudaGetLastError());
   unsigned long long* h = c->h_counters.as<unsigned long long>(2);
