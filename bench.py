@@ -3,10 +3,16 @@
 
 Workload (the configuration the headline metric is quoted on): Voronoi cells of 2M jittered-grid seeds in a
 2 x 2 degree lon/lat box (lon -119..-117, lat 33..35), 4-256 vertices per ring (log-uniform), 5% MultiPolygons
-with 2-4 parts, 2% with one interior hole; gpu_relate self-join with self_pairs 'distinct' (each unordered pair
-once, diagonal included); FP32-filtered + FP64 refinement vs the plain FP64 kernels, pair sets compared.
+with 2-4 parts, 2% with one interior hole; gpu_relate self-join, each unordered pair once (diagonal included);
+the filtered refinement (candidate edge-pair lists) vs the plain FP64 kernels, pair sets and DE-9IM compared;
+plus the serving leg (gsjd under a Poisson request stream, p50/p99 latency).
 
-  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--op relate|area|dwithin|erode|cluster]
+
+--op selects the other configurations of the same metric family (one JSON line each): area = intersects + area of
+20k Voronoi zones (6-40 vertices) x 50 zones; dwithin = 1M parcels x 1M points, ST_DWithin(geography, 5 m);
+erode = ST_Intersects(ST_Buffer(a, -1 m), ST_Buffer(b, -1 m)) self-join and cluster = ST_ClusterIntersecting, both
+on a parcel layer with ~30 vertices per ring (20M parcels by default; --seeds to change).
 
 A step is one full self-join of the resident layer. value = intersecting pairs / device time (CUDA events on the
 engine's stream). e2e = the same join through the C ABI from pinned host buffers: upload (H2D) + LBVH build +
@@ -264,6 +270,158 @@ def serving_leg(ps, n_points=1_000_000, workers=4):
         shutil.rmtree(d, ignore_errors=True)
 
 
+def run_op(args, rank, local, ws):
+    """The other configurations: one JSON line with the same keys as the headline."""
+    import torch
+    import gsj
+    from gsj import gen
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle as O
+    torch.cuda.set_device(local)
+    eng = gsj.Engine(local)
+    ext = torch.cuda.ExternalStream(eng.stream_handle(), device=local)
+    op = args.op
+    t0 = time.time()
+    pts = None
+    if op == "area":
+        A, B = gen.layer_cfg_parcels_small(20000, seed=rank), gen.layer_cfg_zones(50, seed=1)
+        workload = "intersects + area, 20k Voronoi zones (6-40 vertices, LA box) x 50 zones"
+        metric, unit = "join pairs/s (intersects + area, filtered+batched FP64)", "pairs/s"
+    elif op == "dwithin":
+        box = (-119.0, 33.0, -118.0, 34.0)
+        A, B = None, gen.layer_parcels(1_000_000, box, seed=rank)
+        pts = gen.points(1_000_000, box, 7 + rank)
+        workload = "ST_DWithin(geography, 5 m): 1M uniform points x 1M jittered-grid parcels, 1x1 deg"
+        metric, unit = "join pairs/s (points x parcels ST_DWithin 5 m)", "pairs/s"
+    else:
+        n = args.seeds or 20_000_000
+        side = 2.0 * (n / 2e6) ** 0.5
+        box = (-119.0, 33.0, -119.0 + side, 33.0 + side)
+        A = B = gen.layer_cfg5(n, box, seed=rank)
+        if op == "erode":
+            workload = f"ST_Intersects(ST_Buffer(a,-1m), ST_Buffer(b,-1m)) self-join (self_pairs all), {n / 1e6:g}M parcels, ~30 vertices/ring"
+            metric, unit = "join pairs/s (negative-buffer intersects self-join, ra = rb = 1 m)", "pairs/s"
+        else:
+            workload = f"ST_ClusterIntersecting, {n / 1e6:g}M parcels, ~30 vertices/ring"
+            metric, unit = "parcels/s (ST_ClusterIntersecting)", "parcels/s"
+    t_gen = time.time() - t0
+    LA = eng.upload_polygons(A) if A is not None else None
+    LB = LA if B is A else eng.upload_polygons(B)
+    LP = eng.upload_points(pts) if pts is not None else None
+
+    def run(mode):
+        if op == "area":
+            r = eng.join(LA, LB, want_area=True, want_relate=False, refine_mode=mode)
+            return len(r.pairs), r.stats
+        if op == "dwithin":
+            p, st = eng.points_dwithin(LP, LB, 5.0)
+            return len(p), st
+        if op == "erode":   # self_pairs 'all': a parcel's pair with itself is kept when its eroded form is not empty
+            p, st = eng.erode(LA, LA, 1.0, 1.0, same=True, refine_mode=mode)
+            return len(p), st
+        root, st = eng.cluster(LA, refine_mode=mode)
+        return len(root), st
+
+    def timed(mode):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(ext):
+            e0.record()
+        units, st = run(mode)
+        with torch.cuda.stream(ext):
+            e1.record()
+        e1.synchronize()
+        return units, st, e0.elapsed_time(e1)
+
+    modes = [("filtered", gsj.GSJ_REFINE_FILTERED)] + ([] if op == "dwithin" else [("plain", gsj.GSJ_REFINE_PLAIN)])
+    res = {}
+    for name, mode in modes:
+        for _ in range(args.warmup):
+            timed(mode)
+        barrier(ws)
+        torch.cuda.synchronize()
+        ms, units, stats = [], 0, []
+        with Clocks(local) as clk:
+            for _ in range(args.steps):
+                u, st, t = timed(mode)
+                ms.append(t); units += u; stats.append(st)
+        torch.cuda.synchronize()
+        barrier(ws)
+        res[name] = dict(ms=ms, units=units, stats=stats, clocks=clk.summary())
+    f = res["filtered"]
+    value, tot_ms = aggregate(float(np.sum(f["ms"])), float(f["units"]), ws)
+    # end to end through the C ABI from host buffers: upload (+ LBVH) + the op + the rows back
+    e2e_ms, e2e_units = [], 0
+    h2d = sum(int(x.nbytes) for x in ([A.gro, A.rvo, A.xy] if A is not None else []) + ([B.gro, B.rvo, B.xy] if B is not A else []) +
+              ([pts] if pts is not None else []))
+    for i in range(1 + args.steps):
+        t = time.perf_counter()
+        xa = eng.upload_polygons(A) if A is not None else None
+        xb = xa if B is A else eng.upload_polygons(B)
+        xp = eng.upload_points(pts) if pts is not None else None
+        if op == "area":
+            u = len(eng.join(xa, xb, want_area=True).pairs)
+        elif op == "dwithin":
+            u = len(eng.points_dwithin(xp, xb, 5.0)[0])
+        elif op == "erode":
+            u = len(eng.erode(xa, xa, 1.0, 1.0, same=True)[0])
+        else:
+            u = len(eng.cluster(xa)[0])
+        for x in {id(v): v for v in (xa, xb, xp) if v is not None}.values():
+            x.free()
+        if i:
+            e2e_ms.append((time.perf_counter() - t) * 1000.0); e2e_units += u
+    e2e_value, e2e_tot = aggregate(float(np.sum(e2e_ms)), float(e2e_units), ws)
+    st = f["stats"]
+    pk = peaks()
+    hbm = pk.get("hbm_gbs", 6650.0)
+    trav_ms = float(np.mean([s_["traverse_ms"] for s_ in st]))
+    nq = (LP.info["n"] if LP is not None else LA.info["n"])
+    trav_bytes = float(np.mean([s_["node_visits"] for s_ in st]) * 48 + nq * 20 + np.mean([s_["candidates"] for s_ in st]) * 8)
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        t = time.perf_counter()
+        if op == "area":   # CPU-runnable in full
+            OA, OB = O.OSet(A), O.OSet(B)
+            n_cpu = len(O.join(OA, OB, O.params(1, 0))[0]); sample = "the whole workload"
+        elif op == "dwithin":
+            k = 50_000
+            n_cpu = len(O.pt_dwithin(pts[:k], O.OSet(B), 5.0)); sample = f"the first {k} points against the whole layer"
+        else:
+            w = 0.1 * (box[2] - box[0])
+            sub = sub_layer(A, (box[0], box[1], box[0] + w, box[1] + w))
+            S = O.OSet(sub)
+            if op == "erode":
+                n_cpu = len(O.erode(S, S, 1.0, 1.0, same=True))
+            else:
+                O.cluster(S, sub.n); n_cpu = sub.n
+            sample = f"{sub.n} parcels in a {w:.3f} deg corner sub-box"
+        dt = time.perf_counter() - t
+        cpu = {"value": n_cpu / dt, "unit": unit, "cores": os.cpu_count(), "kind": "port",
+               "sample": f"CPU FP64 oracle (OpenMP) on {sample} ({dt:.1f} s)"}
+    line = {
+        "metric": metric, "value": value, "unit": unit, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": tot_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded Voronoi parcels / uniform points)",
+        "config": {"workload": workload, "units_per_step": int(f["units"] / args.steps), "candidates": int(st[0]["candidates"]),
+                   "parallelism": f"replicas x{ws}", "gen_s": round(t_gen, 1)},
+        "phases_ms": {k: float(np.mean([s_[k] for s_ in st])) for k in ("traverse_ms", "refine_ms", "compact_ms", "copy_ms")},
+        "e2e": {"value": e2e_value, "unit": unit, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": int(8 * e2e_units / max(1, args.steps)),
+                "ms_per_step": e2e_tot / args.steps},
+        "roofline": {"kernel": "k_traverse", "bound": "hbm", "achieved": trav_bytes / (trav_ms / 1000.0) / 1e9 if trav_ms > 0 else None,
+                     "peak": hbm, "unit": "GB/s", "frac": trav_bytes / (trav_ms / 1000.0) / 1e9 / hbm if trav_ms > 0 else None, "traffic": None,
+                     "note": "the candidate search; the refinement kernels are FP64/latency-bound"},
+        "gpu_launches": int(sum(s_["launches"] for s_ in st)),
+        "clocks": f["clocks"],
+        "cpu_baseline": cpu,
+    }
+    if "plain" in res:
+        pv, pms = aggregate(float(np.sum(res["plain"]["ms"])), float(res["plain"]["units"]), ws)
+        line["plain_fp64"] = {"value": pv, "ms_per_step": pms / args.steps, "speedup_filtered": (pms / tot_ms) if tot_ms > 0 else None,
+                              "same_units": res["plain"]["units"] == f["units"]}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def run_reference(args, rank, ws):
     """--impl reference: the CPU FP64 port of the reference's predicates, timed on the host cores."""
     from gsj import gen
@@ -292,15 +450,25 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--seeds", type=int, default=N_SEEDS)
+    ap.add_argument("--seeds", type=int, default=None, help="parcels (default 2M; 20M for --op erode / cluster)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-sample-s", type=float, default=0.0, help="CPU seconds per reference-arm step (0: sized from --steps)")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving-latency leg (gsjd under a Poisson request stream)")
+    ap.add_argument("--op", default="relate", choices=["relate", "area", "dwithin", "erode", "cluster"])
     args = ap.parse_args()
+    if args.seeds is None and args.op == "relate":
+        args.seeds = N_SEEDS
     rank, local, ws = dist_setup()
     if args.impl == "reference":
         run_reference(args, rank, ws)
         barrier(ws)
+        return
+    if args.op != "relate":
+        run_op(args, rank, local, ws)
+        barrier(ws)
+        if ws > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
         return
     import torch
     import gsj

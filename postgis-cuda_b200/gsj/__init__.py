@@ -301,11 +301,11 @@ class Engine:
         where = np.concatenate(cw) if cw else np.zeros(0, np.uint8)
         return pairs, where, st.as_dict()
 
-    def cluster(self, P: Layer, nparent: int | None = None):
+    def cluster(self, P: Layer, nparent: int | None = None, refine_mode=GSJ_REFINE_FILTERED):
         nparent = P.info["nparent"] if nparent is None else nparent
         root = np.empty(nparent, np.uint32)
         st = JoinStats()
-        o = join_opts()
+        o = join_opts(refine_mode=refine_mode)
         self._check(lib().gsj_cluster(self.ctx, P.h, nparent, ctypes.byref(o), root.ctypes.data, ctypes.byref(st)))
         return root, st.as_dict()
 
@@ -327,9 +327,9 @@ class Engine:
         o = join_opts(upper=same if upper is None else upper)
         return self._pairs_call(lib().gsj_dwithin, P.h, R.h, float(d), int(same), opts=o)
 
-    def erode(self, P: Layer, R: Layer, ra: float, rb: float, same=False, need_self=None):
+    def erode(self, P: Layer, R: Layer, ra: float, rb: float, same=False, need_self=None, refine_mode=GSJ_REFINE_FILTERED):
         ns = None if need_self is None else np.ascontiguousarray(need_self, dtype=np.uint8)
-        o = join_opts(upper=same)
+        o = join_opts(upper=same, refine_mode=refine_mode)
         return self._pairs_call(lib().gsj_erode, P.h, R.h, float(ra), float(rb), int(same), None if ns is None else ns.ctypes.data, opts=o)
 
     def points_dwithin(self, pts: Layer, R: Layer, d: float):

@@ -131,6 +131,12 @@ def layer_cfg_zones(n=50, seed=1) -> PolygonSet:
     return voronoi(n, LA_BOX, seed, vmin=4, vmax=4)
 
 
+def layer_cfg5(n, box, seed=0) -> PolygonSet:
+    """Jittered-grid parcels with ~30 vertices per ring (uniform 6-54), 5% MultiPolygons (2-4 parts), 2% holes."""
+    return voronoi(n, box, seed, jitter_grid=True, jitter=0.4, vmin=6, vmax=54, log_uniform=False,
+                   mp_frac=0.05, mp_parts=(2, 4), hole_frac=0.02)
+
+
 def layer_parcels(n, box, seed=0) -> PolygonSet:
     """Jittered-grid parcels, 4-256 vertices per ring (log-uniform), 5% MultiPolygons (2-4 parts), 2% holes."""
     return voronoi(n, box, seed, jitter_grid=True, jitter=0.4, vmin=4, vmax=256, log_uniform=True,
