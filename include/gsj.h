@@ -131,6 +131,11 @@ int gsj_dedup(uint64_t n, uint64_t nr, uint64_t nv, const uint64_t* gro, const u
               uint64_t* out_n, uint64_t* out_nr, uint64_t* out_nv, uint64_t** out_gro, uint64_t** out_rvo, double** out_xy,
               uint64_t** out_moff, uint32_t** out_midx);
 void gsj_host_free(void* p);
+/* gsj_dedup computed on the context's GPU (hash, radix sort, exact comparison within equal-hash runs, gathers):
+ * the same output arrays, bit for bit; the host arrays are copied to the device and the results back. */
+int gsj_dedup_gpu(gsj_ctx* ctx, uint64_t n, uint64_t nr, uint64_t nv, const uint64_t* gro, const uint64_t* rvo, const double* xy, int morton,
+                  uint64_t* out_n, uint64_t* out_nr, uint64_t* out_nv, uint64_t** out_gro, uint64_t** out_rvo, double** out_xy,
+                  uint64_t** out_moff, uint32_t** out_midx);
 
 /* Pair sink for distance / buffer joins: (P parent, R parent) pairs. */
 typedef int (*gsj_pairs_sink)(void* user, const uint32_t* pairs, uint64_t n);

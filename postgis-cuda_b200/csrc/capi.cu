@@ -18,6 +18,9 @@ void erode_host(gsj_ctx* c, const gsj_layer* P, const gsj_layer* R, double ra, d
                 gsj_pairs_sink sink, void* user, gsj_join_stats* stp);
 void points_buffer_host(gsj_ctx* c, const gsj_layer* pts, const gsj_layer* R, double d, int erode, const gsj_join_opts* op, gsj_pairs_sink sink,
                         void* user, gsj_join_stats* stp);
+void dedup_gpu(gsj_ctx* c, uint64_t n, uint64_t nr, uint64_t nv, const uint64_t* gro, const uint64_t* rvo, const double* xy, int morton,
+               uint64_t* out_n, uint64_t* out_nr, uint64_t* out_nv, uint64_t** out_gro, uint64_t** out_rvo, double** out_xy, uint64_t** out_moff,
+               uint32_t** out_midx);
 }  // namespace gsj
 
 using gsj::Error;
@@ -101,6 +104,13 @@ int gsj_device_query(int device, char* name, size_t namelen, int* cc_major, int*
   if (free_bytes) *free_bytes = f;
   if (total_bytes) *total_bytes = t;
   return GSJ_OK;
+}
+
+int gsj_dedup_gpu(gsj_ctx* c, uint64_t n, uint64_t nr, uint64_t nv, const uint64_t* gro, const uint64_t* rvo, const double* xy, int morton,
+                  uint64_t* out_n, uint64_t* out_nr, uint64_t* out_nv, uint64_t** out_gro, uint64_t** out_rvo, double** out_xy, uint64_t** out_moff,
+                  uint32_t** out_midx) {
+  if (!c) return GSJ_ERR_ARG;
+  return guard(c, [&] { gsj::dedup_gpu(c, n, nr, nv, gro, rvo, xy, morton, out_n, out_nr, out_nv, out_gro, out_rvo, out_xy, out_moff, out_midx); });
 }
 
 int gsj_ctx_mem_info(gsj_ctx* c, uint64_t* fr, uint64_t* tot, int* sms) {

@@ -284,10 +284,11 @@ std::string build_layer(const std::string& name, const std::string& path, int su
     HostArray<double> dxy, sxy;
     HostArray<uint32_t> dmidx, spar;
     HostArray<uint8_t> ssyn;
-    if (dedup) {   // identical geometries once, rows expand to members (dedup_set, first-occurrence order)
+    Lease lease;
+    if (dedup) {   // identical geometries once, rows expand to members (dedup_set, first-occurrence order; on the GPU)
       uint64_t un, unr, unv;
-      if (gsj_dedup(bn, bnr, bnv, gro, rvo, xy, 0, &un, &unr, &unv, &dgro.p, &drvo.p, &dxy.p, &dmoff.p, &dmidx.p))
-        throw std::runtime_error("dedup failed");
+      check(lease.get(), gsj_dedup_gpu(lease.get(), bn, bnr, bnv, gro, rvo, xy, 0, &un, &unr, &unv, &dgro.p, &drvo.p, &dxy.p, &dmoff.p, &dmidx.p),
+            "dedup");
       L->deduped = true;
       L->moff.assign(dmoff.p, dmoff.p + un + 1);
       L->midx.assign(dmidx.p, dmidx.p + n);
@@ -302,7 +303,6 @@ std::string build_layer(const std::string& name, const std::string& path, int su
     }
     L->gpu_geoms = bn; L->verts = bnv;
     L->prep_s = secs_since(t0);
-    Lease lease;
     uint64_t fr = 0, tot = 0;
     check(lease.get(), gsj_ctx_mem_info(lease.get(), &fr, &tot, nullptr), "memory query");
     const uint64_t need = bnv * 16 + bnr * 8 + bn * 120 + bnv / 8;   // vertices, rings, per-geometry arrays + LBVH

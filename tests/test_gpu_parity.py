@@ -156,3 +156,17 @@ def test_subdivided_points_cluster_dwithin(engine, pieces):
     g, _ = engine.dwithin(pieces["a"][0], pieces["a"][0], 5.0, same=True)
     o, _ = O.dwithin(pieces["a"][1], pieces["a"][1], 5.0, same=True)
     assert set(map(tuple, g.tolist())) == set(map(tuple, o.tolist()))
+
+
+@pytest.mark.parametrize("morton", [False, True])
+def test_dedup_gpu_matches_host(engine, morton):
+    """gsj_dedup_gpu gives the host routine's arrays bit for bit: distinct set, member offsets and indices."""
+    import test_gpu_daemon as TD
+    base = gen.layer_parcels(30000, (-118.3, 33.95, -118.2, 34.05), seed=4)
+    rng = np.random.default_rng(5)
+    ps = TD.with_duplicates(base, rng.choice(base.n, 3000, replace=True))   # groups of 2+ copies, some repeated
+    hu, hmo, hmi = gsj.dedup(ps, morton=morton)
+    gu, gmo, gmi = engine.dedup(ps, morton=morton)
+    assert np.array_equal(hmo, gmo) and np.array_equal(hmi, gmi)
+    assert np.array_equal(hu.gro, gu.gro) and np.array_equal(hu.rvo, gu.rvo) and np.array_equal(hu.xy.view(np.uint64), gu.xy.view(np.uint64))
+    assert hu.n < ps.n
