@@ -170,3 +170,61 @@ def test_dedup_gpu_matches_host(engine, morton):
     assert np.array_equal(hmo, gmo) and np.array_equal(hmi, gmi)
     assert np.array_equal(hu.gro, gu.gro) and np.array_equal(hu.rvo, gu.rvo) and np.array_equal(hu.xy.view(np.uint64), gu.xy.view(np.uint64))
     assert hu.n < ps.n
+
+
+def degenerate_geometries():
+    """Hand-made troublesome rings (degree offsets around shapes.X0, shapes.Y0)."""
+    S = 0.001
+    sq = shapes.square
+    g = []
+    g.append([[(0, 0), (S, 0), (S, 0), (S, S), (0, S), (0, S), (0, 0)]])                        # repeated vertices
+    g.append([[(S, 0), (2 * S, 0), (2 * S, S / 2), (3 * S, S / 2), (2 * S, S / 2), (2 * S, S), (S, S), (S, 0)]])   # spike
+    g.append([[(0, S), (S / 3, S), (2 * S / 3, S), (S, S), (S, 2 * S), (0, 2 * S), (0, S)]])    # collinear run on a shared edge
+    g.append([[(0, 0), (3 * S, 1e-12), (0, 2e-12), (0, 0)]])                                    # sliver
+    g.append([sq(S, S, S)])                                                                     # touches others at points / edges
+    g.append([sq(-S, -S, 4 * S), shapes.cw(sq(0, 0, 2 * S)), sq(S / 2, S / 2, S / 2)])          # hole with an island inside
+    g.append([sq(0, 0, S)])                                                                     # duplicate of an existing square
+    g.append([sq(0, 0, S)])
+    g.append([[(S / 2, 0), (S, S / 2), (S / 2, S), (0, S / 2), (S / 2, 0)]])                   # diamond in a square
+    g.append([[(0, 0), (S, 0), (S, S), (0, 0)], [(2 * S, 0), (3 * S, 0), (3 * S, S), (2 * S, 0)]])   # multipolygon
+    g.append([[(-S, S / 2), (4 * S, S / 2), (4 * S, S / 2 + 1e-9), (-S, S / 2 + 1e-9), (-S, S / 2)]])  # long thin bar across
+    big = [(S * np.cos(t), S * np.sin(t)) for t in np.linspace(0, 2 * np.pi, 400, endpoint=False)]
+    g.append([big + [big[0]]])                                                                  # heavy ring (> 128 edges)
+    return g
+
+
+@pytest.mark.parametrize("mode", MODES)
+def test_degenerate_inputs_bitexact(engine, mode):
+    ps = shapes.make_set(degenerate_geometries())
+    L, S = engine.upload_polygons(ps), O.OSet(ps)
+    for area, rel in ((True, False), (False, True), (True, True)):
+        r = engine.join(L, L, want_area=area, want_relate=rel, upper=True, refine_mode=mode)
+        p, oa, oc, nc = O.join(S, S, O.params(int(area), int(rel)), upper=True)
+        gp, ga, gc = srt(r.pairs, r.area, r.code)
+        assert np.array_equal(gp, p) and len(p) > 10
+        if area:
+            assert np.array_equal(ga, oa)
+        if rel:
+            assert np.array_equal(gc, oc)
+    cand = O.candidates(S, S, upper=True)
+    f, ar, ev, evb = engine.refine_pairs(L, L, cand, want_area=True, want_relate=True, refine_mode=mode)
+    of, oa, oe, ob = O.refine_pairs(S, S, cand, O.params(1, 1))
+    assert np.array_equal(f, of) and np.array_equal(ar, oa) and np.array_equal(ev, oe) and np.array_equal(evb, ob)
+    root, _ = engine.cluster(L)
+    assert np.array_equal(root, O.cluster(S, ps.n))
+    pts = np.concatenate([ps.xy, ps.xy[::3] + 1e-7, np.array([[shapes.X0 + 0.0005, shapes.Y0 + 0.0005]])])   # vertices, near-vertices
+    gp, gw, _ = engine.join_points(engine.upload_points(pts), L)
+    op_, ow, _ = O.pip(pts, S)
+    gp, gw = srt(gp, gw)
+    assert np.array_equal(gp, op_) and np.array_equal(gw, ow)
+
+
+def test_empty_and_tiny_layers(engine):
+    one = shapes.make_set([[shapes.square(0, 0, 0.001)]])
+    L = engine.upload_polygons(one)
+    r = engine.join(L, L, upper=True)
+    assert len(r.pairs) == 1 and r.area[0] > 0
+    far = shapes.make_set([[shapes.square(1.0, 1.0, 0.001)]])
+    assert len(engine.join(L, engine.upload_polygons(far)).pairs) == 0
+    with pytest.raises(gsj.GsjError):
+        engine.upload_polygons(gen.PolygonSet(np.zeros(1, np.uint64), np.zeros(1, np.uint64), np.zeros((0, 2))))
