@@ -136,6 +136,11 @@ void gsj_host_free(void* p);
 int gsj_dedup_gpu(gsj_ctx* ctx, uint64_t n, uint64_t nr, uint64_t nv, const uint64_t* gro, const uint64_t* rvo, const double* xy, int morton,
                   uint64_t* out_n, uint64_t* out_nr, uint64_t* out_nv, uint64_t** out_gro, uint64_t** out_rvo, double** out_xy,
                   uint64_t** out_moff, uint32_t** out_midx);
+/* gsj_subdivide computed on the context's GPU (breadth-first cut rounds, pieces sorted by geometry and cut path):
+ * the same output arrays, bit for bit. */
+int gsj_subdivide_gpu(gsj_ctx* ctx, uint64_t n, uint64_t nr, uint64_t nv, const uint64_t* gro, const uint64_t* rvo, const double* xy, int maxv,
+                      uint64_t* out_n, uint64_t* out_nr, uint64_t* out_nv, uint64_t** out_gro, uint64_t** out_rvo, double** out_xy,
+                      uint32_t** out_parent, uint8_t** out_syn);
 
 /* Pair sink for distance / buffer joins: (P parent, R parent) pairs. */
 typedef int (*gsj_pairs_sink)(void* user, const uint32_t* pairs, uint64_t n);

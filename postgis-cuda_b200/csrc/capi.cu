@@ -21,6 +21,9 @@ void points_buffer_host(gsj_ctx* c, const gsj_layer* pts, const gsj_layer* R, do
 void dedup_gpu(gsj_ctx* c, uint64_t n, uint64_t nr, uint64_t nv, const uint64_t* gro, const uint64_t* rvo, const double* xy, int morton,
                uint64_t* out_n, uint64_t* out_nr, uint64_t* out_nv, uint64_t** out_gro, uint64_t** out_rvo, double** out_xy, uint64_t** out_moff,
                uint32_t** out_midx);
+void subdivide_gpu(gsj_ctx* c, uint64_t n, uint64_t nr, uint64_t nv, const uint64_t* gro, const uint64_t* rvo, const double* xy, int maxv,
+                   uint64_t* out_n, uint64_t* out_nr, uint64_t* out_nv, uint64_t** out_gro, uint64_t** out_rvo, double** out_xy, uint32_t** out_parent,
+                   uint8_t** out_syn);
 }  // namespace gsj
 
 using gsj::Error;
@@ -111,6 +114,13 @@ int gsj_dedup_gpu(gsj_ctx* c, uint64_t n, uint64_t nr, uint64_t nv, const uint64
                   uint32_t** out_midx) {
   if (!c) return GSJ_ERR_ARG;
   return guard(c, [&] { gsj::dedup_gpu(c, n, nr, nv, gro, rvo, xy, morton, out_n, out_nr, out_nv, out_gro, out_rvo, out_xy, out_moff, out_midx); });
+}
+
+int gsj_subdivide_gpu(gsj_ctx* c, uint64_t n, uint64_t nr, uint64_t nv, const uint64_t* gro, const uint64_t* rvo, const double* xy, int maxv,
+                      uint64_t* out_n, uint64_t* out_nr, uint64_t* out_nv, uint64_t** out_gro, uint64_t** out_rvo, double** out_xy,
+                      uint32_t** out_parent, uint8_t** out_syn) {
+  if (!c) return GSJ_ERR_ARG;
+  return guard(c, [&] { gsj::subdivide_gpu(c, n, nr, nv, gro, rvo, xy, maxv, out_n, out_nr, out_nv, out_gro, out_rvo, out_xy, out_parent, out_syn); });
 }
 
 int gsj_ctx_mem_info(gsj_ctx* c, uint64_t* fr, uint64_t* tot, int* sms) {

@@ -295,10 +295,10 @@ std::string build_layer(const std::string& name, const std::string& path, int su
       bn = un; bnr = unr; bnv = unv; gro = dgro.p; rvo = drvo.p; xy = dxy.p;
     }
     L->n_distinct = bn;
-    if (subdiv > 0) {
+    if (subdiv > 0) {   // on the GPU (subdivide_set's pieces, bit for bit)
       uint64_t pn, pnr, pnv;
-      if (gsj_subdivide(bn, bnr, bnv, gro, rvo, xy, subdiv, &pn, &pnr, &pnv, &sgro.p, &srvo.p, &sxy.p, &spar.p, &ssyn.p))
-        throw std::runtime_error("subdivide failed");
+      check(lease.get(), gsj_subdivide_gpu(lease.get(), bn, bnr, bnv, gro, rvo, xy, subdiv, &pn, &pnr, &pnv, &sgro.p, &srvo.p, &sxy.p, &spar.p, &ssyn.p),
+            "subdivide");
       bn = pn; bnr = pnr; bnv = pnv; gro = sgro.p; rvo = srvo.p; xy = sxy.p;
     }
     L->gpu_geoms = bn; L->verts = bnv;

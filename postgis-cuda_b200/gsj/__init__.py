@@ -70,6 +70,9 @@ SIGNATURES = {
     "gsj_dedup_gpu": (ctypes.c_int, [_vp, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64, _vp, _vp, _vp, ctypes.c_int,
                                       ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64),
                                       ctypes.POINTER(_vp), ctypes.POINTER(_vp), ctypes.POINTER(_vp), ctypes.POINTER(_vp), ctypes.POINTER(_vp)]),
+    "gsj_subdivide_gpu": (ctypes.c_int, [_vp, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64, _vp, _vp, _vp, ctypes.c_int,
+                                          ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64),
+                                          ctypes.POINTER(_vp), ctypes.POINTER(_vp), ctypes.POINTER(_vp), ctypes.POINTER(_vp), ctypes.POINTER(_vp)]),
     "gsj_ctx_mem_info": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_int)]),
     "gsj_layer_upload_polygons": (ctypes.c_int, [_vp, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64, _vp, _vp, _vp, _vp, _vp,
                                                  ctypes.POINTER(_vp)]),
@@ -250,6 +253,18 @@ class Engine:
         u = PolygonSet(_take(ptrs[0], n.value + 1, np.uint64), _take(ptrs[1], nr.value + 1, np.uint64),
                        _take(ptrs[2], 2 * nv.value, np.float64).reshape(-1, 2))
         return u, _take(ptrs[3], n.value + 1, np.uint64), _take(ptrs[4], len(gro) - 1, np.uint32)
+
+    def subdivide(self, ps, maxv: int):
+        """Pieces of at most ~maxv vertices computed on this context's GPU (gsj_subdivide_gpu): the same arrays as subdivide()."""
+        from .gen import PolygonSet
+        gro = np.ascontiguousarray(ps.gro, np.uint64); rvo = np.ascontiguousarray(ps.rvo, np.uint64); xy = np.ascontiguousarray(ps.xy, np.float64)
+        n, nr, nv = ctypes.c_uint64(), ctypes.c_uint64(), ctypes.c_uint64()
+        ptrs = [_vp() for _ in range(5)]
+        self._check(lib().gsj_subdivide_gpu(self.ctx, len(gro) - 1, len(rvo) - 1, len(xy), gro.ctypes.data, rvo.ctypes.data, xy.ctypes.data, int(maxv),
+                                            ctypes.byref(n), ctypes.byref(nr), ctypes.byref(nv), *[ctypes.byref(p) for p in ptrs]))
+        return PolygonSet(_take(ptrs[0], n.value + 1, np.uint64), _take(ptrs[1], nr.value + 1, np.uint64),
+                          _take(ptrs[2], 2 * nv.value, np.float64).reshape(-1, 2), parent=_take(ptrs[3], n.value, np.uint32),
+                          syn=_take(ptrs[4], nv.value, np.uint8))
 
     def mem_info(self):
         f, t, s = ctypes.c_uint64(), ctypes.c_uint64(), ctypes.c_int()

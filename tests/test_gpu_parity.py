@@ -228,3 +228,16 @@ def test_empty_and_tiny_layers(engine):
     assert len(engine.join(L, engine.upload_polygons(far)).pairs) == 0
     with pytest.raises(gsj.GsjError):
         engine.upload_polygons(gen.PolygonSet(np.zeros(1, np.uint64), np.zeros(1, np.uint64), np.zeros((0, 2))))
+
+
+@pytest.mark.parametrize("maxv", [12, 24, 64])
+def test_subdivide_gpu_matches_host(engine, maxv):
+    """gsj_subdivide_gpu gives the host routine's pieces bit for bit: order, rings, vertices, cut flags, parents."""
+    layers = [gen.layer_parcels(20000, (-118.3, 33.95, -118.2, 34.05), seed=5), gen.voronoi(50, gen.LA_BOX, 1, vmin=40, vmax=80),
+              shapes.make_set(degenerate_geometries())]
+    for ps in layers:
+        h = gsj.subdivide(ps, maxv)
+        g = engine.subdivide(ps, maxv)
+        assert g.n == h.n and np.array_equal(g.gro, h.gro) and np.array_equal(g.rvo, h.rvo)
+        assert np.array_equal(g.xy.view(np.uint64), h.xy.view(np.uint64))
+        assert np.array_equal(g.parent, h.parent) and np.array_equal(g.syn, h.syn)
