@@ -84,6 +84,9 @@ typedef struct gsj_join_opts {
   int no_agg;                /* report piece pairs instead of parent pairs */
   int refine_mode;           /* GSJ_REFINE_PLAIN / GSJ_REFINE_FILTERED */
   const volatile int* cancel;  /* checked between batches (Conn::broken, gpujoind.cu:225) */
+  uint32_t shard, nshards;   /* probe shard `shard` of `nshards` (nshards <= 1: all probes): contiguous runs of the
+                                probes' Morton order (index ranges kept whole per parent on subdivided layers); the
+                                shards' results partition the join's (multi-GPU: one shard per GPU, R replicated) */
 } gsj_join_opts;
 void gsj_join_opts_default(gsj_join_opts* o);
 

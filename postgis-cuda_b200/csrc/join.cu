@@ -114,15 +114,30 @@ uint64_t candidates_for(gsj_ctx* c, const float4* qbb, const uint32_t* qorder, u
 }
 
 struct Batch { uint32_t q0, nq; };
-// probe batches: whole layer unless batch_q is set; pieces of one parent never straddle two batches
-static std::vector<Batch> make_batches(const gsj_layer* P, uint32_t batch_q) {
+// Probe batches of one join: index ranges that keep a parent's pieces together, or (sharded layers without
+// parents) a contiguous run of Morton positions. morton = the batches index P's Morton order.
+static std::vector<Batch> make_batches(const gsj_layer* P, const gsj_join_opts& o, bool& morton) {
   std::vector<Batch> b;
   const uint32_t n = P->d.n;
-  if (!batch_q || batch_q >= n) { b.push_back({0, n}); return b; }
   const auto& hp = P->h_parent;
-  for (uint32_t q0 = 0, qn; q0 < n; q0 = qn) {
-    qn = std::min<uint32_t>(q0 + batch_q, n);
-    if (!hp.empty()) while (qn < n && hp[qn] == hp[qn - 1]) qn++;
+  uint32_t lo = 0, hi = n;
+  if (o.nshards > 1) {
+    if (o.shard >= o.nshards) throw Error(GSJ_ERR_ARG, "shard >= nshards");
+    lo = (uint32_t)((uint64_t)n * o.shard / o.nshards);
+    hi = (uint32_t)((uint64_t)n * (o.shard + 1) / o.nshards);
+    if (!hp.empty()) {   // a parent's pieces stay in the shard of its first piece
+      while (lo > 0 && lo < n && hp[lo] == hp[lo - 1]) lo++;
+      while (hi > 0 && hi < n && hp[hi] == hp[hi - 1]) hi++;
+    }
+  }
+  const uint32_t bq = o.batch_q;
+  // Morton order: the whole layer in one batch, or a shard of a layer without parents (positions of the order)
+  morton = (o.nshards <= 1 && (!bq || bq >= n)) || (o.nshards > 1 && hp.empty());
+  if (lo >= hi) return b;
+  if (!bq || bq >= hi - lo) { b.push_back({lo, hi - lo}); return b; }
+  for (uint32_t q0 = lo, qn; q0 < hi; q0 = qn) {
+    qn = std::min<uint32_t>(q0 + bq, hi);
+    if (!hp.empty()) while (qn < hi && hp[qn] == hp[qn - 1]) qn++;
     b.push_back({q0, qn - q0});
   }
   return b;
@@ -147,8 +162,9 @@ void run_join(gsj_ctx* c, const gsj_layer* P, const gsj_layer* R, const RefineAr
   const bool rel = rp.want_relate != 0;
   Timer tm(s);
   // Morton-ordered probes for coherent traversal; batches by index ranges keep a parent's pieces together
-  const bool whole = !o.batch_q || o.batch_q >= P->d.n;
-  for (const Batch& bt : make_batches(P, o.batch_q)) {
+  bool whole = false;
+  const std::vector<Batch> batches = make_batches(P, o, whole);
+  for (const Batch& bt : batches) {
     if (o.cancel && *o.cancel) throw Error(GSJ_ERR_CANCELLED, "cancelled");
     tm.start();
     uint2* pairs = nullptr;
@@ -288,13 +304,21 @@ void run_points(gsj_ctx* c, const gsj_layer* pts, const gsj_layer* R, const gsj_
   cudaStream_t s = c->stream;
   Timer tm(s);
   const uint32_t n = pts->d.n;
-  const uint32_t bq = (o.batch_q && o.batch_q < n) ? o.batch_q : n;
-  for (uint32_t q0 = 0; q0 < n; q0 += bq) {
+  uint32_t lo = 0, hi = n;   // probe shard: a run of Morton positions
+  if (o.nshards > 1) {
+    if (o.shard >= o.nshards) throw Error(GSJ_ERR_ARG, "shard >= nshards");
+    lo = (uint32_t)((uint64_t)n * o.shard / o.nshards);
+    hi = (uint32_t)((uint64_t)n * (o.shard + 1) / o.nshards);
+  }
+  const uint32_t span = hi - lo;
+  const uint32_t bq = (o.batch_q && o.batch_q < span) ? o.batch_q : span;
+  const bool morton = bq == span || o.nshards > 1;
+  for (uint32_t q0 = lo; q0 < hi; q0 += bq) {
     if (o.cancel && *o.cancel) throw Error(GSJ_ERR_CANCELLED, "cancelled");
-    const uint32_t nq = std::min(bq, n - q0);
+    const uint32_t nq = std::min(bq, hi - q0);
     tm.start();
     uint2* pairs = nullptr;
-    uint64_t np = candidates_for(c, pts->d.bb, bq == n ? pts->bvh.order : nullptr, q0, nq, R->bvh, 0, &pairs);
+    uint64_t np = candidates_for(c, pts->d.bb, morton ? pts->bvh.order : nullptr, q0, nq, R->bvh, 0, &pairs);
     st.traverse_ms += tm.stop(); st.candidates += np; st.batches++;
     if (!np) continue;
     tm.start();

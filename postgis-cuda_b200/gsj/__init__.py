@@ -33,7 +33,7 @@ class RefineParams(ctypes.Structure):
 
 class JoinOpts(ctypes.Structure):
     _fields_ = [("batch_q", ctypes.c_uint32), ("max_pairs", ctypes.c_uint64), ("upper", ctypes.c_int), ("no_agg", ctypes.c_int),
-                ("refine_mode", ctypes.c_int), ("cancel", ctypes.POINTER(ctypes.c_int))]
+                ("refine_mode", ctypes.c_int), ("cancel", ctypes.POINTER(ctypes.c_int)), ("shard", ctypes.c_uint32), ("nshards", ctypes.c_uint32)]
 
 
 class JoinStats(ctypes.Structure):
@@ -123,10 +123,11 @@ def refine_params(want_area=True, want_relate=False, snap_half_ulp=False) -> Ref
     return p
 
 
-def join_opts(upper=False, no_agg=False, refine_mode=GSJ_REFINE_FILTERED, batch_q=0) -> JoinOpts:
+def join_opts(upper=False, no_agg=False, refine_mode=GSJ_REFINE_FILTERED, batch_q=0, shard=0, nshards=1) -> JoinOpts:
     o = JoinOpts()
     lib().gsj_join_opts_default(ctypes.byref(o))
     o.upper, o.no_agg, o.refine_mode, o.batch_q = int(upper), int(no_agg), int(refine_mode), int(batch_q)
+    o.shard, o.nshards = int(shard), int(nshards)
     return o
 
 
@@ -294,9 +295,9 @@ class Engine:
 
     # ---- joins ----
     def join(self, P: Layer, R: Layer, want_area=True, want_relate=False, upper=False, no_agg=False,
-             refine_mode=GSJ_REFINE_FILTERED, batch_q=0, snap_half_ulp=False) -> JoinResult:
+             refine_mode=GSJ_REFINE_FILTERED, batch_q=0, snap_half_ulp=False, shard=0, nshards=1) -> JoinResult:
         rp = refine_params(want_area, want_relate, snap_half_ulp)
-        o = join_opts(upper, no_agg, refine_mode, batch_q)
+        o = join_opts(upper, no_agg, refine_mode, batch_q, shard, nshards)
         chunks_p, chunks_a, chunks_c = [], [], []
 
         def sink(user, pairs, area, code, n):
@@ -315,8 +316,8 @@ class Engine:
         code = (np.concatenate(chunks_c) if chunks_c else np.zeros(0, np.uint32)) if want_relate else None
         return JoinResult(pairs, area, code, st.as_dict())
 
-    def join_points(self, pts: Layer, R: Layer, batch_q=0):
-        o = join_opts(batch_q=batch_q)
+    def join_points(self, pts: Layer, R: Layer, batch_q=0, shard=0, nshards=1):
+        o = join_opts(batch_q=batch_q, shard=shard, nshards=nshards)
         cp, cw = [], []
 
         def sink(user, pairs, where, n):

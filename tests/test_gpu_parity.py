@@ -241,3 +241,23 @@ def test_subdivide_gpu_matches_host(engine, maxv):
         assert g.n == h.n and np.array_equal(g.gro, h.gro) and np.array_equal(g.rvo, h.rvo)
         assert np.array_equal(g.xy.view(np.uint64), h.xy.view(np.uint64))
         assert np.array_equal(g.parent, h.parent) and np.array_equal(g.syn, h.syn)
+
+
+@pytest.mark.parametrize("nshards", [2, 3, 8])
+def test_probe_shards_partition_the_join(engine, layers, pieces, nshards):
+    """Probe shards (one per GPU in a multi-GPU run) partition the join: their union is the whole result, values equal."""
+    cases = [(layers["parcels"][0], layers["parcels"][0], True), (layers["parcels"][0], layers["parcels2"][0], False),
+             (pieces["a"][0], pieces["a"][0], True), (pieces["a"][0], pieces["b"][0], False)]
+    for P, R, upper in cases:
+        full = engine.join(P, R, want_area=True, want_relate=True, upper=upper)
+        parts = [engine.join(P, R, want_area=True, want_relate=True, upper=upper, shard=k, nshards=nshards) for k in range(nshards)]
+        fp, fa, fc = srt(full.pairs, full.area, full.code)
+        sp, sa, sc = srt(np.concatenate([x.pairs for x in parts]), np.concatenate([x.area for x in parts]), np.concatenate([x.code for x in parts]))
+        assert np.array_equal(fp, sp) and np.array_equal(fa, sa) and np.array_equal(fc, sc)
+    pts = gen.points(40000, (-118.3, 33.95, -118.1, 34.15), 9)
+    L = engine.upload_points(pts)
+    fp, fw, _ = engine.join_points(L, layers["parcels"][0])
+    parts = [engine.join_points(L, layers["parcels"][0], shard=k, nshards=nshards) for k in range(nshards)]
+    a, aw = srt(fp, fw)
+    b, bw = srt(np.concatenate([x[0] for x in parts]), np.concatenate([x[1] for x in parts]))
+    assert np.array_equal(a, b) and np.array_equal(aw, bw)
