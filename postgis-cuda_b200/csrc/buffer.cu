@@ -439,9 +439,13 @@ struct BEd { double x0, y0, x1, y1, ux, uy, L, ci, si; int succ, vt; };   // rea
 struct BEl { double x0, y0, x1, y1; };                                  // element of the raw offset curve
 constexpr double FILLET_QUANTUM = 3.14159265358979323846 / 16.0;       // 8 segments per quarter circle (GEOS default)
 constexpr int ER_WARPS = 2, ER_CAPE = 64, ER_CAPL = 128, ER_MAX_DEPTH = 12;
-constexpr size_t ER_SMEM_WARP = 2 * ER_CAPE * sizeof(BEd) + 2 * ER_CAPL * sizeof(BEl);
+constexpr int ER_QCAP = 64;                                                // crossing candidates queued per warp
+constexpr size_t ER_SMEM_WARP = 2 * ER_CAPE * sizeof(BEd) + 2 * ER_CAPL * sizeof(BEl) + ER_QCAP * sizeof(uint2);
 constexpr size_t ER_SMEM = (size_t)ER_WARPS * ER_SMEM_WARP;
-struct ErScratch { BEd* EA; BEd* EB; BEl* LA; BEl* LB; int capE, capL; };
+struct ErScratch { BEd* EA; BEd* EB; BEl* LA; BEl* LB; uint2* Q; int capE, capL; };
+__host__ __device__ constexpr size_t er_scratch_bytes(size_t capE, size_t capL) {
+  return 2 * capE * sizeof(BEd) + 2 * capL * sizeof(BEl) + ER_QCAP * sizeof(uint2);
+}
 struct ETile { uint32_t pair, depth; double4 box; };
 struct ErCtr { unsigned int ntile, nslab; int needE, needL; };
 struct EFrame { double ox, oy, kx, ky; };
@@ -677,21 +681,51 @@ __device__ int er_pair(const DLayer& P, const DLayer& R, uint2 ga, uint2 gb, dou
   __syncwarp();
   const BEd* EA = sc.EA; const BEd* EB = sc.EB; const BEl* LA = sc.LA; const BEl* LB = sc.LB;
   auto inW = [&](double x, double y) { return x >= Wx0 - eps && x <= Wx1 + eps && y >= Wy0 - eps && y <= Wy1 + eps; };
-  // (a) the eroded boundaries cross outside both exclusion zones
+  // (a) the eroded boundaries cross outside both exclusion zones. The la x lb element grid is scanned 32 cells a
+  // wave; cells whose boxes overlap are queued and tested 32 at a time, one per lane, so that the warp runs the
+  // exclusion tests side by side (the answer is an any-of, so the order of the tests does not change it).
   bool hit = false;
-  for (int i = lane; i < la && !hit; i += 32) {
-    const BEl p = LA[i];
-    const double px0 = fmin(p.x0, p.x1), px1 = fmax(p.x0, p.x1), py0 = fmin(p.y0, p.y1), py1 = fmax(p.y0, p.y1);
-    for (int j = 0; j < lb && !hit; j++) {
-      const BEl q = LB[j];
-      if (fmax(q.x0, q.x1) < px0 || fmin(q.x0, q.x1) > px1 || fmax(q.y0, q.y1) < py0 || fmin(q.y0, q.y1) > py1) continue;
-      if (!seg_isect(p.x0, p.y0, p.x1, p.y1, q.x0, q.y0, q.x1, q.y1)) continue;
+  if (la && lb) {
+    const unsigned lt = (1u << lane) - 1;
+    uint2* Q = sc.Q;
+    auto cross = [&](uint2 e) {
+      const BEl p = LA[e.x], q = LB[e.y];
+      if (!seg_isect(p.x0, p.y0, p.x1, p.y1, q.x0, q.y0, q.x1, q.y1)) return false;
       double xs[3], ys[3]; const int k = seg_points(p, q, xs, ys);
-      for (int t = 0; t < k && !hit; t++)
-        if (inW(xs[t], ys[t]) && !in_excl(EA, na, rA, xs[t], ys[t], eps) && !in_excl(EB, nb, rB, xs[t], ys[t], eps)) hit = true;
+      for (int t = 0; t < k; t++)
+        if (inW(xs[t], ys[t]) && !in_excl(EA, na, rA, xs[t], ys[t], eps) && !in_excl(EB, nb, rB, xs[t], ys[t], eps)) return true;
+      return false;
+    };
+    const uint64_t tot = (uint64_t)la * (uint64_t)lb;
+    const int di = 32 / lb, dj = 32 % lb;
+    int i = lane / lb, j = lane % lb, qn = 0;
+    for (uint64_t base = 0; base < tot; base += 32) {
+      bool c = false;
+      if (i < la) {
+        const BEl p = LA[i], q = LB[j];
+        c = !(fmax(q.x0, q.x1) < fmin(p.x0, p.x1) || fmin(q.x0, q.x1) > fmax(p.x0, p.x1) || fmax(q.y0, q.y1) < fmin(p.y0, p.y1) ||
+              fmin(q.y0, q.y1) > fmax(p.y0, p.y1));
+      }
+      const unsigned m = __ballot_sync(0xffffffffu, c);
+      if (c) Q[qn + __popc(m & lt)] = make_uint2((unsigned)i, (unsigned)j);
+      qn += __popc(m);
+      i += di; j += dj;
+      if (j >= lb) { j -= lb; i++; }
+      if (qn >= 32) {
+        __syncwarp();
+        if (__any_sync(0xffffffffu, cross(Q[lane]))) return 1;
+        const int rest = qn - 32;
+        const uint2 t = lane < rest ? Q[32 + lane] : make_uint2(0, 0);
+        __syncwarp();
+        if (lane < rest) Q[lane] = t;
+        __syncwarp();
+        qn = rest;
+      }
     }
+    __syncwarp();
+    if (__any_sync(0xffffffffu, lane < qn && cross(Q[lane]))) return 1;
+    __syncwarp();
   }
-  if (__any_sync(0xffffffffu, hit)) return 1;
   // (b), (c) a vertex of one eroded boundary inside the other eroded polygon
   const double cx = Wx0 + 0.381966 * (Wx1 - Wx0), cy = Wy0 + 0.414213 * (Wy1 - Wy0);
   const bool inA_c = pip_parent(P, ga.x, ga.y, F, cx, cy, lane);
@@ -728,6 +762,7 @@ __device__ __forceinline__ ErScratch er_smem(unsigned char* raw, int wib) {
   ErScratch sc;
   sc.EA = reinterpret_cast<BEd*>(base); sc.EB = sc.EA + ER_CAPE;
   sc.LA = reinterpret_cast<BEl*>(sc.EB + ER_CAPE); sc.LB = sc.LA + ER_CAPL;
+  sc.Q = reinterpret_cast<uint2*>(sc.LB + ER_CAPL);
   sc.capE = ER_CAPE; sc.capL = ER_CAPL;
   return sc;
 }
@@ -840,10 +875,11 @@ __global__ void k_erode_slab(DLayer P, DLayer R, const uint32_t* pfP, const uint
                              double ra, double rb, uint8_t* flag, unsigned char* scratch, int capE, int capL, ETile* again, ErCtr* c) {
   const int lane = threadIdx.x & 31;
   const uint64_t w = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
-  unsigned char* base = scratch + w * (2 * (size_t)capE * sizeof(BEd) + 2 * (size_t)capL * sizeof(BEl));
+  unsigned char* base = scratch + w * er_scratch_bytes(capE, capL);
   ErScratch sc;
   sc.EA = reinterpret_cast<BEd*>(base); sc.EB = sc.EA + capE;
   sc.LA = reinterpret_cast<BEl*>(sc.EB + capE); sc.LB = sc.LA + capL;
+  sc.Q = reinterpret_cast<uint2*>(sc.LB + capL);
   sc.capE = capE; sc.capL = capL;
   for (uint64_t i = w; i < ni; i += nw) {
     ETile t = items[i];
@@ -945,7 +981,7 @@ void erode_host(gsj_ctx* c, const gsj_layer* P, const gsj_layer* R, double ra, d
         for (int sround = 0; ns; sround++) {
           if (sround >= 4) throw Error(GSJ_ERR_CUDA, "erosion slab tiles still overflow after 4 rounds");
           const int capE = std::max<int>(hc.needE, ER_CAPE), capL = std::max<int>(std::max<int>(hc.needL, 17 * capE / 4), ER_CAPL);
-          const size_t per = 2 * (size_t)capE * sizeof(BEd) + 2 * (size_t)capL * sizeof(BEl);
+          const size_t per = er_scratch_bytes(capE, capL);
           uint64_t nwarps = std::max<uint64_t>(1, std::min<uint64_t>(ns, (1ull << 30) / per));
           nwarps = (nwarps + 3) / 4 * 4;
           unsigned char* scr = c->er_scr.as<unsigned char>(per * nwarps);
