@@ -384,6 +384,42 @@ __global__ void k_uf_union(const uint2* __restrict__ pairs, uint64_t n, uint32_t
     if (atomicCAS(&par[rb], rb, ra) == rb) return;   // the larger root goes under the smaller: roots are component minima
   }
 }
+constexpr uint32_t CLUSTER_ROUNDS = 8;
+// Cluster rounds (filtered mode): candidate i = t * R + r belongs to round r; it is refined only while its two
+// parents are still in different components. A skipped pair joins two geometries that are already connected, so
+// the components (and root[]) are those of the full intersects graph.
+__global__ void k_cl_select(const uint2* __restrict__ pairs, uint64_t n, uint32_t r, uint32_t R, const uint32_t* __restrict__ parent,
+                            uint32_t* par, uint32_t* keep) {
+  const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x, i = t * R + r;
+  if (i >= n) return;
+  const uint2 p = pairs[i];
+  const uint32_t a = parent ? parent[p.x] : p.x, b = parent ? parent[p.y] : p.y;
+  keep[t] = a != b && uf_find(par, a) != uf_find(par, b);
+}
+__global__ void k_cl_gather(const uint2* __restrict__ pairs, uint64_t n, uint32_t r, uint32_t R, const uint32_t* __restrict__ keep,
+                            const uint32_t* __restrict__ off, uint2* out) {
+  const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x, i = t * R + r;
+  if (i < n && keep[t]) out[off[t]] = pairs[i];
+}
+__global__ void k_cl_union(const uint2* __restrict__ pairs, const uint8_t* __restrict__ flag, uint64_t n, const uint32_t* __restrict__ parent,
+                           uint32_t* par, unsigned long long* hits) {
+  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const bool h = i < n && flag[i];
+  const unsigned m = __ballot_sync(0xffffffffu, h);
+  if ((threadIdx.x & 31) == 0 && m) atomicAdd(hits, (unsigned long long)__popc(m));
+  if (!h) return;
+  uint32_t a = parent ? parent[pairs[i].x] : pairs[i].x, b = parent ? parent[pairs[i].y] : pairs[i].y;
+  for (;;) {
+    uint32_t ra = uf_find(par, a), rb = uf_find(par, b);
+    if (ra == rb) return;
+    if (ra > rb) { uint32_t t = ra; ra = rb; rb = t; }
+    if (atomicCAS(&par[rb], rb, ra) == rb) return;
+  }
+}
+__global__ void k_uf_flatten(uint32_t* par, uint32_t n) {   // concurrent readers see an ancestor either way
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) par[i] = uf_find(par, i);
+}
 __global__ void k_uf_roots(uint32_t* par, uint32_t n, uint32_t* root) {
   uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) root[i] = uf_find(par, i);
@@ -462,9 +498,54 @@ void cluster_host(gsj_ctx* c, const gsj_layer* P, uint32_t nparent, const gsj_jo
   uint32_t* par = c->uf.as<uint32_t>(2 * (size_t)nparent);
   uint32_t* droot = par + nparent;
   k_uf_init<<<grid_for(nparent, 256), 256, 0, s>>>(par, nparent); c->launches++;
-  run_join(c, P, P, rp, o, st, [&](const JoinOut& out) {
-    if (out.n) { k_uf_union<<<grid_for(out.n, 256), 256, 0, s>>>(out.pairs, out.n, par); c->launches++; }
-  });
+  if (o.refine_mode == GSJ_REFINE_PLAIN) {   // every candidate refined, as the reference does
+    run_join(c, P, P, rp, o, st, [&](const JoinOut& out) {
+      if (out.n) { k_uf_union<<<grid_for(out.n, 256), 256, 0, s>>>(out.pairs, out.n, par); c->launches++; }
+    });
+  } else {   // rounds that skip pairs whose parents are already connected
+    Timer tm(s);
+    bool whole = false;
+    const std::vector<Batch> batches = make_batches(P, o, whole);
+    unsigned long long* hits = c->misc3.as<unsigned long long>(1);
+    GSJ_CK(cudaMemsetAsync(hits, 0, sizeof(unsigned long long), s));
+    for (const Batch& bt : batches) {
+      if (o.cancel && *o.cancel) throw Error(GSJ_ERR_CANCELLED, "cancelled");
+      tm.start();
+      uint2* pairs = nullptr;
+      const uint64_t np = candidates_for(c, P->d.bb, whole ? P->bvh.order : nullptr, bt.q0, bt.nq, P->bvh, 1, &pairs);
+      st.traverse_ms += tm.stop();
+      st.candidates += np;
+      st.batches++;
+      if (!np) continue;
+      const uint32_t R = np < (1u << 16) ? 1 : CLUSTER_ROUNDS;
+      for (uint32_t r = 0; r < R; r++) {
+        if (o.cancel && *o.cancel) throw Error(GSJ_ERR_CANCELLED, "cancelled");
+        tm.start();
+        const uint64_t nt = (np - r + R - 1) / R;   // candidates r, r + R, ... < np
+        uint32_t* keep = c->keep.as<uint32_t>(nt);
+        uint32_t* off = c->idx.as<uint32_t>(nt);
+        k_cl_select<<<grid_for(nt, 256), 256, 0, s>>>(pairs, np, r, R, P->d.parent, par, keep); c->launches++;
+        exclusive_scan(c, keep, off, nt);
+        const uint64_t ns = read_last(c, off, keep, nt);
+        uint2* sel = c->opairs.as<uint2>(ns);
+        if (ns) { k_cl_gather<<<grid_for(nt, 256), 256, 0, s>>>(pairs, np, r, R, keep, off, sel); c->launches++; }
+        st.compact_ms += tm.stop();
+        if (!ns) continue;
+        tm.start();
+        uint8_t* flag = c->flag.as<uint8_t>(ns);
+        st.heavy += refine(c, P, P, sel, ns, rp, o.refine_mode, flag, nullptr, nullptr, nullptr);
+        st.refine_ms += tm.stop();
+        tm.start();
+        k_cl_union<<<grid_for(ns, 256), 256, 0, s>>>(sel, flag, ns, P->d.parent, par, hits); c->launches++;
+        k_uf_flatten<<<grid_for(nparent, 256), 256, 0, s>>>(par, nparent); c->launches++;
+        st.compact_ms += tm.stop();
+      }
+    }
+    unsigned long long hh = 0;
+    GSJ_CK(cudaMemcpyAsync(&hh, hits, sizeof(hh), cudaMemcpyDeviceToHost, s));
+    GSJ_CK(cudaStreamSynchronize(s));
+    st.hits = hh;
+  }
   k_uf_roots<<<grid_for(nparent, 256), 256, 0, s>>>(par, nparent, droot); c->launches++;
   GSJ_CK(cudaGetLastError());
   GSJ_CK(cudaMemcpyAsync(root, droot, (size_t)nparent * 4, cudaMemcpyDeviceToHost, s));

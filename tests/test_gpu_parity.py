@@ -116,6 +116,38 @@ def test_cluster(engine, layers):
     assert root.tolist() == [0, 0, 0, 3, 3]
 
 
+def shrunk_parcels(n, box, seed, frac=0.55, f=0.9):
+    """Parcels with a seeded fraction shrunk by f toward their bbox centre. Only neighbours that both keep their
+    size touch, so the intersects graph falls into components of every size (site percolation)."""
+    ps = gen.layer_parcels(n, box, seed=seed)
+    shrink = np.random.default_rng(seed).random(ps.n) < frac
+    ring_g = np.repeat(np.arange(ps.n), np.diff(ps.gro).astype(np.int64))
+    vg = ring_g[np.repeat(np.arange(len(ps.rvo) - 1), np.diff(ps.rvo).astype(np.int64))]
+    lo, hi = np.full((ps.n, 2), np.inf), np.full((ps.n, 2), -np.inf)
+    np.minimum.at(lo, vg, ps.xy)
+    np.maximum.at(hi, vg, ps.xy)
+    c = 0.5 * (lo + hi)
+    m = shrink[vg]
+    xy = ps.xy.copy()
+    xy[m] = c[vg[m]] + f * (xy[m] - c[vg[m]])
+    return gen.PolygonSet(ps.gro, ps.rvo, xy)
+
+
+@pytest.mark.parametrize("mode", MODES)
+def test_cluster_many_components(engine, mode):
+    """More than 65536 candidates (the filtered cluster then refines in rounds that skip pairs already connected)
+    and components of every size: roots equal the oracle's, for the whole layer and for its pieces."""
+    ps = shrunk_parcels(40000, (-118.3, 33.95, -118.1, 34.15), seed=11)
+    want = O.cluster(O.OSet(ps), ps.n)
+    sizes = np.unique(want, return_counts=True)[1]
+    assert (sizes >= 2).sum() > 500 and (sizes >= 100).sum() > 5
+    root, st = engine.cluster(engine.upload_polygons(ps), refine_mode=mode)
+    assert st["candidates"] > 1 << 16 and np.array_equal(root, want)
+    sub = gsj.subdivide(ps, 12)
+    root, st = engine.cluster(engine.upload_polygons(sub), ps.n, refine_mode=mode)
+    assert st["candidates"] > 1 << 16 and np.array_equal(root, O.cluster(O.OSet(sub), ps.n))
+
+
 def test_bad_arguments_are_errors(engine, layers):
     with pytest.raises(gsj.GsjError):
         engine.join(layers["parcels"][0], engine.upload_points(np.zeros((3, 2))))
