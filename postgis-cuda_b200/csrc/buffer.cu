@@ -639,9 +639,11 @@ __device__ int seg_points(const BEl& p, const BEl& q, double* xs, double* ys) { 
 }
 
 // X_A meets X_B within the window (intersected with tile when given): 1 / 0, or -1 when a list overflowed
-// (needE / needL = sizes required, *wout = the window tested) (buffer.cuh:499-588)
+// (needE / needL = sizes required, *wout = the window tested) (buffer.cuh:499-588). mirror: B is A (same layer,
+// same pieces, same radius), so B's edge and element lists, centre test and vertex pass are A's and are not
+// built twice; every value they would hold is computed from the same inputs by the same code.
 __device__ int er_pair(const DLayer& P, const DLayer& R, uint2 ga, uint2 gb, double ra_nom, double rb_nom, const ErScratch& sc, int lane, int* needE,
-                       int* needL, const double4* tile, double4* wout) {
+                       int* needL, const double4* tile, double4* wout, bool mirror) {
   if (ga.x >= ga.y || gb.x >= gb.y) return 0;
   double abx0 = 1e300, aby0 = 1e300, abx1 = -1e300, aby1 = -1e300, bbx0 = 1e300, bby0 = 1e300, bbx1 = -1e300, bby1 = -1e300;
   for (uint32_t g = ga.x; g < ga.y; g++) {
@@ -654,7 +656,7 @@ __device__ int er_pair(const DLayer& P, const DLayer& R, uint2 ga, uint2 gb, dou
   }
   double dax, day, dbx, dby;
   deg_cover(aby0, aby1, ra_nom * 0.998, false, dax, day);   // shrink by a lower bound of the true radius
-  deg_cover(bby0, bby1, rb_nom * 0.998, false, dbx, dby);
+  if (mirror) { dbx = dax; dby = day; } else deg_cover(bby0, bby1, rb_nom * 0.998, false, dbx, dby);
   double wx0 = fmax(abx0 + dax, bbx0 + dbx), wx1 = fmin(abx1 - dax, bbx1 - dbx);
   double wy0 = fmax(aby0 + day, bby0 + dby), wy1 = fmin(aby1 - day, bby1 - dby);
   if (tile) { wx0 = fmax(wx0, tile->x); wy0 = fmax(wy0, tile->y); wx1 = fmin(wx1, tile->z); wy1 = fmin(wy1, tile->w); }
@@ -662,7 +664,7 @@ __device__ int er_pair(const DLayer& P, const DLayer& R, uint2 ga, uint2 gb, dou
   if (wout) *wout = make_double4(wx0, wy0, wx1, wy1);
   const double clon = 0.5 * (wx0 + wx1), clat = 0.5 * (wy0 + wy1);
   const double rA = ra_nom > 0 ? ra_nom / utm_k(0.5 * (abx0 + abx1), 0.5 * (aby0 + aby1), clon, clat) : 0.0;
-  const double rB = rb_nom > 0 ? rb_nom / utm_k(0.5 * (bbx0 + bbx1), 0.5 * (bby0 + bby1), clon, clat) : 0.0;
+  const double rB = mirror ? rA : rb_nom > 0 ? rb_nom / utm_k(0.5 * (bbx0 + bbx1), 0.5 * (bby0 + bby1), clon, clat) : 0.0;
   EFrame F; { const double2 o = P.origin[ga.x]; F.ox = o.x; F.oy = o.y; } m_per_deg(clat, F.kx, F.ky);
   const double Wx0 = (wx0 - F.ox) * F.kx, Wx1 = (wx1 - F.ox) * F.kx, Wy0 = (wy0 - F.oy) * F.ky, Wy1 = (wy1 - F.oy) * F.ky;
   const double ext = fmax(fmax(fabs(Wx0), fabs(Wx1)), fmax(fabs(Wy0), fabs(Wy1))) + fmax(rA, rB);
@@ -670,16 +672,17 @@ __device__ int er_pair(const DLayer& P, const DLayer& R, uint2 ga, uint2 gb, dou
   const double fe = 1.0 + 2.0 * 0.5 * (wy1 - wy0) * DEG * (fabs(tan(clat * DEG)) + 0.05);
   const double ma = rA * fe + 1e-6, mb = rB * fe + 1e-6;
   const int na = collect_side(P, ga.x, ga.y, F, Wx0 - ma, Wy0 - ma, Wx1 + ma, Wy1 + ma, sc.EA, sc.capE, lane);
-  const int nb = collect_side(R, gb.x, gb.y, F, Wx0 - mb, Wy0 - mb, Wx1 + mb, Wy1 + mb, sc.EB, sc.capE, lane);
+  BEd* const EBw = mirror ? sc.EA : sc.EB;
+  const int nb = mirror ? na : collect_side(R, gb.x, gb.y, F, Wx0 - mb, Wy0 - mb, Wx1 + mb, Wy1 + mb, EBw, sc.capE, lane);
   if (na > sc.capE || nb > sc.capE) { if (needE) *needE = max(na, nb); return -1; }
   __syncwarp();
   prepare_side(sc.EA, na, rA, lane);
-  prepare_side(sc.EB, nb, rB, lane);
+  if (!mirror) prepare_side(EBw, nb, rB, lane);
   const int la = build_elements(sc.EA, na, rA, Wx0, Wy0, Wx1, Wy1, eps, sc.LA, sc.capL, lane);
-  const int lb = build_elements(sc.EB, nb, rB, Wx0, Wy0, Wx1, Wy1, eps, sc.LB, sc.capL, lane);
+  const int lb = mirror ? la : build_elements(EBw, nb, rB, Wx0, Wy0, Wx1, Wy1, eps, sc.LB, sc.capL, lane);
   if (la > sc.capL || lb > sc.capL) { if (needE) *needE = max(na, nb); if (needL) *needL = max(la, lb); return -1; }
   __syncwarp();
-  const BEd* EA = sc.EA; const BEd* EB = sc.EB; const BEl* LA = sc.LA; const BEl* LB = sc.LB;
+  const BEd* EA = sc.EA; const BEd* EB = EBw; const BEl* LA = sc.LA; const BEl* LB = mirror ? sc.LA : sc.LB;
   auto inW = [&](double x, double y) { return x >= Wx0 - eps && x <= Wx1 + eps && y >= Wy0 - eps && y <= Wy1 + eps; };
   // (a) the eroded boundaries cross outside both exclusion zones. The la x lb element grid is scanned 32 cells a
   // wave; cells whose boxes overlap are queued and tested 32 at a time, one per lane, so that the warp runs the
@@ -693,7 +696,7 @@ __device__ int er_pair(const DLayer& P, const DLayer& R, uint2 ga, uint2 gb, dou
       if (!seg_isect(p.x0, p.y0, p.x1, p.y1, q.x0, q.y0, q.x1, q.y1)) return false;
       double xs[3], ys[3]; const int k = seg_points(p, q, xs, ys);
       for (int t = 0; t < k; t++)
-        if (inW(xs[t], ys[t]) && !in_excl(EA, na, rA, xs[t], ys[t], eps) && !in_excl(EB, nb, rB, xs[t], ys[t], eps)) return true;
+        if (inW(xs[t], ys[t]) && !in_excl(EA, na, rA, xs[t], ys[t], eps) && (mirror || !in_excl(EB, nb, rB, xs[t], ys[t], eps))) return true;
       return false;
     };
     const uint64_t tot = (uint64_t)la * (uint64_t)lb;
@@ -729,8 +732,8 @@ __device__ int er_pair(const DLayer& P, const DLayer& R, uint2 ga, uint2 gb, dou
   // (b), (c) a vertex of one eroded boundary inside the other eroded polygon
   const double cx = Wx0 + 0.381966 * (Wx1 - Wx0), cy = Wy0 + 0.414213 * (Wy1 - Wy0);
   const bool inA_c = pip_parent(P, ga.x, ga.y, F, cx, cy, lane);
-  const bool inB_c = pip_parent(R, gb.x, gb.y, F, cx, cy, lane);
-  for (int side = 0; side < 2; side++) {
+  const bool inB_c = mirror ? inA_c : pip_parent(R, gb.x, gb.y, F, cx, cy, lane);
+  for (int side = 0; side < (mirror ? 1 : 2); side++) {
     const BEd* ES = side ? EB : EA; const BEd* EO = side ? EA : EB;
     const BEl* LS = side ? LB : LA;
     const int ns = side ? nb : na, no = side ? na : nb, ls = side ? lb : la;
@@ -820,13 +823,16 @@ __global__ void k_er_filter(const uint2* __restrict__ pr, const double* __restri
   keep[i] = k;
 }
 __global__ void __launch_bounds__(ER_WARPS * 32) k_erode_main(DLayer P, DLayer R, const uint32_t* pfP, const uint32_t* pfR, const uint2* __restrict__ pairs,
-                                                              uint64_t np, double ra, double rb, uint8_t* flag, uint32_t* heavy, unsigned int* nheavy) {
+                                                              uint64_t np, double ra, double rb, bool self_layer, uint8_t* flag, uint32_t* heavy,
+                                                              unsigned int* nheavy) {
   extern __shared__ __align__(16) unsigned char smem[];
   const int lane = threadIdx.x & 31;
   const ErScratch sc = er_smem(smem, threadIdx.x >> 5);
   const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
   for (uint64_t p = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; p < np; p += nw) {
-    const int r = er_pair(P, R, piece_range(pfP, pairs[p].x), piece_range(pfR, pairs[p].y), ra, rb, sc, lane, nullptr, nullptr, nullptr, nullptr);
+    const uint2 pr = pairs[p];
+    const int r = er_pair(P, R, piece_range(pfP, pr.x), piece_range(pfR, pr.y), ra, rb, sc, lane, nullptr, nullptr, nullptr, nullptr,
+                          self_layer && pr.x == pr.y);
     if (lane == 0) { flag[p] = r > 0 ? 1 : 0; if (r < 0) heavy[atomicAdd(nheavy, 1u)] = (uint32_t)p; }
     __syncwarp();
   }
@@ -852,8 +858,8 @@ __device__ void er_overflow(uint32_t p, uint32_t depth, double4 w, double rmax, 
   }
 }
 __global__ void __launch_bounds__(ER_WARPS * 32) k_erode_tiles(DLayer P, DLayer R, const uint32_t* pfP, const uint32_t* pfR, const uint2* __restrict__ pairs,
-                                                               const ETile* items, uint64_t ni, double ra, double rb, uint8_t* flag, ETile* next, ETile* slab,
-                                                               ErCtr* c) {
+                                                               const ETile* items, uint64_t ni, double ra, double rb, bool self_layer, uint8_t* flag,
+                                                               ETile* next, ETile* slab, ErCtr* c) {
   extern __shared__ __align__(16) unsigned char smem[];
   const int lane = threadIdx.x & 31;
   const ErScratch sc = er_smem(smem, threadIdx.x >> 5);
@@ -862,7 +868,8 @@ __global__ void __launch_bounds__(ER_WARPS * 32) k_erode_tiles(DLayer P, DLayer 
     ETile t = items[i];
     if (flag[t.pair]) continue;   // another tile already found an intersection
     int ne = 0, nl = 0; double4 win = t.box;
-    const int r = er_pair(P, R, piece_range(pfP, pairs[t.pair].x), piece_range(pfR, pairs[t.pair].y), ra, rb, sc, lane, &ne, &nl, &t.box, &win);
+    const uint2 pr = pairs[t.pair];
+    const int r = er_pair(P, R, piece_range(pfP, pr.x), piece_range(pfR, pr.y), ra, rb, sc, lane, &ne, &nl, &t.box, &win, self_layer && pr.x == pr.y);
     if (lane == 0) {
       if (r > 0) flag[t.pair] = 1;
       else if (r < 0) er_overflow(t.pair, t.depth, win, fmax(ra, rb), ne, nl, next, slab, c);
@@ -872,7 +879,7 @@ __global__ void __launch_bounds__(ER_WARPS * 32) k_erode_tiles(DLayer P, DLayer 
 }
 // tiles that cannot usefully be split: per-warp lists in global scratch sized by the reported need
 __global__ void k_erode_slab(DLayer P, DLayer R, const uint32_t* pfP, const uint32_t* pfR, const uint2* __restrict__ pairs, const ETile* items, uint64_t ni,
-                             double ra, double rb, uint8_t* flag, unsigned char* scratch, int capE, int capL, ETile* again, ErCtr* c) {
+                             double ra, double rb, bool self_layer, uint8_t* flag, unsigned char* scratch, int capE, int capL, ETile* again, ErCtr* c) {
   const int lane = threadIdx.x & 31;
   const uint64_t w = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
   unsigned char* base = scratch + w * er_scratch_bytes(capE, capL);
@@ -885,7 +892,8 @@ __global__ void k_erode_slab(DLayer P, DLayer R, const uint32_t* pfP, const uint
     ETile t = items[i];
     if (flag[t.pair]) continue;
     int ne = 0, nl = 0;
-    const int r = er_pair(P, R, piece_range(pfP, pairs[t.pair].x), piece_range(pfR, pairs[t.pair].y), ra, rb, sc, lane, &ne, &nl, &t.box, nullptr);
+    const uint2 pr = pairs[t.pair];
+    const int r = er_pair(P, R, piece_range(pfP, pr.x), piece_range(pfR, pr.y), ra, rb, sc, lane, &ne, &nl, &t.box, nullptr, self_layer && pr.x == pr.y);
     if (lane == 0) {
       if (r > 0) flag[t.pair] = 1;
       else if (r < 0) { again[atomicAdd(&c->nslab, 1u)] = t; atomicMax(&c->needE, ne); atomicMax(&c->needL, nl); }
@@ -925,6 +933,7 @@ void erode_host(gsj_ctx* c, const gsj_layer* P, const gsj_layer* R, double ra, d
     c->er_attr = 1;
   }
   const double rmin = (ra > 0 && rb > 0) ? std::min(ra, rb) : (ra > 0 || rb > 0 ? 0.0 : -1.0);
+  const bool self_layer = P == R && ra == rb;   // a pair (g, g) then erodes one geometry against itself
   RefineArgs rp{1e-12, 1e-7, 1e-11, 1, 0, 0};
   PairsOut emit{c, sink, user, &st};
   PrefilterFn pre;
@@ -955,7 +964,7 @@ void erode_host(gsj_ctx* c, const gsj_layer* P, const gsj_layer* R, double ra, d
     ErCtr* ctr = c->er_ctr.as<ErCtr>(2);
     GSJ_CK(cudaMemsetAsync(ctr, 0, sizeof(ErCtr), s));
     const int G = (int)std::min<uint64_t>((ne * 32 + 63) / 64, (uint64_t)c->sm_count * 32);
-    k_erode_main<<<G, ER_WARPS * 32, ER_SMEM, s>>>(P->d, R->d, pfP, pfR, ep, ne, ra, rb, flag, heavy, &ctr->ntile); c->launches++;
+    k_erode_main<<<G, ER_WARPS * 32, ER_SMEM, s>>>(P->d, R->d, pfP, pfR, ep, ne, ra, rb, self_layer, flag, heavy, &ctr->ntile); c->launches++;
     GSJ_CK(cudaGetLastError());
     ErCtr h{};
     GSJ_CK(cudaMemcpyAsync(&h, ctr, sizeof(ErCtr), cudaMemcpyDeviceToHost, s));
@@ -972,7 +981,7 @@ void erode_host(gsj_ctx* c, const gsj_layer* P, const gsj_layer* R, double ra, d
         ETile* slab = c->er_slab.as<ETile>(ni);
         GSJ_CK(cudaMemsetAsync(ctr, 0, sizeof(ErCtr), s));
         const int GT = (int)std::min<uint64_t>((ni * 32 + 63) / 64, (uint64_t)c->sm_count * 32);
-        k_erode_tiles<<<GT, ER_WARPS * 32, ER_SMEM, s>>>(P->d, R->d, pfP, pfR, ep, items, ni, ra, rb, flag, next, slab, ctr); c->launches++;
+        k_erode_tiles<<<GT, ER_WARPS * 32, ER_SMEM, s>>>(P->d, R->d, pfP, pfR, ep, items, ni, ra, rb, self_layer, flag, next, slab, ctr); c->launches++;
         GSJ_CK(cudaGetLastError());
         ErCtr hc{};
         GSJ_CK(cudaMemcpyAsync(&hc, ctr, sizeof(ErCtr), cudaMemcpyDeviceToHost, s));
@@ -988,7 +997,7 @@ void erode_host(gsj_ctx* c, const gsj_layer* P, const gsj_layer* R, double ra, d
           // ping-pong between er_again and er_tiles (this round's tiles are consumed by now)
           ETile* again = (sround % 2 ? c->er_tiles : c->er_again).as<ETile>(ns);
           GSJ_CK(cudaMemsetAsync(ctr, 0, sizeof(ErCtr), s));
-          k_erode_slab<<<(int)(nwarps / 4), 128, 0, s>>>(P->d, R->d, pfP, pfR, ep, slab, ns, ra, rb, flag, scr, capE, capL, again, ctr); c->launches++;
+          k_erode_slab<<<(int)(nwarps / 4), 128, 0, s>>>(P->d, R->d, pfP, pfR, ep, slab, ns, ra, rb, self_layer, flag, scr, capE, capL, again, ctr); c->launches++;
           GSJ_CK(cudaGetLastError());
           ErCtr h2{};
           GSJ_CK(cudaMemcpyAsync(&h2, ctr, sizeof(ErCtr), cudaMemcpyDeviceToHost, s));
