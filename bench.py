@@ -211,8 +211,15 @@ def serving_schedule(rng, qpoly, qpts):
     return "\n".join(lines) + "\n"
 
 
+SERVE_ARMS = (   # name -> gsjd flags; the same daemon, schedule and priming, only the refinement differs
+    ("filtered", ["--refine", "filtered"]),
+    ("plain", ["--refine", "plain"]),
+)
+
+
 def serving_leg(ps, n_points=1_000_000, workers=4):
-    """gsjd serving a Poisson request stream against the resident layer, filtered and plain refinement."""
+    """gsjd serving a Poisson request stream against the resident layer, filtered and plain FP64 refinement on the
+    same schedule, each after an untimed priming pass over the schedule's distinct requests."""
     import shutil
     import tempfile
     from gsj import client as C
@@ -241,12 +248,15 @@ def serving_leg(ps, n_points=1_000_000, workers=4):
             qsizes.append(n)
         sched = os.path.join(d, "schedule.tsv")
         open(sched, "w").write(serving_schedule(rng, qpoly, qpts))
+        distinct = sorted({ln.split("\t", 1)[1] for ln in open(sched).read().splitlines() if ln})
+        prime = os.path.join(d, "prime.tsv")
+        open(prime, "w").write("".join(f"{0.02 * (i // 8):.3f}\t{req}\n" for i, req in enumerate(distinct * 2)))
         prep_s = time.time() - t0
         out = {}
-        for mode in ("filtered", "plain"):
+        for mode, flags in SERVE_ARMS:
             sock = os.path.join(d, f"gsjd_{mode}.sock")
             log = open(os.path.join(d, f"gsjd_{mode}.log"), "w")
-            p = D.start(sock, d, workers=workers, threads=max(4, (os.cpu_count() or 8) // 2), log=log, extra=["--refine", mode])
+            p = D.start(sock, d, workers=workers, threads=max(4, (os.cpu_count() or 8) // 2), log=log, extra=flags)
             try:
                 cl = C.Client(sock)
                 cl.load("resident", "resident.gset", dedup=False)
@@ -254,6 +264,9 @@ def serving_leg(ps, n_points=1_000_000, workers=4):
                     cl.load(q, q + ".gset", dedup=False)
                 for q in qpts:
                     cl.load(q, q + ".pset")
+                # untimed priming: every distinct request of the schedule, 8 at a time, so each context has grown
+                # its scratch for the largest requests before the measured replay (steady-state serving)
+                subprocess.run([lib_path("gsjd_loadgen"), "--socket", sock, "--schedule", prime], capture_output=True, text=True, timeout=900)
                 r = subprocess.run([lib_path("gsjd_loadgen"), "--socket", sock, "--schedule", sched, "--warmup", str(SERVE_WARMUP)],
                                    capture_output=True, text=True, timeout=900)
                 res = json.loads(r.stdout.strip().splitlines()[-1])

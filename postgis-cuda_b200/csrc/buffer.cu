@@ -385,13 +385,14 @@ void dwithin_host(gsj_ctx* c, const gsj_layer* P, const gsj_layer* R, double d, 
   PairsOut emit{c, sink, user, &st};
   const uint32_t n = P->d.n;
   const bool whole = !o.batch_q || o.batch_q >= n;
+  const bool morton = whole || P->h_parent.empty();   // batches of a layer without parents: runs of Morton positions
   for (uint32_t q0 = 0, qn; q0 < n; q0 = qn) {
     qn = whole ? n : std::min<uint32_t>(q0 + o.batch_q, n);
     if (!whole && !P->h_parent.empty()) while (qn < n && P->h_parent[qn] == P->h_parent[qn - 1]) qn++;
     if (o.cancel && *o.cancel) throw Error(GSJ_ERR_CANCELLED, "cancelled");
     tm.start();
     uint2* pairs = nullptr;
-    const uint64_t np = candidates_for(c, qbb, whole ? P->bvh.order : nullptr, q0, qn - q0, R->bvh, o.upper, &pairs);
+    const uint64_t np = candidates_for(c, qbb, morton ? P->bvh.order : nullptr, q0, qn - q0, R->bvh, o.upper, &pairs);
     st.traverse_ms += tm.stop(); st.candidates += np; st.batches++;
     if (!np) continue;
     tm.start();
@@ -1136,7 +1137,7 @@ void points_buffer_host(gsj_ctx* c, const gsj_layer* pts, const gsj_layer* R, do
     const uint32_t nq = std::min(bq, n - q0);
     tm.start();
     uint2* pairs = nullptr;
-    const uint64_t np = candidates_for(c, qbb, bq == n ? pts->bvh.order : nullptr, q0, nq, R->bvh, 0, &pairs);
+    const uint64_t np = candidates_for(c, qbb, pts->bvh.order, q0, nq, R->bvh, 0, &pairs);   // runs of Morton positions
     st.traverse_ms += tm.stop(); st.candidates += np; st.batches++;
     if (!np) continue;
     tm.start();

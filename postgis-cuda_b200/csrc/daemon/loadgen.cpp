@@ -3,7 +3,10 @@
 // result stream to its end, and prints a JSON summary of the latencies (arrival to end of stream, so time spent
 // queueing in the daemon counts) and row counts.
 //
-//   gsjd_loadgen --socket PATH [--token TOKEN] --schedule FILE [--warmup N]
+//   gsjd_loadgen --socket PATH [--token TOKEN] --schedule FILE [--warmup N] [--detail FILE]
+//
+// --detail writes one TSV line per request: index, op, first argument (the query layer), arrival s, latency ms
+// (-1 on error), rows, first-row ms (arrival to the first frame header), and the daemon's stats JSON.
 //
 // Schedule lines: <arrival seconds> TAB <op name> TAB <arg> TAB <arg> ...   (op: JOIN RELATE DWITHIN CLUSTER)
 #include <sys/socket.h>
@@ -38,8 +41,9 @@ struct Req {
   std::vector<std::string> args;
 };
 struct Result {
-  double latency_s = -1;
+  double latency_s = -1, first_s = -1;
   uint64_t rows = 0;
+  std::string stats;
   bool ok = false;
   std::string err;
 };
@@ -57,7 +61,15 @@ class Sock {
     }
     return true;
   }
-  bool read(void* p, size_t n) {   // buffered
+  bool read(void* p, size_t n) {   // buffered; the common case is a copy out of the buffer
+    if (len_ - pos_ >= n) { std::memcpy(p, buf_ + pos_, n); pos_ += n; return true; }
+    return read_slow(p, n);
+  }
+  bool skip(size_t n) {
+    if (len_ - pos_ >= n) { pos_ += n; return true; }
+    return skip_slow(n);
+  }
+  bool read_slow(void* p, size_t n) {
     char* o = static_cast<char*>(p);
     while (n) {
       if (pos_ == len_) {
@@ -71,7 +83,7 @@ class Sock {
     }
     return true;
   }
-  bool skip(size_t n) {
+  bool skip_slow(size_t n) {
     while (n) {
       if (pos_ == len_) {
         const ssize_t r = ::read(fd_, buf_, sizeof buf_);
@@ -93,7 +105,7 @@ class Sock {
 
  private:
   int fd_;
-  char buf_[1 << 16];
+  char buf_[1 << 20];
   size_t pos_ = 0, len_ = 0;
 };
 
@@ -125,6 +137,7 @@ Result run(const Req& q, Clock::time_point arrival) {
   for (;;) {
     uint32_t n;
     if (!s.u32(n)) { res.err = "stream cut"; return res; }
+    if (res.first_s < 0) res.first_s = std::chrono::duration<double>(Clock::now() - arrival).count();
     if (n == GSP_FRAME_ERR) { s.str(res.err); return res; }
     if (n == 0) break;
     for (uint32_t i = 0; i < n; i++) {
@@ -135,8 +148,7 @@ Result run(const Req& q, Clock::time_point arrival) {
     }
     res.rows += n;
   }
-  std::string stats;
-  if (!s.str(stats)) { res.err = "no stats"; return res; }
+  if (!s.str(res.stats)) { res.err = "no stats"; return res; }
   res.latency_s = std::chrono::duration<double>(Clock::now() - arrival).count();
   res.ok = true;
   return res;
@@ -161,7 +173,7 @@ uint32_t op_code(const std::string& s) {
 }  // namespace
 
 int main(int argc, char** argv) {
-  std::string sched;
+  std::string sched, detail;
   size_t warmup = 0;
   for (int i = 1; i < argc; i++) {
     const std::string a = argv[i];
@@ -169,7 +181,8 @@ int main(int argc, char** argv) {
     else if (a == "--token" && i + 1 < argc) g_token = argv[++i];
     else if (a == "--schedule" && i + 1 < argc) sched = argv[++i];
     else if (a == "--warmup" && i + 1 < argc) warmup = (size_t)atol(argv[++i]);
-    else { fprintf(stderr, "usage: gsjd_loadgen --socket PATH [--token T] --schedule FILE [--warmup N]\n"); return 2; }
+    else if (a == "--detail" && i + 1 < argc) detail = argv[++i];
+    else { fprintf(stderr, "usage: gsjd_loadgen --socket PATH [--token T] --schedule FILE [--warmup N] [--detail FILE]\n"); return 2; }
   }
   std::ifstream f(sched);
   if (!f) { fprintf(stderr, "cannot read schedule %s\n", sched.c_str()); return 2; }
@@ -199,6 +212,15 @@ int main(int argc, char** argv) {
   }
   for (auto& t : th) t.join();
   const double span = std::chrono::duration<double>(Clock::now() - t0).count();
+  if (!detail.empty()) {
+    FILE* df = fopen(detail.c_str(), "w");
+    if (!df) { fprintf(stderr, "cannot write %s\n", detail.c_str()); return 2; }
+    for (size_t i = 0; i < res.size(); i++)
+      fprintf(df, "%zu\t%s\t%s\t%.6f\t%.4f\t%llu\t%.4f\t%s\n", i, reqs[i].name.c_str(), reqs[i].args.empty() ? "" : reqs[i].args[0].c_str(),
+              reqs[i].t, res[i].ok ? 1e3 * res[i].latency_s : -1.0, (unsigned long long)res[i].rows, 1e3 * res[i].first_s,
+              res[i].stats.c_str());
+    fclose(df);
+  }
   std::vector<double> lat;
   std::map<std::string, std::vector<double>> per;
   uint64_t rows = 0, errors = 0;

@@ -3,7 +3,9 @@
 // daemon/gpujoind.cu (lines cited per function); the encoding follows daemon/protocol.h.
 #pragma once
 #include <cstdint>
+#include <algorithm>
 #include <cstring>
+#include <memory>
 #include <string>
 #include <vector>
 
@@ -61,28 +63,45 @@ inline uint64_t pair_row_count(uint32_t a, uint32_t b, const Members& A, const M
 }
 
 // Frames of rows: { u32 nrows, rows } closed once they hold GSP_FRAME_BYTES (FrameBuf, gpujoind.cu:178-190).
+// A raw grow-only buffer: one capacity check and one copy per field; reset() keeps the capacity for the next
+// request.
 class FrameWriter {
  public:
-  std::string out;
   uint64_t rows = 0;
-  void begin() { fstart_ = out.size(); out.append(4, '\0'); cnt_ = 0; }
+  const char* data() const { return buf_.get(); }
+  size_t size() const { return len_; }
+  void reset() { len_ = 0; rows = 0; fstart_ = 0; cnt_ = 0; }
+  void reserve(size_t n) { if (n > cap_) grow(n); }
+  void begin() { fstart_ = len_; ensure(4); len_ += 4; cnt_ = 0; }
   void id(const char* p, size_t n) {
     const uint16_t l = (uint16_t)(n < 65535 ? n : 65535);
-    out.append(reinterpret_cast<const char*>(&l), 2);
-    out.append(p, l);
+    ensure(2 + (size_t)l);
+    std::memcpy(buf_.get() + len_, &l, 2);
+    std::memcpy(buf_.get() + len_ + 2, p, l);
+    len_ += 2 + (size_t)l;
   }
-  void f64(double x) { out.append(reinterpret_cast<const char*>(&x), 8); }
-  void u32(uint32_t x) { out.append(reinterpret_cast<const char*>(&x), 4); }
-  void raw(const char* p, size_t n) { out.append(p, n); }
+  void f64(double x) { put(&x, 8); }
+  void u32(uint32_t x) { put(&x, 4); }
+  void raw(const char* p, size_t n) { put(p, n); }
   void row_done() {
     cnt_++; rows++;
-    if (out.size() - fstart_ >= GSP_FRAME_BYTES) { close(); begin(); }
+    if (len_ - fstart_ >= GSP_FRAME_BYTES) { close(); begin(); }
   }
-  void finish() { if (cnt_) close(); else out.resize(fstart_); }
+  void finish() { if (cnt_) close(); else len_ = fstart_; }
 
  private:
-  void close() { std::memcpy(&out[fstart_], &cnt_, 4); }
-  size_t fstart_ = 0;
+  void put(const void* p, size_t n) { ensure(n); std::memcpy(buf_.get() + len_, p, n); len_ += n; }
+  void ensure(size_t n) { if (len_ + n > cap_) grow(len_ + n); }
+  void grow(size_t need) {
+    const size_t c = std::max(need, 2 * cap_ + 4096);
+    std::unique_ptr<char[]> b(new char[c]);
+    if (len_) std::memcpy(b.get(), buf_.get(), len_);
+    buf_ = std::move(b);
+    cap_ = c;
+  }
+  void close() { std::memcpy(buf_.get() + fstart_, &cnt_, 4); }
+  std::unique_ptr<char[]> buf_;
+  size_t len_ = 0, cap_ = 0, fstart_ = 0;
   uint32_t cnt_ = 0;
 };
 

@@ -9,6 +9,11 @@
 //    queueing behind one device lock (g_gpu, gpujoind.cu:35). Small requests use high-priority streams. Admission
 //    is first come, first served per pool, as a context and the request's scratch-memory estimate (within
 //    --mem-budget-gb) become free.
+//  - optionally, rows stream while the GPU works: with --stream-batch N, JOIN, RELATE and DWITHIN run in probe
+//    batches of N query geometries and each batch's rows are encoded and written by a sender thread while the
+//    engine refines the next batch. The default (0) is the reference's scheme: one batch, rows sent after it.
+//  - rows are encoded by a pool of --threads encoder threads started once, into per-thread buffers kept across
+//    requests; every engine context is created at start-up.
 #include <arpa/inet.h>
 #include <netinet/in.h>
 #include <netinet/tcp.h>
@@ -26,6 +31,8 @@
 #include <cmath>
 #include <condition_variable>
 #include <csignal>
+#include <deque>
+#include <functional>
 #include <cstdarg>
 #include <cstdio>
 #include <cstdlib>
@@ -58,6 +65,7 @@ struct Config {
   int device = 0, workers = 2, threads = 16;
   int refine_mode = GSJ_REFINE_FILTERED;
   double mem_budget_gb = 0;   // scratch budget shared by running requests (0: half of the free memory at first use)
+  uint32_t stream_batch = 0;   // probe geometries per engine batch when rows are streamed (0: one batch)
 };
 Config g_cfg;
 std::atomic<bool> g_stop{false};
@@ -127,18 +135,10 @@ class GpuPool {
     gsj_ctx* c = nullptr;
     if (!free_.empty()) { c = free_.back(); free_.pop_back(); }
     else {
-      const int rc = gsj_ctx_create_prio(g_cfg.device, high_, &c);
+      const int rc = create(&c);
       if (rc) {
         cv_.notify_all();
         throw std::runtime_error("no usable CUDA device " + std::to_string(g_cfg.device) + " (gsj_ctx_create: " + std::to_string(rc) + ")");
-      }
-      created_++;
-      if (!budget_set_) {
-        uint64_t fr = 0, tot = 0;
-        gsj_ctx_mem_info(c, &fr, &tot, nullptr);
-        const uint64_t all = g_cfg.mem_budget_gb > 0 ? (uint64_t)(g_cfg.mem_budget_gb * 1073741824.0) : fr / 2;
-        budget_ = all / 2;
-        budget_set_ = true;
       }
     }
     busy_++;
@@ -153,6 +153,17 @@ class GpuPool {
     used_ -= est;
     cv_.notify_all();
   }
+  // Every context of the pool at start-up: creating one later happens under the pool lock, in front of the
+  // request that needed it. Best effort: without a usable device the first request reports the error.
+  void prewarm() {
+    std::lock_guard<std::mutex> lk(m_);
+    while (created_ < size()) {
+      gsj_ctx* c = nullptr;
+      const int rc = create(&c);
+      if (rc) { logf("no engine context at start-up (gsj_ctx_create: %d); creating on first use", rc); return; }
+      free_.push_back(c);
+    }
+  }
   void counts(int* busy, uint64_t* queued, uint64_t* used, uint64_t* budget) {
     std::lock_guard<std::mutex> lk(m_);
     *busy += busy_;
@@ -163,6 +174,19 @@ class GpuPool {
 
  private:
   int size() const { return std::max(1, share_ == 0 ? g_cfg.workers / 2 : g_cfg.workers - g_cfg.workers / 2); }
+  int create(gsj_ctx** c) {   // caller holds m_
+    const int rc = gsj_ctx_create_prio(g_cfg.device, high_, c);
+    if (rc) return rc;
+    created_++;
+    if (!budget_set_) {
+      uint64_t fr = 0, tot = 0;
+      gsj_ctx_mem_info(*c, &fr, &tot, nullptr);
+      const uint64_t all = g_cfg.mem_budget_gb > 0 ? (uint64_t)(g_cfg.mem_budget_gb * 1073741824.0) : fr / 2;
+      budget_ = all / 2;
+      budget_set_ = true;
+    }
+    return 0;
+  }
   int high_, share_;
   std::mutex m_;
   std::condition_variable cv_;
@@ -358,27 +382,163 @@ struct Conn {
   void end_stream(const std::string& stats) { u32(0); str(stats); }
 };
 
-// Encode rows of n items in parallel into independent runs of complete frames, send them in order
-// (send_parallel, gpujoind.cu:192-206). enc(i, FrameWriter&) writes the rows of item i.
-template <class Enc> uint64_t send_rows(Conn& c, uint64_t n, Enc&& enc) {
+// Encoder threads shared by all requests (started once: connection threads are short-lived, so a per-call thread
+// team would be created afresh for every request). run(nch, f) calls f(0 .. nch-1) on the pool and the calling
+// thread and returns when all are done.
+class EncodePool {
+ public:
+  void start(int n) {
+    for (int i = 0; i < n; i++) std::thread([this] { loop(); }).detach();
+    threads_ = n;
+  }
+  template <class F> void run(uint64_t nch, F&& f) {
+    if (threads_ == 0 || nch < 2) { for (uint64_t k = 0; k < nch; k++) f(k); return; }
+    Job j;
+    j.fn = [&f](uint64_t k) { f(k); };
+    j.n = nch;
+    { std::lock_guard<std::mutex> l(m_); q_.push_back(&j); }
+    cv_.notify_all();
+    work(j);
+    std::unique_lock<std::mutex> l(m_);
+    done_cv_.wait(l, [&] { return j.finished == j.n && j.helpers == 0; });
+    drop(&j);   // under the same lock as the check: no helper can pick the job up any more
+  }
+
+ private:
+  struct Job { std::function<void(uint64_t)> fn; uint64_t n = 0, finished = 0; std::atomic<uint64_t> next{0}; int helpers = 0; };
+  void drop(Job* j) {   // caller holds m_
+    for (auto it = q_.begin(); it != q_.end(); ++it)
+      if (*it == j) { q_.erase(it); return; }
+  }
+  void work(Job& j) {
+    for (;;) {
+      const uint64_t k = j.next.fetch_add(1);
+      if (k >= j.n) return;
+      j.fn(k);
+      std::lock_guard<std::mutex> l(m_);
+      if (++j.finished == j.n) done_cv_.notify_all();
+    }
+  }
+  void loop() {
+    for (;;) {
+      Job* j = nullptr;
+      {
+        std::unique_lock<std::mutex> l(m_);
+        cv_.wait(l, [&] { return !q_.empty(); });
+        j = q_.front();
+        j->helpers++;
+      }
+      work(*j);
+      std::lock_guard<std::mutex> l(m_);
+      drop(j);   // its chunks are all taken
+      j->helpers--;
+      done_cv_.notify_all();
+    }
+  }
+  int threads_ = 0;
+  std::mutex m_;
+  std::condition_variable cv_, done_cv_;
+  std::deque<Job*> q_;
+};
+EncodePool& g_encode = *new EncodePool;   // never destroyed: its detached threads wait on it until exit
+
+// Encode rows of n items into independent runs of complete frames and send them in order (send_parallel,
+// gpujoind.cu:192-206): in parallel on the encoder threads for a whole join's rows, on the calling thread for one
+// streamed batch (the GPU runs the next batch meanwhile). enc(i, FrameWriter&) writes the rows of item i.
+// enc_s / wr_s (optional) accumulate the encoding and writing seconds.
+thread_local bool t_sequential_encode = false;
+template <class Enc> uint64_t send_rows(Conn& c, uint64_t n, Enc&& enc, double* enc_s = nullptr, double* wr_s = nullptr) {
   if (!n || c.broken) return 0;
-  const int T = std::max(1, g_cfg.threads);
-  const uint64_t nch = std::min<uint64_t>(n, (uint64_t)T * 4);
-  std::vector<FrameWriter> fw(nch);
-#pragma omp parallel for num_threads(T) schedule(dynamic, 1)
-  for (int64_t k = 0; k < (int64_t)nch; k++) {
+  const auto t0 = Clock::now();
+  const bool par = !t_sequential_encode && n >= 4096;
+  const uint64_t nch = par ? std::min<uint64_t>(n, (uint64_t)std::max(1, g_cfg.threads) * 4) : 1;
+  thread_local std::vector<FrameWriter> t_fw;   // kept with their capacity: steady-state requests touch no new pages
+  if (t_fw.size() < nch) t_fw.resize(nch);
+  FrameWriter* fw = t_fw.data();
+  auto one = [&](uint64_t k) {
     const uint64_t i0 = n * k / nch, i1 = n * (k + 1) / nch;
-    fw[k].out.reserve((i1 - i0) * 64);
+    fw[k].reset();
+    fw[k].reserve((i1 - i0) * 48);
     fw[k].begin();
     for (uint64_t i = i0; i < i1; i++) enc(i, fw[k]);
     fw[k].finish();
-  }
+  };
+  if (par) g_encode.run(nch, one);
+  else one(0);
+  const auto t1 = Clock::now();
   uint64_t rows = 0;
-  for (auto& f : fw) {
-    if (!c.write_full(f.out.data(), f.out.size())) break;
-    rows += f.rows;
+  for (uint64_t k = 0; k < nch; k++) {
+    if (!c.write_full(fw[k].data(), fw[k].size())) break;
+    rows += fw[k].rows;
   }
+  if (enc_s) *enc_s += std::chrono::duration<double>(t1 - t0).count();
+  if (wr_s) *wr_s += secs_since(t1);
   return rows;
+}
+
+// Rows of finished engine batches, sent either at once (sync: the consumer reads the engine's host buffers in
+// the sink) or by a sender thread (the sink copies the batch out, since the engine reuses its buffers, and
+// returns so that the GPU starts the next batch while this one is encoded and written). At most kMaxQueued
+// batches wait; a sink that would exceed that blocks until the sender catches up.
+class Streamer {
+ public:
+  using Fn = std::function<void(const uint32_t* p, const double* ar, const uint32_t* code, const uint8_t* wh, uint64_t n)>;
+  Streamer(bool pipelined, Fn fn) : fn_(std::move(fn)), on_(pipelined) {
+    if (on_) th_ = std::thread([this] { t_sequential_encode = true; run(); });
+  }
+  ~Streamer() { finish(); }
+  Streamer(const Streamer&) = delete;
+  Streamer& operator=(const Streamer&) = delete;
+
+  void push(const uint32_t* p, const double* ar, const uint32_t* code, const uint8_t* wh, uint64_t n) {
+    if (!on_) { fn_(p, ar, code, wh, n); return; }
+    Batch b;
+    b.n = n;
+    b.p.assign(p, p + 2 * n);
+    if (ar) b.ar.assign(ar, ar + n);
+    if (code) b.code.assign(code, code + n);
+    if (wh) b.wh.assign(wh, wh + n);
+    std::unique_lock<std::mutex> l(m_);
+    room_.wait(l, [&] { return q_.size() < kMaxQueued; });
+    q_.push_back(std::move(b));
+    ready_.notify_one();
+  }
+  void finish() {   // every pushed batch sent (or dropped by the consumer on a broken connection)
+    if (!on_ || !th_.joinable()) return;
+    { std::lock_guard<std::mutex> l(m_); done_ = true; }
+    ready_.notify_one();
+    th_.join();
+  }
+
+ private:
+  struct Batch { std::vector<uint32_t> p; std::vector<double> ar; std::vector<uint32_t> code; std::vector<uint8_t> wh; uint64_t n = 0; };
+  static constexpr size_t kMaxQueued = 4;
+  void run() {
+    for (;;) {
+      Batch b;
+      {
+        std::unique_lock<std::mutex> l(m_);
+        ready_.wait(l, [&] { return done_ || !q_.empty(); });
+        if (q_.empty()) return;
+        b = std::move(q_.front());
+        q_.pop_front();
+        room_.notify_one();
+      }
+      fn_(b.p.data(), b.ar.empty() ? nullptr : b.ar.data(), b.code.empty() ? nullptr : b.code.data(), b.wh.empty() ? nullptr : b.wh.data(), b.n);
+    }
+  }
+  Fn fn_;
+  bool on_;
+  std::thread th_;
+  std::mutex m_;
+  std::condition_variable ready_, room_;
+  std::deque<Batch> q_;
+  bool done_ = false;
+};
+
+// send_rows with the request's encode / write seconds accumulated in its run record
+template <class Run, class Enc> uint64_t send_rows_acc(Run& r, Conn& c, uint64_t n, Enc&& enc) {
+  return send_rows(c, n, std::forward<Enc>(enc), &r.enc_s, &r.wr_s);
 }
 
 constexpr double kNaN = std::numeric_limits<double>::quiet_NaN();
@@ -409,11 +569,11 @@ struct JoinRun {
   const Layer *LA, *LB; // output order
   bool same, distinct, want_area, stats_only, swapped;
   uint64_t total = 0;
-  double area_sum = 0, host_s = 0;
+  double area_sum = 0, host_s = 0, enc_s = 0, wr_s = 0;
+  Streamer* out = nullptr;
 };
 
-int join_sink(void* u, const uint32_t* p, const double* ar, const uint32_t*, uint64_t n) {
-  JoinRun& J = *static_cast<JoinRun*>(u);
+void join_rows(JoinRun& J, const uint32_t* p, const double* ar, uint64_t n) {
   const auto th = Clock::now();
   const Members MA = J.A->members(), MB = J.B->members();
   if (J.stats_only) {
@@ -426,11 +586,11 @@ int join_sink(void* u, const uint32_t* p, const double* ar, const uint32_t*, uin
       if (ar) as += ar[i] * (double)k;
     }
     J.total += t; J.area_sum += as; J.host_s += secs_since(th);
-    return 0;
+    return;
   }
   const Layer& A = *J.A;
   const Layer& B = *J.B;
-  J.total += send_rows(*J.c, n, [&](uint64_t i, FrameWriter& f) {
+  J.total += send_rows_acc(J, *J.c, n, [&](uint64_t i, FrameWriter& f) {
     const double area = ar ? ar[i] : kNaN;
     pair_rows(p[2 * i], p[2 * i + 1], MA, MB, J.same, J.distinct, [&](uint32_t ra, uint32_t rb, bool) {
       const Layer& OB = J.same ? A : B;
@@ -438,19 +598,22 @@ int join_sink(void* u, const uint32_t* p, const double* ar, const uint32_t*, uin
     });
   });
   J.host_s += secs_since(th);
+}
+int join_sink(void* u, const uint32_t* p, const double* ar, const uint32_t*, uint64_t n) {
+  JoinRun& J = *static_cast<JoinRun*>(u);
+  J.out->push(p, ar, nullptr, nullptr, n);
   return J.c->broken ? 1 : 0;
 }
 
-int join_points_sink(void* u, const uint32_t* p, const uint8_t*, uint64_t n) {
-  JoinRun& J = *static_cast<JoinRun*>(u);
+void join_points_rows(JoinRun& J, const uint32_t* p, uint64_t n) {
   const auto th = Clock::now();
   const Members MB = J.B->members();
   if (J.stats_only) {
     for (uint64_t i = 0; i < n; i++) J.total += MB.count(p[2 * i + 1]);
     J.host_s += secs_since(th);
-    return 0;
+    return;
   }
-  J.total += send_rows(*J.c, n, [&](uint64_t i, FrameWriter& f) {
+  J.total += send_rows_acc(J, *J.c, n, [&](uint64_t i, FrameWriter& f) {
     MB.each(p[2 * i + 1], [&](uint32_t rb) {
       uint32_t ra = p[2 * i];
       if (J.swapped) std::swap(ra, rb);
@@ -459,6 +622,10 @@ int join_points_sink(void* u, const uint32_t* p, const uint8_t*, uint64_t n) {
     });
   });
   J.host_s += secs_since(th);
+}
+int join_points_sink(void* u, const uint32_t* p, const uint8_t*, uint64_t n) {
+  JoinRun& J = *static_cast<JoinRun*>(u);
+  J.out->push(p, nullptr, nullptr, nullptr, n);
   return J.c->broken ? 1 : 0;
 }
 
@@ -482,21 +649,31 @@ void op_join(Conn& c, const std::vector<std::string>& a) {
   o.refine_mode = g_cfg.refine_mode;
   const auto t0 = Clock::now();
   JoinRun J{&c, A.get(), B.get(), swapped ? B.get() : A.get(), swapped ? A.get() : B.get(), same, distinct, want_area, stats_only, swapped};
+  const bool pipe = !stats_only && g_cfg.stream_batch > 0;
+  if (pipe) o.batch_q = g_cfg.stream_batch;
+  Streamer out(pipe, [&](const uint32_t* p, const double* ar, const uint32_t*, const uint8_t*, uint64_t n) {
+    if (J.A->points()) join_points_rows(J, p, n); else join_rows(J, p, ar, n);
+  });
+  J.out = &out;
   gsj_join_stats st{};
   std::string stats;
   if (A->points()) {
-    engine_status(c, ctx, gsj_join_points(ctx, A->h, B->h, &o, join_points_sink, &J, &st), "join");
+    const int rc = gsj_join_points(ctx, A->h, B->h, &o, join_points_sink, &J, &st);
+    out.finish();
+    engine_status(c, ctx, rc, "join");
     stats = Json().str("kind", "point_in_polygon").u64("candidates", st.candidates).u64("gpu_hits", st.hits).u64("rows", J.total)
-        .num("traverse_ms", st.traverse_ms).num("refine_ms", st.refine_ms).num("host_encode_send_s", J.host_s).num("total_s", secs_since(t0)).done();
+        .num("traverse_ms", st.traverse_ms).num("refine_ms", st.refine_ms).num("host_encode_send_s", J.host_s).num("host_encode_s", J.enc_s).num("host_write_s", J.wr_s).num("total_s", secs_since(t0)).done();
   } else {
     gsj_refine_params rp;
     gsj_refine_params_default(&rp);
     rp.want_area = want_area ? 1 : 0;
     o.upper = same;   // self-join: each unordered pair once, mirrored by the row rules
-    engine_status(c, ctx, gsj_join(ctx, A->h, B->h, &rp, &o, join_sink, &J, &st), "join");
+    const int rc = gsj_join(ctx, A->h, B->h, &rp, &o, join_sink, &J, &st);
+    out.finish();
+    engine_status(c, ctx, rc, "join");
     stats = Json().str("kind", "polygon_polygon").u64("candidates", st.candidates).u64("gpu_hits", st.hits).u64("rows", J.total)
         .u64("heavy", st.heavy).num("traverse_ms", st.traverse_ms).num("refine_ms", st.refine_ms).num("compact_ms", st.compact_ms)
-        .num("d2h_ms", st.copy_ms).num("host_encode_send_s", J.host_s).num("total_s", secs_since(t0)).done();
+        .num("d2h_ms", st.copy_ms).num("host_encode_send_s", J.host_s).num("host_encode_s", J.enc_s).num("host_write_s", J.wr_s).num("total_s", secs_since(t0)).done();
   }
   if (stats_only) stats = with_stats_only(stats, want_area, J.area_sum);
   if (!c.broken) c.end_stream(stats);
@@ -541,7 +718,8 @@ struct RelateRun {
   bool same, distinct, swapped;
   std::string pat;
   uint64_t total = 0;
-  double host_s = 0;
+  double host_s = 0, enc_s = 0, wr_s = 0;
+  Streamer* out = nullptr;
 };
 
 void put_relate(FrameWriter& f, const RelateRun& R, const Layer& LA, uint32_t ra, const Layer& LB, uint32_t rb, uint32_t code) {
@@ -551,27 +729,29 @@ void put_relate(FrameWriter& f, const RelateRun& R, const Layer& LA, uint32_t ra
   f.id(LA.ids.data(ra), LA.ids.len(ra)); f.id(LB.ids.data(rb), LB.ids.len(rb)); f.raw(m, 9); f.row_done();
 }
 
-int relate_sink(void* u, const uint32_t* p, const double*, const uint32_t* code, uint64_t n) {
-  RelateRun& R = *static_cast<RelateRun*>(u);
+void relate_rows(RelateRun& R, const uint32_t* p, const uint32_t* code, uint64_t n) {
   const auto th = Clock::now();
   const Members MA = R.A->members(), MB = R.B->members();
   const Layer& A = *R.A;
   const Layer& OB = R.same ? *R.A : *R.B;
-  R.total += send_rows(*R.c, n, [&](uint64_t i, FrameWriter& f) {
+  R.total += send_rows_acc(R, *R.c, n, [&](uint64_t i, FrameWriter& f) {
     const uint32_t cd = code[i], ct = gsj_de9im_transpose(cd);
     pair_rows(p[2 * i], p[2 * i + 1], MA, MB, R.same, R.distinct, [&](uint32_t ra, uint32_t rb, bool tr) {
       put_relate(f, R, A, ra, OB, rb, tr ? ct : cd);
     });
   });
   R.host_s += secs_since(th);
+}
+int relate_sink(void* u, const uint32_t* p, const double*, const uint32_t* code, uint64_t n) {
+  RelateRun& R = *static_cast<RelateRun*>(u);
+  R.out->push(p, nullptr, code, nullptr, n);
   return R.c->broken ? 1 : 0;
 }
 
-int relate_points_sink(void* u, const uint32_t* p, const uint8_t* wh, uint64_t n) {
-  RelateRun& R = *static_cast<RelateRun*>(u);
+void relate_points_rows(RelateRun& R, const uint32_t* p, const uint8_t* wh, uint64_t n) {
   const auto th = Clock::now();
   const Members MB = R.B->members();
-  R.total += send_rows(*R.c, n, [&](uint64_t i, FrameWriter& f) {
+  R.total += send_rows_acc(R, *R.c, n, [&](uint64_t i, FrameWriter& f) {
     const uint32_t code = wh[i] == 2 ? kPtBoundary : kPtInterior;   // relate(point, polygon)
     MB.each(p[2 * i + 1], [&](uint32_t rb) {
       if (R.swapped) put_relate(f, R, *R.B, rb, *R.A, p[2 * i], gsj_de9im_transpose(code));
@@ -579,6 +759,10 @@ int relate_points_sink(void* u, const uint32_t* p, const uint8_t* wh, uint64_t n
     });
   });
   R.host_s += secs_since(th);
+}
+int relate_points_sink(void* u, const uint32_t* p, const uint8_t* wh, uint64_t n) {
+  RelateRun& R = *static_cast<RelateRun*>(u);
+  R.out->push(p, nullptr, nullptr, wh, n);
   return R.c->broken ? 1 : 0;
 }
 
@@ -606,19 +790,29 @@ void op_relate(Conn& c, const std::vector<std::string>& a) {
   o.refine_mode = g_cfg.refine_mode;
   const auto t0 = Clock::now();
   RelateRun R{&c, A.get(), B.get(), same, distinct, swapped, pat};
+  const bool pipe = g_cfg.stream_batch > 0;
+  if (pipe) o.batch_q = g_cfg.stream_batch;
+  Streamer out(pipe, [&](const uint32_t* p, const double*, const uint32_t* code, const uint8_t* wh, uint64_t n) {
+    if (R.A->points()) relate_points_rows(R, p, wh, n); else relate_rows(R, p, code, n);
+  });
+  R.out = &out;
   gsj_join_stats st{};
   if (A->points()) {
-    engine_status(c, ctx, gsj_join_points(ctx, A->h, B->h, &o, relate_points_sink, &R, &st), "relate");
+    const int rc = gsj_join_points(ctx, A->h, B->h, &o, relate_points_sink, &R, &st);
+    out.finish();
+    engine_status(c, ctx, rc, "relate");
   } else {
     gsj_refine_params rp;
     gsj_refine_params_default(&rp);
     rp.want_area = 0;
     rp.want_relate = 1;
     o.upper = same;
-    engine_status(c, ctx, gsj_join(ctx, A->h, B->h, &rp, &o, relate_sink, &R, &st), "relate");
+    const int rc = gsj_join(ctx, A->h, B->h, &rp, &o, relate_sink, &R, &st);
+    out.finish();
+    engine_status(c, ctx, rc, "relate");
   }
   const std::string stats = Json().str("kind", "relate").str("pattern", pat).u64("candidates", st.candidates).u64("gpu_hits", st.hits)
-      .u64("rows", R.total).num("host_encode_send_s", R.host_s).num("total_s", secs_since(t0)).done();
+      .u64("rows", R.total).num("host_encode_send_s", R.host_s).num("host_encode_s", R.enc_s).num("host_write_s", R.wr_s).num("total_s", secs_since(t0)).done();
   if (!c.broken) c.end_stream(stats);
   logf("relate %s x %s: %s%s", a[0].c_str(), a[1].c_str(), stats.c_str(), c.broken ? " (client went away)" : "");
 }
@@ -636,18 +830,18 @@ struct PairsRun {
   const Layer *A, *B, *LA, *LB;
   bool same, distinct, stats_only, swapped;
   uint64_t total = 0;
-  double host_s = 0;
+  double host_s = 0, enc_s = 0, wr_s = 0;
+  Streamer* out = nullptr;
 };
 
-int pairs_sink(void* u, const uint32_t* p, uint64_t n) {
-  PairsRun& P = *static_cast<PairsRun*>(u);
+void pairs_rows(PairsRun& P, const uint32_t* p, uint64_t n) {
   const auto th = Clock::now();
   const Members MA = P.A->members(), MB = P.B->members();
   if (P.A->points()) {   // (point, polygon parent) pairs
     if (P.stats_only) {
       for (uint64_t i = 0; i < n; i++) P.total += MB.count(p[2 * i + 1]);
     } else {
-      P.total += send_rows(*P.c, n, [&](uint64_t i, FrameWriter& f) {
+      P.total += send_rows_acc(P, *P.c, n, [&](uint64_t i, FrameWriter& f) {
         MB.each(p[2 * i + 1], [&](uint32_t rb) {
           uint32_t ra = p[2 * i];
           if (P.swapped) std::swap(ra, rb);
@@ -663,13 +857,17 @@ int pairs_sink(void* u, const uint32_t* p, uint64_t n) {
   } else {
     const Layer& A = *P.A;
     const Layer& OB = P.same ? *P.A : *P.B;
-    P.total += send_rows(*P.c, n, [&](uint64_t i, FrameWriter& f) {
+    P.total += send_rows_acc(P, *P.c, n, [&](uint64_t i, FrameWriter& f) {
       pair_rows(p[2 * i], p[2 * i + 1], MA, MB, P.same, P.distinct, [&](uint32_t ra, uint32_t rb, bool) {
         f.id(A.ids.data(ra), A.ids.len(ra)); f.id(OB.ids.data(rb), OB.ids.len(rb)); f.f64(kNaN); f.row_done();
       });
     });
   }
   P.host_s += secs_since(th);
+}
+int pairs_sink(void* u, const uint32_t* p, uint64_t n) {
+  PairsRun& P = *static_cast<PairsRun*>(u);
+  P.out->push(p, nullptr, nullptr, nullptr, n);
   return P.c->broken ? 1 : 0;
 }
 
@@ -707,9 +905,15 @@ void op_dwithin(Conn& c, const std::vector<std::string>& a) {
   o.refine_mode = g_cfg.refine_mode;
   const auto t0 = Clock::now();
   PairsRun P{&c, A.get(), B.get(), swapped ? B.get() : A.get(), swapped ? A.get() : B.get(), same, distinct, stats_only, swapped};
+  // erosion keeps one batch: its pass-2 tiles work on the whole candidate set
+  const bool pipe = !stats_only && !erode && g_cfg.stream_batch > 0;
+  if (pipe) o.batch_q = g_cfg.stream_batch;
+  Streamer out(pipe, [&](const uint32_t* p, const double*, const uint32_t*, const uint8_t*, uint64_t n) { pairs_rows(P, p, n); });
+  P.out = &out;
   gsj_join_stats st{};
   if (A->points()) {
     const int rc = erode ? gsj_points_erode(ctx, A->h, B->h, rb, &o, pairs_sink, &P, &st) : gsj_points_dwithin(ctx, A->h, B->h, d, &o, pairs_sink, &P, &st);
+    out.finish();
     engine_status(c, ctx, rc, "dwithin");
   } else {
     o.upper = same;
@@ -719,15 +923,19 @@ void op_dwithin(Conn& c, const std::vector<std::string>& a) {
         need.assign(A->n_distinct, 0);
         if (A->deduped) for (uint64_t g = 0; g < A->n_distinct; g++) need[g] = A->moff[g + 1] - A->moff[g] > 1;
       }
-      engine_status(c, ctx, gsj_erode(ctx, A->h, B->h, ra, rb, same, need.empty() ? nullptr : need.data(), &o, pairs_sink, &P, &st), "dwithin");
+      const int rc = gsj_erode(ctx, A->h, B->h, ra, rb, same, need.empty() ? nullptr : need.data(), &o, pairs_sink, &P, &st);
+      out.finish();
+      engine_status(c, ctx, rc, "dwithin");
     } else {
-      engine_status(c, ctx, gsj_dwithin(ctx, A->h, B->h, d, same, &o, pairs_sink, &P, &st), "dwithin");
+      const int rc = gsj_dwithin(ctx, A->h, B->h, d, same, &o, pairs_sink, &P, &st);
+      out.finish();
+      engine_status(c, ctx, rc, "dwithin");
     }
   }
   const std::string stats = Json().str("kind", erode ? "buffer_intersects" : "dwithin").num("distance_m", d).num("erode_a_m", swapped ? rb : ra)
       .num("erode_b_m", swapped ? ra : rb).u64("candidates", st.candidates).u64("tested", st.candidates).u64("gpu_hits", st.hits)
       .u64("rows", P.total).u64("heavy", st.heavy).num("traverse_ms", st.traverse_ms).num("refine_ms", st.refine_ms)
-      .num("compact_ms", st.compact_ms).num("d2h_ms", st.copy_ms).num("host_encode_send_s", P.host_s).num("total_s", secs_since(t0))
+      .num("compact_ms", st.compact_ms).num("d2h_ms", st.copy_ms).num("host_encode_send_s", P.host_s).num("host_encode_s", P.enc_s).num("host_write_s", P.wr_s).num("total_s", secs_since(t0))
       .boolean("stats_only", stats_only).done();
   if (!c.broken) c.end_stream(stats);
   logf("dwithin %s x %s %s %s %s: %s%s", a[0].c_str(), a[1].c_str(), mode.c_str(), a[3].c_str(), a[4].c_str(), stats.c_str(),
@@ -874,7 +1082,7 @@ void on_signal(int) { g_stop = true; }
 
 const char* kUsage =
     "usage: gsjd [--socket PATH] [--tcp HOST:PORT] [--token-file FILE] [--data-dir DIR] [--device N] [--workers N]\n"
-    "            [--threads N] [--mem-budget-gb G] [--refine plain|filtered]\n"
+    "            [--threads N] [--mem-budget-gb G] [--refine plain|filtered] [--stream-batch N]\n"
     "            [--conninfo STR (accepted, unused: layers load from files)]\n";
 
 }  // namespace
@@ -882,6 +1090,9 @@ const char* kUsage =
 
 extern "C" int gsjd_main(int argc, char** argv) {
   using namespace gsjd;
+  // a server: load every kernel at context creation, not at its first launch in the middle of a request (unless
+  // the caller chose a loading mode)
+  setenv("CUDA_MODULE_LOADING", "EAGER", 0);
   for (int i = 1; i < argc; i++) {
     const std::string a = argv[i];
     const bool has = i + 1 < argc;
@@ -892,6 +1103,7 @@ extern "C" int gsjd_main(int argc, char** argv) {
     else if (a == "--workers" && has) g_cfg.workers = std::max(1, atoi(argv[++i]));
     else if (a == "--threads" && has) g_cfg.threads = std::max(1, atoi(argv[++i]));
     else if (a == "--mem-budget-gb" && has) g_cfg.mem_budget_gb = atof(argv[++i]);
+    else if (a == "--stream-batch" && has) g_cfg.stream_batch = (uint32_t)std::max(0, atoi(argv[++i]));
     else if (a == "--refine" && has) {
       const std::string m = argv[++i];
       if (m != "plain" && m != "filtered") { fputs("--refine plain|filtered\n", stderr); return 1; }
@@ -913,6 +1125,9 @@ extern "C" int gsjd_main(int argc, char** argv) {
   sa.sa_handler = on_signal;   // no SA_RESTART: poll() returns and the loop sees the flag
   sigaction(SIGTERM, &sa, nullptr);
   sigaction(SIGINT, &sa, nullptr);
+  g_encode.start(std::max(0, g_cfg.threads - 1));
+  g_pool_small.prewarm();   // before the socket exists: a client that can connect finds the contexts ready
+  g_pool_large.prewarm();
   std::vector<pollfd> fds;
   const int u = listen_unix(g_cfg.socket);
   if (u < 0) return 1;

@@ -2,6 +2,7 @@
 // Errors are thrown as gsj::Error inside the library and turned into status codes at the C ABI (capi.cu).
 #pragma once
 #include <cuda_runtime.h>
+#include <algorithm>
 #include <cstdint>
 #include <cstdio>
 #include <stdexcept>
@@ -47,20 +48,30 @@ struct DevBuf {
   void release() { if (p) { if (s) cudaFreeAsync(p, s); else cudaFree(p); } p = nullptr; cap = 0; }
   ~DevBuf() { release(); }
 };
+// grow-only pinned host staging. A buffer outgrown mid-request is retired, not freed: cudaFreeHost can wait for
+// the whole device, which would stall the other contexts' requests; growth doubles, so the retired ones add up to
+// less than the live one, and all are freed with the context.
 struct PinnedBuf {
   void* p = nullptr; size_t cap = 0;
+  std::vector<void*> retired;
   void* get(size_t n) {
     if (n > cap) {
-      if (p) cudaFreeHost(p);
-      p = nullptr; cap = 0;
-      size_t want = n + n / 4 + 256;
+      if (p) retired.push_back(p);
+      p = nullptr;
+      size_t want = std::max(n + n / 4 + 256, 2 * cap);
+      cap = 0;
       GSJ_CK(cudaHostAlloc(&p, want, cudaHostAllocDefault));
       cap = want;
     }
     return p;
   }
   template <class T> T* as(size_t count) { return reinterpret_cast<T*>(get(count * sizeof(T) + 16)); }
-  void release() { if (p) cudaFreeHost(p); p = nullptr; cap = 0; }
+  void release() {
+    if (p) cudaFreeHost(p);
+    for (void* q : retired) cudaFreeHost(q);
+    retired.clear();
+    p = nullptr; cap = 0;
+  }
   ~PinnedBuf() { release(); }
 };
 

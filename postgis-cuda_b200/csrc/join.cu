@@ -114,8 +114,8 @@ uint64_t candidates_for(gsj_ctx* c, const float4* qbb, const uint32_t* qorder, u
 }
 
 struct Batch { uint32_t q0, nq; };
-// Probe batches of one join: index ranges that keep a parent's pieces together, or (sharded layers without
-// parents) a contiguous run of Morton positions. morton = the batches index P's Morton order.
+// Probe batches of one join: runs of Morton positions (layers without parents: each batch a compact region), or
+// index ranges that keep a parent's pieces together. morton = the batches index P's Morton order.
 static std::vector<Batch> make_batches(const gsj_layer* P, const gsj_join_opts& o, bool& morton) {
   std::vector<Batch> b;
   const uint32_t n = P->d.n;
@@ -131,8 +131,8 @@ static std::vector<Batch> make_batches(const gsj_layer* P, const gsj_join_opts& 
     }
   }
   const uint32_t bq = o.batch_q;
-  // Morton order: the whole layer in one batch, or a shard of a layer without parents (positions of the order)
-  morton = (o.nshards <= 1 && (!bq || bq >= n)) || (o.nshards > 1 && hp.empty());
+  // Morton order: the whole layer in one batch, or any batch or shard of a layer without parents
+  morton = hp.empty() || (o.nshards <= 1 && (!bq || bq >= n));
   if (lo >= hi) return b;
   if (!bq || bq >= hi - lo) { b.push_back({lo, hi - lo}); return b; }
   for (uint32_t q0 = lo, qn; q0 < hi; q0 = qn) {
@@ -312,13 +312,12 @@ void run_points(gsj_ctx* c, const gsj_layer* pts, const gsj_layer* R, const gsj_
   }
   const uint32_t span = hi - lo;
   const uint32_t bq = (o.batch_q && o.batch_q < span) ? o.batch_q : span;
-  const bool morton = bq == span || o.nshards > 1;
   for (uint32_t q0 = lo; q0 < hi; q0 += bq) {
     if (o.cancel && *o.cancel) throw Error(GSJ_ERR_CANCELLED, "cancelled");
     const uint32_t nq = std::min(bq, hi - q0);
     tm.start();
     uint2* pairs = nullptr;
-    uint64_t np = candidates_for(c, pts->d.bb, morton ? pts->bvh.order : nullptr, q0, nq, R->bvh, 0, &pairs);
+    uint64_t np = candidates_for(c, pts->d.bb, pts->bvh.order, q0, nq, R->bvh, 0, &pairs);   // runs of Morton positions
     st.traverse_ms += tm.stop(); st.candidates += np; st.batches++;
     if (!np) continue;
     tm.start();
