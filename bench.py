@@ -327,7 +327,7 @@ def run_op(args, rank, local, ws):
             r = eng.join(LA, LB, want_area=True, want_relate=False, refine_mode=mode)
             return len(r.pairs), r.stats
         if op == "dwithin":
-            p, st = eng.points_dwithin(LP, LB, 5.0)
+            p, st = eng.points_dwithin(LP, LB, 5.0, refine_mode=mode)   # warp / thread per (point, parcel)
             return len(p), st
         if op == "erode":   # self_pairs 'all': a parcel's pair with itself is kept when its eroded form is not empty
             p, st = eng.erode(LA, LA, 1.0, 1.0, same=True, refine_mode=mode)
@@ -345,7 +345,7 @@ def run_op(args, rank, local, ws):
         e1.synchronize()
         return units, st, e0.elapsed_time(e1)
 
-    modes = [("filtered", gsj.GSJ_REFINE_FILTERED)] + ([] if op == "dwithin" else [("plain", gsj.GSJ_REFINE_PLAIN)])
+    modes = [("filtered", gsj.GSJ_REFINE_FILTERED), ("plain", gsj.GSJ_REFINE_PLAIN)]
     res = {}
     for name, mode in modes:
         for _ in range(args.warmup):

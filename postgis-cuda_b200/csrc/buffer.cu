@@ -292,6 +292,69 @@ __global__ void k_pt_dwithin(const double2* __restrict__ pts, DLayer R, const ui
   hit[i] = (h || par) ? 1 : 0;
 }
 
+// The same decision with a warp per (point, piece): lanes take consecutive edges of each ring (coalesced vertex
+// loads), each edge evaluated by exactly the code above; "within" is an any-of and the crossing parity an XOR over
+// the edges, so the ballots give the thread kernel's answer. A warp stops after the chunk in which some lane found
+// an edge within d (the answer is then 1 whatever the parity). The per-point set-up (scales, band) of 32 pairs is
+// computed one pair per lane and handed to the warp with shuffles, the same values bit for bit.
+__device__ __forceinline__ double shfl_d(double v, int k) { return __shfl_sync(0xffffffffu, v, k); }
+__global__ void __launch_bounds__(128) k_pt_dwithin_warp(const double2* __restrict__ pts, DLayer R, const uint2* __restrict__ pairs, uint64_t np,
+                                                          double d, uint8_t* hit) {
+  const int lane = threadIdx.x & 31;
+  const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  for (uint64_t i0 = (((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32; i0 < np; i0 += nw * 32) {
+    uint2 mpr = make_uint2(0, 0);
+    double mx = 0, my = 0, mkx = 0, mky = 0, mtl = 0, mdelta = 0;
+    if (i0 + lane < np) {
+      mpr = pairs[i0 + lane];
+      const double2 pt = pts[mpr.x];
+      mx = pt.x; my = pt.y;
+      m_per_deg(pt.y, mkx, mky);
+      const double gy = d / mky;
+      mtl = fabs(tan(pt.y * DEG)) + 0.01;
+      mdelta = 2.0 * gy * DEG * (mtl + 0.04) + 1e-9;
+    }
+    const int cnt = np - i0 < 32 ? (int)(np - i0) : 32;
+    for (int k = 0; k < cnt; k++) {
+      const uint32_t g = __shfl_sync(0xffffffffu, mpr.y, k);
+      const double2 pt = make_double2(shfl_d(mx, k), shfl_d(my, k));
+      const double kx = shfl_d(mkx, k), ky = shfl_d(mky, k), tl = shfl_d(mtl, k), delta = shfl_d(mdelta, k);
+      const double2 o = R.origin[g];
+      const Frame B = frame_of(R, g, o.x, o.y);
+      const double px = pt.x - o.x, py = pt.y - o.y;
+      const double ox = B.shx - 1.0;
+      bool par = false, h = false;
+      for (uint32_t r = B.r0; r < B.r1; r++) {
+        const uint64_t s0 = R.rvo[r], e = R.rvo[r + 1];
+        for (uint64_t base = s0 + 1; base < e; base += 32) {
+          const uint64_t j = base + lane;
+          if (j < e) {
+            double x0, y0, x1, y1; B.v(j - 1, x0, y0); B.v(j, x1, y1);
+            if (!R.syn(j - 1)) {
+              const double d2 = pt_seg_d2(px * kx, py * ky, x0 * kx, y0 * ky, x1 * kx, y1 * ky);
+              const double ex = (x1 - x0) * kx, ey = (y1 - y0) * ky;
+              const double band = geog_band(d, delta, ex * ex + ey * ey, 0.0, tl), dlo = d - band, dhi = d + band;
+              if (d2 <= dlo * dlo || (d2 <= dhi * dhi && geog_dist(o.x + x0, o.y + y0, o.x + x1, o.y + y1, pt.x, pt.y, pt.x, pt.y, true) <= d)) h = true;
+            }
+            if (!((y0 > py) == (y1 > py) && y0 != py && y1 != py)) {
+              const bool so = left_of(x0, y0, x1, y1, ox, py), sp = left_of(x0, y0, x1, y1, px, py);
+              if (so != sp) {
+                const bool su = orient(ox, py, px, py, x0, y0) > 0, sv = orient(ox, py, px, py, x1, y1) > 0;
+                if (su != sv) par = !par;
+              }
+            }
+          }
+          if (__any_sync(0xffffffffu, h)) break;
+        }
+        if (__any_sync(0xffffffffu, h)) break;
+      }
+      const bool within = __any_sync(0xffffffffu, h);
+      const bool inside = (__popc(__ballot_sync(0xffffffffu, par)) & 1) != 0;
+      if (lane == 0) hit[i0 + k] = (within || inside) ? 1 : 0;
+    }
+  }
+}
+
 // ---- shared driver pieces ----------------------------------------------------------------------------------------
 __global__ void k_flag_keep(const uint8_t* __restrict__ f, uint64_t n, uint8_t want, uint32_t* keep) {
   const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -1143,7 +1206,11 @@ void points_buffer_host(gsj_ctx* c, const gsj_layer* pts, const gsj_layer* R, do
     tm.start();
     uint8_t* hit = c->flag.as<uint8_t>(np);
     if (erode) { k_pt_erode<<<grid_for(np, 128), 128, 0, s>>>(pts->pts, R->d, pairs, np, d, hit); c->launches++; }
-    else { k_pt_dwithin<<<grid_for(np, 128), 128, 0, s>>>(pts->pts, R->d, pairs, np, d, hit); c->launches++; }
+    else if (o.refine_mode == GSJ_REFINE_PLAIN) { k_pt_dwithin<<<grid_for(np, 128), 128, 0, s>>>(pts->pts, R->d, pairs, np, d, hit); c->launches++; }
+    else {
+      const int G = (int)std::min<uint64_t>((np + 127) / 128, (uint64_t)c->sm_count * 16);   // a warp per 32 pairs
+      k_pt_dwithin_warp<<<G, 128, 0, s>>>(pts->pts, R->d, pairs, np, d, hit); c->launches++;
+    }
     GSJ_CK(cudaGetLastError());
     st.refine_ms += tm.stop();
     tm.start();

@@ -316,8 +316,8 @@ class Engine:
         code = (np.concatenate(chunks_c) if chunks_c else np.zeros(0, np.uint32)) if want_relate else None
         return JoinResult(pairs, area, code, st.as_dict())
 
-    def join_points(self, pts: Layer, R: Layer, batch_q=0, shard=0, nshards=1):
-        o = join_opts(batch_q=batch_q, shard=shard, nshards=nshards)
+    def join_points(self, pts: Layer, R: Layer, batch_q=0, shard=0, nshards=1, refine_mode=GSJ_REFINE_FILTERED):
+        o = join_opts(batch_q=batch_q, shard=shard, nshards=nshards, refine_mode=refine_mode)
         cp, cw = [], []
 
         def sink(user, pairs, where, n):
@@ -363,11 +363,11 @@ class Engine:
         o = join_opts(upper=same, refine_mode=refine_mode)
         return self._pairs_call(lib().gsj_erode, P.h, R.h, float(ra), float(rb), int(same), None if ns is None else ns.ctypes.data, opts=o)
 
-    def points_dwithin(self, pts: Layer, R: Layer, d: float):
-        return self._pairs_call(lib().gsj_points_dwithin, pts.h, R.h, float(d))
+    def points_dwithin(self, pts: Layer, R: Layer, d: float, refine_mode=GSJ_REFINE_FILTERED):
+        return self._pairs_call(lib().gsj_points_dwithin, pts.h, R.h, float(d), opts=join_opts(refine_mode=refine_mode))
 
-    def points_erode(self, pts: Layer, R: Layer, r: float):
-        return self._pairs_call(lib().gsj_points_erode, pts.h, R.h, float(r))
+    def points_erode(self, pts: Layer, R: Layer, r: float, refine_mode=GSJ_REFINE_FILTERED):
+        return self._pairs_call(lib().gsj_points_erode, pts.h, R.h, float(r), opts=join_opts(refine_mode=refine_mode))
 
     # ---- parity / diagnostics ----
     def candidates(self, P: Layer, R: Layer, upper=False) -> np.ndarray:

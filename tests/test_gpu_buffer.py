@@ -2,6 +2,7 @@
 import numpy as np
 import pytest
 
+import gsj
 import pyoracle as O
 from gsj import gen
 
@@ -35,11 +36,12 @@ def test_dwithin_two_layers(engine, layers, a, b, d):
     assert as_set(g) == as_set(o) and len(o) > 0
 
 
+@pytest.mark.parametrize("mode", [gsj.GSJ_REFINE_PLAIN, gsj.GSJ_REFINE_FILTERED])   # thread / warp per (point, piece)
 @pytest.mark.parametrize("d", [0.0, 5.0, 100.0])
-def test_points_dwithin(engine, layers, d):
+def test_points_dwithin(engine, layers, d, mode):
     pts = gen.points(30000, BOX, 3)
     ps = layers["parcels"][2]
     pts = np.concatenate([pts, ps.xy[::131]])   # boundary points
-    g, st = engine.points_dwithin(engine.upload_points(pts), layers["parcels"][0], d)
+    g, st = engine.points_dwithin(engine.upload_points(pts), layers["parcels"][0], d, refine_mode=mode)
     o = O.pt_dwithin(pts, layers["parcels"][1], d)
     assert as_set(g) == as_set(o) and len(o) > 0

@@ -93,13 +93,14 @@ def test_batches_give_same_rows(engine, layers):
     assert all(np.array_equal(x, y) for x, y in zip(a, b))
 
 
-def test_points_in_polygons(engine, layers):
+@pytest.mark.parametrize("mode", MODES)   # thread / warp per (point, piece)
+def test_points_in_polygons(engine, layers, mode):
     pts = gen.points(50000, (-118.3, 33.95, -118.1, 34.15), 3)
     # include vertices and edge midpoints (boundary cases) of the parcels
     ps = layers["parcels"][2]
     extra = np.concatenate([ps.xy[::97], 0.5 * (ps.xy[:-1:89] + ps.xy[1::89])])
     pts = np.concatenate([pts, extra])
-    gp, gw, st = engine.join_points(engine.upload_points(pts), layers["parcels"][0])
+    gp, gw, st = engine.join_points(engine.upload_points(pts), layers["parcels"][0], refine_mode=mode)
     op, ow, nc = O.pip(pts, layers["parcels"][1])
     gp, gw = srt(gp, gw)
     assert np.array_equal(gp, op) and np.array_equal(gw, ow)
@@ -179,10 +180,11 @@ def test_subdivided_join_bitexact(engine, pieces, mode):
 
 def test_subdivided_points_cluster_dwithin(engine, pieces):
     pts = gen.points(20000, (-118.3, 33.95, -118.2, 34.05), 8)
-    gp, gw, _ = engine.join_points(engine.upload_points(pts), pieces["a"][0])
     op, ow, _ = O.pip(pts, pieces["a"][1])
-    gp, gw = srt(gp, gw)
-    assert np.array_equal(gp, op) and np.array_equal(gw, ow)
+    for mode in MODES:
+        gp, gw, _ = engine.join_points(engine.upload_points(pts), pieces["a"][0], refine_mode=mode)
+        gp, gw = srt(gp, gw)
+        assert np.array_equal(gp, op) and np.array_equal(gw, ow)
     root, _ = engine.cluster(pieces["a"][0])
     assert np.array_equal(root, O.cluster(pieces["a"][1], pieces["a"][0].info["nparent"]))
     g, _ = engine.dwithin(pieces["a"][0], pieces["a"][0], 5.0, same=True)
@@ -245,7 +247,7 @@ def test_degenerate_inputs_bitexact(engine, mode):
     root, _ = engine.cluster(L)
     assert np.array_equal(root, O.cluster(S, ps.n))
     pts = np.concatenate([ps.xy, ps.xy[::3] + 1e-7, np.array([[shapes.X0 + 0.0005, shapes.Y0 + 0.0005]])])   # vertices, near-vertices
-    gp, gw, _ = engine.join_points(engine.upload_points(pts), L)
+    gp, gw, _ = engine.join_points(engine.upload_points(pts), L, refine_mode=mode)
     op_, ow, _ = O.pip(pts, S)
     gp, gw = srt(gp, gw)
     assert np.array_equal(gp, op_) and np.array_equal(gw, ow)
