@@ -167,8 +167,15 @@ __global__ void k_expand_points(const double2* __restrict__ pts, uint32_t n, dou
 }
 
 // ---- ST_DWithin, polygon x polygon: warp per piece pair (dw_pair, buffer.cuh:185-236) ------------------------
-// 1 / 0, or -1 when a local list exceeded cap (*need = edges required)
-__device__ int dw_pair(const DLayer& P, const DLayer& R, uint32_t a, uint32_t b, double d, EList LA, EList LB, int cap, int lane, int* need) {
+// 1 / 0, or -1 when a local list exceeded cap (*need = edges required).
+// Q (filtered mode): the edge pairs that pass the box test are found by scanning the na x nb grid 32 cells a wave
+// and are tested 32 at a time, one per lane, from a per-warp queue Q (64 entries), so that the warp runs the
+// distance tests side by side; the same pairs pass the same box test and "within" is an any-of, so the answer is
+// the one of the lane-per-A-edge sweep (Q = false, the reference's scheme).
+constexpr int DW_QCAP = 64;
+template <bool QUEUED>
+__device__ int dw_pair(const DLayer& P, const DLayer& R, uint32_t a, uint32_t b, double d, EList LA, EList LB, int cap, int lane, int* need,
+                       uint2* Q) {
   const double2 oa = P.origin[a], ob = R.origin[b], ea = P.ext[a], eb = R.ext[b];
   const double sx = ob.x - oa.x, sy = ob.y - oa.y;
   double gx, gy;
@@ -184,6 +191,54 @@ __device__ int dw_pair(const DLayer& P, const DLayer& R, uint32_t a, uint32_t b,
   const double tl = fabs(tan(phi0 * DEG)) + 0.01;
   const double delta = 2.0 * 0.5 * (ov.y1 - ov.y0) * DEG * (tl + 0.04) + 1e-9;
   bool hit = false;
+  if constexpr (QUEUED) {
+    auto within = [&](uint2 e) {
+      const int i = (int)e.x, j = (int)e.y;
+      const double ex0 = LA.x0[i], ey0 = LA.y0[i], ex1 = LA.x1[i], ey1 = LA.y1[i];
+      const double fx0 = LB.x0[j], fy0 = LB.y0[j], fx1 = LB.x1[j], fy1 = LB.y1[j];
+      if (seg_isect(ex0, ey0, ex1, ey1, fx0, fy0, fx1, fy1)) return true;
+      const double exm = (ex1 - ex0) * kx, eym = (ey1 - ey0) * ky, La2 = exm * exm + eym * eym;
+      const double d2 = seg_seg_d2(ex0 * kx, ey0 * ky, ex1 * kx, ey1 * ky, fx0 * kx, fy0 * ky, fx1 * kx, fy1 * ky);
+      const double fxm = (fx1 - fx0) * kx, fym = (fy1 - fy0) * ky;
+      const double band = geog_band(d, delta, La2, fxm * fxm + fym * fym, tl);
+      const double dlo = d - band, dhi = d + band;
+      if (d2 <= dlo * dlo) return true;
+      return d2 <= dhi * dhi &&
+             geog_dist(oa.x + ex0, oa.y + ey0, oa.x + ex1, oa.y + ey1, oa.x + fx0, oa.y + fy0, oa.x + fx1, oa.y + fy1, false) <= d;
+    };
+    if (na && nb) {
+      const unsigned lt = (1u << lane) - 1;
+      const uint64_t tot = (uint64_t)na * (uint64_t)nb;
+      const int di = 32 / nb, dj = 32 % nb;
+      int i = lane / nb, j = lane % nb, qn = 0;
+      for (uint64_t base = 0; base < tot; base += 32) {
+        bool c = false;
+        if (i < na && !(LA.fl[i] & 1u) && !(LB.fl[j] & 1u)) {
+          const double ex0 = LA.x0[i], ey0 = LA.y0[i], ex1 = LA.x1[i], ey1 = LA.y1[i];
+          const double bx0 = fmin(ex0, ex1) - gx, bx1 = fmax(ex0, ex1) + gx, by0 = fmin(ey0, ey1) - gy, by1 = fmax(ey0, ey1) + gy;
+          c = !out_cmp(LB.x0[j], LB.y0[j], LB.x1[j], LB.y1[j], bx0, by0, bx1, by1);
+        }
+        const unsigned m = __ballot_sync(0xffffffffu, c);
+        if (c) Q[qn + __popc(m & lt)] = make_uint2((unsigned)i, (unsigned)j);
+        qn += __popc(m);
+        i += di; j += dj;
+        if (j >= nb) { j -= nb; i++; }
+        if (qn >= 32) {
+          __syncwarp();
+          if (__any_sync(0xffffffffu, within(Q[lane]))) return 1;
+          const int rest = qn - 32;
+          const uint2 t = lane < rest ? Q[32 + lane] : make_uint2(0, 0);
+          __syncwarp();
+          if (lane < rest) Q[lane] = t;
+          __syncwarp();
+          qn = rest;
+        }
+      }
+      __syncwarp();
+      if (__any_sync(0xffffffffu, lane < qn && within(Q[lane]))) return 1;
+      __syncwarp();
+    }
+  } else
   for (int i = lane; i < na && !hit; i += 32) {
     if (LA.fl[i] & 1u) continue;
     const double ex0 = LA.x0[i], ey0 = LA.y0[i], ex1 = LA.x1[i], ey1 = LA.y1[i];
@@ -221,18 +276,22 @@ __device__ int dw_pair(const DLayer& P, const DLayer& R, uint32_t a, uint32_t b,
 
 constexpr int DW_CAP = 128, DW_WARPS = 4;
 constexpr size_t DW_EDGE = 4 * sizeof(double) + sizeof(uint32_t);
-constexpr size_t DW_SMEM = (size_t)DW_WARPS * 2 * DW_CAP * DW_EDGE;
+__host__ __device__ constexpr size_t dw_warp_bytes(size_t cap) { return 2 * cap * DW_EDGE + DW_QCAP * sizeof(uint2); }   // lists, queue
+constexpr size_t DW_SMEM = (size_t)DW_WARPS * dw_warp_bytes(DW_CAP);
 
+template <bool QUEUED>
 __global__ void __launch_bounds__(DW_WARPS * 32) k_dwithin(DLayer P, DLayer R, const uint2* __restrict__ pairs, uint64_t np, double d, int same,
                                                            uint8_t* flag, uint32_t* heavy, unsigned long long* nheavy) {
   extern __shared__ __align__(16) unsigned char smem[];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-  EList LA = carve(smem + (size_t)wib * 2 * DW_CAP * DW_EDGE, DW_CAP), LB = carve(smem + ((size_t)wib * 2 + 1) * DW_CAP * DW_EDGE, DW_CAP);
+  unsigned char* wbase = smem + (size_t)wib * dw_warp_bytes(DW_CAP);
+  EList LA = carve(wbase, DW_CAP), LB = carve(wbase + (size_t)DW_CAP * DW_EDGE, DW_CAP);
+  uint2* Q = reinterpret_cast<uint2*>(wbase + 2 * (size_t)DW_CAP * DW_EDGE);
   const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
   for (uint64_t p = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; p < np; p += nw) {
     const uint2 pr = pairs[p];
     if (same && P.pid(pr.x) == R.pid(pr.y)) { if (lane == 0) flag[p] = 1; continue; }   // pieces of one geometry (buffer.cuh:247-250)
-    const int r = dw_pair(P, R, pr.x, pr.y, d, LA, LB, DW_CAP, lane, nullptr);
+    const int r = dw_pair<QUEUED>(P, R, pr.x, pr.y, d, LA, LB, DW_CAP, lane, nullptr, Q);
     if (lane == 0) {
       if (r < 0) { heavy[atomicAdd(nheavy, 1ull)] = (uint32_t)p; flag[p] = 0; }
       else flag[p] = (uint8_t)r;
@@ -240,15 +299,17 @@ __global__ void __launch_bounds__(DW_WARPS * 32) k_dwithin(DLayer P, DLayer R, c
     __syncwarp();
   }
 }
+template <bool QUEUED>
 __global__ void __launch_bounds__(128) k_dwithin_scratch(DLayer P, DLayer R, const uint2* __restrict__ pairs, const uint32_t* __restrict__ heavy, uint64_t nh,
                                                         double d, uint8_t* flag, unsigned char* scratch, int cap, int* err) {
   const int lane = threadIdx.x & 31;
   const uint64_t w = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
-  unsigned char* base = scratch + w * 2 * (size_t)cap * DW_EDGE;
+  unsigned char* base = scratch + w * dw_warp_bytes((size_t)cap);
   EList LA = carve(base, cap), LB = carve(base + (size_t)cap * DW_EDGE, cap);
+  uint2* Q = reinterpret_cast<uint2*>(base + 2 * (size_t)cap * DW_EDGE);
   for (uint64_t h = w; h < nh; h += nw) {
     const uint32_t p = heavy[h];
-    const int r = dw_pair(P, R, pairs[p].x, pairs[p].y, d, LA, LB, cap, lane, nullptr);
+    const int r = dw_pair<QUEUED>(P, R, pairs[p].x, pairs[p].y, d, LA, LB, cap, lane, nullptr, Q);
     if (lane == 0) { if (r < 0) *err = 1; else flag[p] = (uint8_t)r; }
     __syncwarp();
   }
@@ -444,7 +505,12 @@ void dwithin_host(gsj_ctx* c, const gsj_layer* P, const gsj_layer* R, double d, 
     GSJ_CK(cudaGetLastError());
     qbb = e;
   }
-  if (!c->dw_attr) { GSJ_CK(cudaFuncSetAttribute(k_dwithin, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)DW_SMEM)); c->dw_attr = 1; }
+  if (!c->dw_attr) {
+    GSJ_CK(cudaFuncSetAttribute(k_dwithin<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)DW_SMEM));
+    GSJ_CK(cudaFuncSetAttribute(k_dwithin<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)DW_SMEM));
+    c->dw_attr = 1;
+  }
+  const bool queued = o.refine_mode != GSJ_REFINE_PLAIN;
   PairsOut emit{c, sink, user, &st};
   const uint32_t n = P->d.n;
   const bool whole = !o.batch_q || o.batch_q >= n;
@@ -465,7 +531,9 @@ void dwithin_host(gsj_ctx* c, const gsj_layer* P, const gsj_layer* R, double d, 
     int* err = reinterpret_cast<int*>(ctr + 1);
     GSJ_CK(cudaMemsetAsync(ctr, 0, 16, s));
     const int blocks = (int)std::min<uint64_t>((np + DW_WARPS - 1) / DW_WARPS, (uint64_t)c->sm_count * 8);
-    k_dwithin<<<blocks, DW_WARPS * 32, DW_SMEM, s>>>(P->d, R->d, pairs, np, d, same, flag, heavy, ctr); c->launches++;
+    if (queued) k_dwithin<true><<<blocks, DW_WARPS * 32, DW_SMEM, s>>>(P->d, R->d, pairs, np, d, same, flag, heavy, ctr);
+    else k_dwithin<false><<<blocks, DW_WARPS * 32, DW_SMEM, s>>>(P->d, R->d, pairs, np, d, same, flag, heavy, ctr);
+    c->launches++;
     GSJ_CK(cudaGetLastError());
     unsigned long long* h = c->h_counters.as<unsigned long long>(2);
     GSJ_CK(cudaMemcpyAsync(h, ctr, 16, cudaMemcpyDeviceToHost, s));
@@ -473,11 +541,13 @@ void dwithin_host(gsj_ctx* c, const gsj_layer* P, const gsj_layer* R, double d, 
     const uint64_t nh = h[0];
     if (nh) {
       const int cap = (int)((std::max<uint32_t>(std::max(P->max_geom_edges, R->max_geom_edges), 1u) + 7u) & ~7u);
-      const size_t per = 2 * (size_t)cap * DW_EDGE;
+      const size_t per = dw_warp_bytes((size_t)cap);
       uint64_t nwarps = std::min<uint64_t>(std::min<uint64_t>(nh, std::max<uint64_t>(1, (1ull << 30) / per)), (uint64_t)c->sm_count * 32);
       nwarps = (nwarps + 3) / 4 * 4;
       unsigned char* scr = c->scratch.as<unsigned char>(per * nwarps);
-      k_dwithin_scratch<<<(int)(nwarps / 4), 128, 0, s>>>(P->d, R->d, pairs, heavy, nh, d, flag, scr, cap, err); c->launches++;
+      if (queued) k_dwithin_scratch<true><<<(int)(nwarps / 4), 128, 0, s>>>(P->d, R->d, pairs, heavy, nh, d, flag, scr, cap, err);
+      else k_dwithin_scratch<false><<<(int)(nwarps / 4), 128, 0, s>>>(P->d, R->d, pairs, heavy, nh, d, flag, scr, cap, err);
+      c->launches++;
       GSJ_CK(cudaGetLastError());
       GSJ_CK(cudaMemcpyAsync(h, ctr, 16, cudaMemcpyDeviceToHost, s));
       GSJ_CK(cudaStreamSynchronize(s));

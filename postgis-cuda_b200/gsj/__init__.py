@@ -354,8 +354,8 @@ class Engine:
         pairs = np.concatenate(chunks).reshape(-1, 2) if chunks else np.zeros((0, 2), np.uint32)
         return pairs, st.as_dict()
 
-    def dwithin(self, P: Layer, R: Layer, d: float, same=False, upper=None):
-        o = join_opts(upper=same if upper is None else upper)
+    def dwithin(self, P: Layer, R: Layer, d: float, same=False, upper=None, refine_mode=GSJ_REFINE_FILTERED):
+        o = join_opts(upper=same if upper is None else upper, refine_mode=refine_mode)
         return self._pairs_call(lib().gsj_dwithin, P.h, R.h, float(d), int(same), opts=o)
 
     def erode(self, P: Layer, R: Layer, ra: float, rb: float, same=False, need_self=None, refine_mode=GSJ_REFINE_FILTERED):

@@ -21,17 +21,22 @@ def layers(engine):
     return {k: (engine.upload_polygons(v), O.OSet(v), v) for k, v in hs.items()}
 
 
+MODES = [gsj.GSJ_REFINE_PLAIN, gsj.GSJ_REFINE_FILTERED]   # lane per A edge / queued edge pairs
+
+
+@pytest.mark.parametrize("mode", MODES)
 @pytest.mark.parametrize("d", [0.0, 5.0, 40.0])
-def test_dwithin_self(engine, layers, d):
+def test_dwithin_self(engine, layers, d, mode):
     L, S, _ = layers["parcels"]
-    g, st = engine.dwithin(L, L, d, same=True)
+    g, st = engine.dwithin(L, L, d, same=True, refine_mode=mode)
     o, nc = O.dwithin(S, S, d, same=True)
     assert as_set(g) == as_set(o) and st["candidates"] == nc
 
 
+@pytest.mark.parametrize("mode", MODES)
 @pytest.mark.parametrize("a,b,d", [("parcels", "parcels2", 5.0), ("parcels2", "zones", 1000.0), ("zones", "parcels", 25.0)])
-def test_dwithin_two_layers(engine, layers, a, b, d):
-    g, st = engine.dwithin(layers[a][0], layers[b][0], d)
+def test_dwithin_two_layers(engine, layers, a, b, d, mode):
+    g, st = engine.dwithin(layers[a][0], layers[b][0], d, refine_mode=mode)
     o, nc = O.dwithin(layers[a][1], layers[b][1], d)
     assert as_set(g) == as_set(o) and len(o) > 0
 
