@@ -1230,6 +1230,97 @@ __global__ void k_pt_erode(const double2* __restrict__ pts, DLayer R, const uint
   }
   bits[i] = ex ? 2 : (par ? 1 : 0);
 }
+// The same decision with a warp per (point, piece): lanes take consecutive edges of each ring. The exclusion test
+// of an edge reads the direction of the last earlier real edge of the ring with non-zero length (cut edges clear
+// it, zero-length edges leave it, the ring starts from its closing edge's): a lane finds the nearest earlier lane
+// whose edge is a cut or a real one with a ballot, takes that lane's state by shuffle, or the state carried from the
+// previous chunk, so every edge sees the state the sequential walk gives it. "Excluded" is an any-of (it decides 2
+// whatever the parity), the crossing parity an XOR. The set-up of 32 pairs is computed one pair per lane.
+__global__ void __launch_bounds__(128) k_pt_erode_warp(const double2* __restrict__ pts, DLayer R, const uint2* __restrict__ pairs, uint64_t np,
+                                                        double r_nom, uint8_t* bits) {
+  const int lane = threadIdx.x & 31;
+  const unsigned lt = (1u << lane) - 1;
+  const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  for (uint64_t i0 = (((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32; i0 < np; i0 += nw * 32) {
+    uint32_t mg = 0;
+    double mx = 0, my = 0, mr = 0, mkx = 0, mky = 0;
+    if (i0 + lane < np) {
+      const uint2 pr = pairs[i0 + lane];
+      const double2 pt = pts[pr.x], o = R.origin[pr.y], ext = R.ext[pr.y];
+      mg = pr.y; mx = pt.x; my = pt.y;
+      mr = r_nom / utm_k(o.x + 0.5 * ext.x, o.y + 0.5 * ext.y, pt.x, pt.y);
+      m_per_deg(pt.y, mkx, mky);
+    }
+    const int cnt = np - i0 < 32 ? (int)(np - i0) : 32;
+    for (int k = 0; k < cnt; k++) {
+      const uint32_t g = __shfl_sync(0xffffffffu, mg, k);
+      const double ptx = __shfl_sync(0xffffffffu, mx, k), pty = __shfl_sync(0xffffffffu, my, k);
+      const double r = __shfl_sync(0xffffffffu, mr, k), kx = __shfl_sync(0xffffffffu, mkx, k), ky = __shfl_sync(0xffffffffu, mky, k);
+      const double2 o = R.origin[g];
+      const double eps = 1e-9;
+      const double shx = o.x - ptx, shy = o.y - pty, ox = shx * kx - 1.0;   // frame: meters relative to the point
+      auto vx = [&](uint64_t j, double& x, double& y) { const double2 q = R.xy[j]; x = (shx + q.x) * kx; y = (shy + q.y) * ky; };
+      bool par = false, ex = false;
+      for (uint32_t rr = R.gro[g]; rr < R.gro[g + 1]; rr++) {
+        const uint64_t s0 = R.rvo[rr], e = R.rvo[rr + 1];
+        if (e - s0 < 2) continue;
+        bool cpv = false; double cux = 0, cuy = 0;   // state carried into the chunk: the ring's closing edge first
+        {
+          const uint64_t j = e - 2;
+          if (!R.syn(j)) {
+            double a, b, c2, dd; vx(j, a, b); vx(j + 1, c2, dd);
+            const double L = hypot(c2 - a, dd - b);
+            if (L > 0) { cpv = true; cux = (c2 - a) / L; cuy = (dd - b) / L; }
+          }
+        }
+        for (uint64_t base = s0; base + 1 < e; base += 32) {
+          const uint64_t j = base + lane;
+          const bool valid = j + 1 < e;
+          double x0 = 0, y0 = 0, x1 = 0, y1 = 0, L = 0, ux = 0, uy = 0;
+          bool syn = false;
+          if (valid) {
+            vx(j, x0, y0); vx(j + 1, x1, y1);
+            if (!((y0 > 0) == (y1 > 0) && y0 != 0 && y1 != 0)) {
+              const bool so = left_of(x0, y0, x1, y1, ox, 0.0), sp = left_of(x0, y0, x1, y1, 0.0, 0.0);
+              if (so != sp) {
+                const bool su = orient(ox, 0.0, 0.0, 0.0, x0, y0) > 0, sv = orient(ox, 0.0, 0.0, 0.0, x1, y1) > 0;
+                if (su != sv) par = !par;
+              }
+            }
+            L = hypot(x1 - x0, y1 - y0);
+            syn = R.syn(j);
+            if (!syn && L != 0) { ux = (x1 - x0) / L; uy = (y1 - y0) / L; }
+          }
+          const bool real = valid && !syn && L != 0, marker = valid && (syn || L != 0);
+          const unsigned mk = __ballot_sync(0xffffffffu, marker);
+          // the state before this lane's edge: the nearest earlier marker lane, else the carried state
+          const unsigned before = mk & lt;
+          const int src = before ? 31 - __clz(before) : lane;
+          const bool spv = __shfl_sync(0xffffffffu, (int)real, src) != 0;
+          const double sux = __shfl_sync(0xffffffffu, ux, src), suy = __shfl_sync(0xffffffffu, uy, src);
+          const bool pv = before ? spv : cpv;
+          const double pux = before ? sux : cux, puy = before ? suy : cuy;
+          if (real && r > 0) {
+            const double t = -x0 * ux - y0 * uy, sd = -y0 * ux + x0 * uy;
+            if (fabs(sd) < r - eps && t > -eps && t < L + eps) ex = true;
+            else if (pv && vertex_excl(pux, puy, ux, uy, r, -x0, -y0, eps)) ex = true;
+          }
+          if (mk) {   // carry the last marker's state into the next chunk
+            const int last = 31 - __clz(mk);
+            cpv = __shfl_sync(0xffffffffu, (int)real, last) != 0;
+            cux = __shfl_sync(0xffffffffu, ux, last);
+            cuy = __shfl_sync(0xffffffffu, uy, last);
+          }
+          if (__any_sync(0xffffffffu, ex)) break;
+        }
+        if (__any_sync(0xffffffffu, ex)) break;
+      }
+      const bool excl = __any_sync(0xffffffffu, ex);
+      const bool inside = (__popc(__ballot_sync(0xffffffffu, par)) & 1) != 0;
+      if (lane == 0) bits[i0 + k] = excl ? 2 : (inside ? 1 : 0);
+    }
+  }
+}
 // (point, parent) keys of every candidate with its bits
 __global__ void k_pt_keys(const uint2* __restrict__ pairs, uint64_t n, const uint32_t* parR, unsigned long long* keys) {
   const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -1275,7 +1366,11 @@ void points_buffer_host(gsj_ctx* c, const gsj_layer* pts, const gsj_layer* R, do
     if (!np) continue;
     tm.start();
     uint8_t* hit = c->flag.as<uint8_t>(np);
-    if (erode) { k_pt_erode<<<grid_for(np, 128), 128, 0, s>>>(pts->pts, R->d, pairs, np, d, hit); c->launches++; }
+    if (erode && o.refine_mode == GSJ_REFINE_PLAIN) { k_pt_erode<<<grid_for(np, 128), 128, 0, s>>>(pts->pts, R->d, pairs, np, d, hit); c->launches++; }
+    else if (erode) {
+      const int G = (int)std::min<uint64_t>((np + 127) / 128, (uint64_t)c->sm_count * 16);   // a warp per 32 pairs
+      k_pt_erode_warp<<<G, 128, 0, s>>>(pts->pts, R->d, pairs, np, d, hit); c->launches++;
+    }
     else if (o.refine_mode == GSJ_REFINE_PLAIN) { k_pt_dwithin<<<grid_for(np, 128), 128, 0, s>>>(pts->pts, R->d, pairs, np, d, hit); c->launches++; }
     else {
       const int G = (int)std::min<uint64_t>((np + 127) / 128, (uint64_t)c->sm_count * 16);   // a warp per 32 pairs

@@ -72,13 +72,14 @@ def test_erode_overflow_passes(engine):
             assert st["heavy"] > 0 and len(o) == 3
 
 
+@pytest.mark.parametrize("mode", [gsj.GSJ_REFINE_PLAIN, gsj.GSJ_REFINE_FILTERED])   # thread / warp per (point, piece)
 @pytest.mark.parametrize("r", [0.0, 1.0, 3.0, 25.0])
-def test_points_erode(engine, layers, r):
+def test_points_erode(engine, layers, r, mode):
     pts = gen.points(30000, BOX, 3)
     pts = np.concatenate([pts, layers["parcels"][2].xy[::131]])   # boundary points
     P = engine.upload_points(pts)
     for k in ("parcels", "sub"):
-        g, st = engine.points_erode(P, layers[k][0], r)
+        g, st = engine.points_erode(P, layers[k][0], r, refine_mode=mode)
         o = O.pt_erode(pts, layers[k][1], r)
         assert as_set(g) == as_set(o) and len(o) > 0
 
@@ -100,6 +101,7 @@ def test_erode_reference_golden(engine):
     g = engine.erode(P, P, 1.0, 1.0, same=True, need_self=none)[0]
     assert as_set(g) == golden("pp_erode1")
     pts = engine.upload_points(L["points"])
-    assert as_set(engine.points_erode(pts, P, 1.0)[0]) == golden("pts_erode1")
-    assert as_set(engine.points_erode(pts, SP, 3.0)[0]) == golden("pts_erode3_sub32")
-    assert as_set(engine.dwithin(P, Q, 5.0)[0]) == golden("pq_dwithin5")
+    for mode in (gsj.GSJ_REFINE_PLAIN, gsj.GSJ_REFINE_FILTERED):
+        assert as_set(engine.points_erode(pts, P, 1.0, refine_mode=mode)[0]) == golden("pts_erode1")
+        assert as_set(engine.points_erode(pts, SP, 3.0, refine_mode=mode)[0]) == golden("pts_erode3_sub32")
+        assert as_set(engine.dwithin(P, Q, 5.0, refine_mode=mode)[0]) == golden("pq_dwithin5")
