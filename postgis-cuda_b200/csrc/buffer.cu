@@ -128,7 +128,7 @@ __device__ double arc_pt(double slon, double slat, double elon, double elat, dou
   return best;
 }
 // geography distance (meters) of edge a from edge b (or from point b0 when b_is_point); degrees in
-__device__ __noinline__ double geog_dist(double a0x, double a0y, double a1x, double a1y, double b0x, double b0y, double b1x, double b1y, bool b_is_point) {
+__device__ __forceinline__ double geog_dist_inl(double a0x, double a0y, double a1x, double a1y, double b0x, double b0y, double b1x, double b1y, bool b_is_point) {
   const double R = DEG;
   double p1x, p1y, p2x, p2y, cx = 0, cy = 0;
   double best = arc_pt(a0x * R, a0y * R, a1x * R, a1y * R, b0x * R, b0y * R, cx, cy);
@@ -142,6 +142,11 @@ __device__ __noinline__ double geog_dist(double a0x, double a0y, double a1x, dou
     if (d < best) { best = d; p1x = a1x * R; p1y = a1y * R; p2x = cx; p2y = cy; }
   }
   return vincenty_m(p1x / R, p1y / R, p2x / R, p2y / R);
+}
+// Out of line for the kernels that call it rarely; kernels bounded to fewer registers inline geog_dist_inl instead
+// (a call would need the callee's 254 registers), and spill in this rare near-threshold path only.
+__device__ __noinline__ double geog_dist(double a0x, double a0y, double a1x, double a1y, double b0x, double b0y, double b1x, double b1y, bool b_is_point) {
+  return geog_dist_inl(a0x, a0y, a1x, a1y, b0x, b0y, b1x, b1y, b_is_point);
 }
 // half-width of the band around d where the straight-edge frame distance may disagree with geography
 __device__ __forceinline__ double geog_band(double d, double rel_frame, double La2, double Lb2, double tl) {
@@ -204,7 +209,7 @@ __device__ int dw_pair(const DLayer& P, const DLayer& R, uint32_t a, uint32_t b,
       const double dlo = d - band, dhi = d + band;
       if (d2 <= dlo * dlo) return true;
       return d2 <= dhi * dhi &&
-             geog_dist(oa.x + ex0, oa.y + ey0, oa.x + ex1, oa.y + ey1, oa.x + fx0, oa.y + fy0, oa.x + fx1, oa.y + fy1, false) <= d;
+             geog_dist_inl(oa.x + ex0, oa.y + ey0, oa.x + ex1, oa.y + ey1, oa.x + fx0, oa.y + fy0, oa.x + fx1, oa.y + fy1, false) <= d;
     };
     if (na && nb) {
       const unsigned lt = (1u << lane) - 1;
@@ -253,7 +258,7 @@ __device__ int dw_pair(const DLayer& P, const DLayer& R, uint32_t a, uint32_t b,
       const double band = geog_band(d, delta, La2, fxm * fxm + fym * fym, tl);
       const double dlo = d - band, dhi = d + band;
       if (d2 <= dlo * dlo) { hit = true; break; }
-      if (d2 <= dhi * dhi && geog_dist(oa.x + ex0, oa.y + ey0, oa.x + ex1, oa.y + ey1, oa.x + fx0, oa.y + fy0, oa.x + fx1, oa.y + fy1, false) <= d) {
+      if (d2 <= dhi * dhi && geog_dist_inl(oa.x + ex0, oa.y + ey0, oa.x + ex1, oa.y + ey1, oa.x + fx0, oa.y + fy0, oa.x + fx1, oa.y + fy1, false) <= d) {
         hit = true; break;
       }
     }
@@ -280,7 +285,7 @@ __host__ __device__ constexpr size_t dw_warp_bytes(size_t cap) { return 2 * cap 
 constexpr size_t DW_SMEM = (size_t)DW_WARPS * dw_warp_bytes(DW_CAP);
 
 template <bool QUEUED>
-__global__ void __launch_bounds__(DW_WARPS * 32) k_dwithin(DLayer P, DLayer R, const uint2* __restrict__ pairs, uint64_t np, double d, int same,
+__global__ void __launch_bounds__(DW_WARPS * 32, 4) k_dwithin(DLayer P, DLayer R, const uint2* __restrict__ pairs, uint64_t np, double d, int same,
                                                            uint8_t* flag, uint32_t* heavy, unsigned long long* nheavy) {
   extern __shared__ __align__(16) unsigned char smem[];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
@@ -359,7 +364,7 @@ __global__ void k_pt_dwithin(const double2* __restrict__ pts, DLayer R, const ui
 // an edge within d (the answer is then 1 whatever the parity). The per-point set-up (scales, band) of 32 pairs is
 // computed one pair per lane and handed to the warp with shuffles, the same values bit for bit.
 __device__ __forceinline__ double shfl_d(double v, int k) { return __shfl_sync(0xffffffffu, v, k); }
-__global__ void __launch_bounds__(128) k_pt_dwithin_warp(const double2* __restrict__ pts, DLayer R, const uint2* __restrict__ pairs, uint64_t np,
+__global__ void __launch_bounds__(128, 4) k_pt_dwithin_warp(const double2* __restrict__ pts, DLayer R, const uint2* __restrict__ pairs, uint64_t np,
                                                           double d, uint8_t* hit) {
   const int lane = threadIdx.x & 31;
   const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
@@ -395,7 +400,7 @@ __global__ void __launch_bounds__(128) k_pt_dwithin_warp(const double2* __restri
               const double d2 = pt_seg_d2(px * kx, py * ky, x0 * kx, y0 * ky, x1 * kx, y1 * ky);
               const double ex = (x1 - x0) * kx, ey = (y1 - y0) * ky;
               const double band = geog_band(d, delta, ex * ex + ey * ey, 0.0, tl), dlo = d - band, dhi = d + band;
-              if (d2 <= dlo * dlo || (d2 <= dhi * dhi && geog_dist(o.x + x0, o.y + y0, o.x + x1, o.y + y1, pt.x, pt.y, pt.x, pt.y, true) <= d)) h = true;
+              if (d2 <= dlo * dlo || (d2 <= dhi * dhi && geog_dist_inl(o.x + x0, o.y + y0, o.x + x1, o.y + y1, pt.x, pt.y, pt.x, pt.y, true) <= d)) h = true;
             }
             if (!((y0 > py) == (y1 > py) && y0 != py && y1 != py)) {
               const bool so = left_of(x0, y0, x1, y1, ox, py), sp = left_of(x0, y0, x1, y1, px, py);
