@@ -345,7 +345,7 @@ def run_op(args, rank, local, ws):
         e1.synchronize()
         return units, st, e0.elapsed_time(e1)
 
-    modes = [("filtered", gsj.GSJ_REFINE_FILTERED), ("plain", gsj.GSJ_REFINE_PLAIN)]
+    modes = [(n, m) for n, m in (("filtered", gsj.GSJ_REFINE_FILTERED), ("plain", gsj.GSJ_REFINE_PLAIN)) if n in args.arms.split(",")]
     res = {}
     for name, mode in modes:
         for _ in range(args.warmup):
@@ -480,6 +480,7 @@ def main():
     ap.add_argument("--cpu-sample-s", type=float, default=0.0, help="CPU seconds per reference-arm step (0: sized from --steps)")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving-latency leg (gsjd under a Poisson request stream)")
     ap.add_argument("--op", default="relate", choices=["relate", "area", "dwithin", "erode", "cluster"])
+    ap.add_argument("--arms", default="filtered,plain", help="refinement variants an --op run times (filtered first; for profiling one)")
     ap.add_argument("--shard", action="store_true",
                     help="N > 1: every rank joins the same layer, each its shard of the probes (strong scaling) instead of its own layer")
     args = ap.parse_args()
