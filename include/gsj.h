@@ -183,6 +183,38 @@ int gsj_refine_pairs(gsj_ctx* ctx, const gsj_layer* P, const gsj_layer* R, const
 int gsj_refine_pairs_noalloc(gsj_ctx* ctx, const gsj_layer* P, const gsj_layer* R, const uint32_t* d_pairs, uint64_t np,
                              const gsj_refine_params* rp, uint8_t* d_flag, double* d_area, double* d_ev, uint32_t* d_evb);
 
+/* Row encoding on the device (replaces the daemon's host encoder, send_parallel / FrameBuf, gpujoind.cu:178-206).
+ * A rowset is a device copy of a layer's row ids (id_blob bytes, id_off[n_rows + 1] offsets) and, for a deduplicated
+ * layer, its members (moff[n_geoms + 1], midx: the rows each distinct geometry stands for; NULL: geometry = row).
+ * gsj_encode_rows turns n engine results (host arrays as the sinks receive them) into the gpujoind byte stream of
+ * frames {u32 nrows, rows}, rows as gpujoind writes them (u16 length + id, u16 length + id, then the payload), and
+ * calls sink(user, bytes, nbytes, nrows) once with complete frames (not with an empty stream). Modes:
+ *   GSJ_ENC_PAIRS   polygon pairs (a, b) of P x Q expanded by the row rules (members x members; same: "all"
+ *                   mirrors, "distinct" keeps one of each; gpujoind.cu:271-283), payload f64 area[i] or NaN (area NULL)
+ *   GSJ_ENC_RELATE  the same rows, payload the 9-char DE-9IM of code[i] (transposed for mirrored rows), kept when it
+ *                   matches pattern (empty: all) (gpujoind.cu:356-367)
+ *   GSJ_ENC_POINTS  (point p, polygon q) pairs: one row per member of q, payload f64 point_value; swapped: the
+ *                   polygon's id first (gpujoind.cu:244-252, 460-468)
+ *   GSJ_ENC_POINT_RELATE  the same rows, payload relate(point, polygon) from where[i] (2: boundary, else interior),
+ *                   transposed when swapped, kept when it matches pattern
+ * P holds the ids of the pairs' first members, Q of the second (for same, pass the same rowset twice).
+ * Frames hold whole pairs' rows, ~1 MiB each for ids up to ~16 bytes; frame boundaries are not the host
+ * encoder's, the rows are the same. Runs on the context's stream; returns after the sink returned. */
+typedef struct gsj_rowset gsj_rowset;
+enum { GSJ_ENC_PAIRS = 0, GSJ_ENC_RELATE = 1, GSJ_ENC_POINTS = 2, GSJ_ENC_POINT_RELATE = 3 };
+typedef struct {
+  int mode, same, distinct, swapped;
+  double point_value;
+  char pattern[10];   /* 9 chars + NUL, or "" */
+} gsj_encode_spec;
+typedef int (*gsj_bytes_sink)(void* user, const uint8_t* bytes, uint64_t nbytes, uint64_t nrows);
+int gsj_rowset_upload(gsj_ctx* ctx, uint64_t n_geoms, const uint64_t* moff, const uint32_t* midx, uint64_t n_rows, const char* id_blob,
+                      const uint64_t* id_off, gsj_rowset** out);
+void gsj_rowset_free(gsj_rowset* rs);
+int gsj_encode_rows(gsj_ctx* ctx, const gsj_rowset* P, const gsj_rowset* Q, const gsj_encode_spec* spec, const uint32_t* pairs,
+                    const double* area, const uint32_t* code, const uint8_t* where, uint64_t n, gsj_bytes_sink sink, void* user,
+                    uint64_t* rows_out);
+
 /* DE-9IM helpers: de9im_str / de9im_transpose / de9im_match (engine.cuh:871-888). out gets 9 chars (no NUL). */
 void gsj_de9im_str(uint32_t code, char* out9);
 uint32_t gsj_de9im_transpose(uint32_t code);

@@ -236,6 +236,23 @@ int gsj_refine_pairs(gsj_ctx* c, const gsj_layer* P, const gsj_layer* R, const u
   return guard(c, [&] { gsj::refine_pairs_host(c, P, R, pairs, np, rp, mode, flag, area, ev, evb); });
 }
 
+int gsj_rowset_upload(gsj_ctx* c, uint64_t n_geoms, const uint64_t* moff, const uint32_t* midx, uint64_t n_rows, const char* id_blob,
+                      const uint64_t* id_off, gsj_rowset** out) {
+  if (!c || !out || !id_off || (moff && !midx) || (id_off[n_rows] && !id_blob)) return GSJ_ERR_ARG;
+  *out = nullptr;
+  return guard(c, [&] { *out = gsj::rowset_upload(c, n_geoms, moff, midx, n_rows, id_blob, id_off); });
+}
+void gsj_rowset_free(gsj_rowset* rs) { gsj::rowset_free(rs); }
+int gsj_encode_rows(gsj_ctx* c, const gsj_rowset* P, const gsj_rowset* Q, const gsj_encode_spec* spec, const uint32_t* pairs, const double* area,
+                    const uint32_t* code, const uint8_t* where, uint64_t n, gsj_bytes_sink sink, void* user, uint64_t* rows_out) {
+  if (!c || !P || !Q || !spec || (n && !pairs)) return GSJ_ERR_ARG;
+  if (rows_out) *rows_out = 0;
+  return guard(c, [&] {
+    const uint64_t r = gsj::encode_rows(c, P, Q, spec, pairs, area, code, where, n, sink, user);
+    if (rows_out) *rows_out = r;
+  });
+}
+
 void gsj_de9im_str(uint32_t code, char* out) {
   for (int k = 0; k < 9; k++) out[k] = "F012"[(code >> (2 * k)) & 3];
 }

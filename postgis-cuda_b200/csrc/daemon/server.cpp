@@ -66,6 +66,7 @@ struct Config {
   int refine_mode = GSJ_REFINE_FILTERED;
   double mem_budget_gb = 0;   // scratch budget shared by running requests (0: half of the free memory at first use)
   uint32_t stream_batch = 0;   // probe geometries per engine batch when rows are streamed (0: one batch)
+  int gpu_encode = 1;           // rows encoded on the device (gsj_encode_rows) when they are sent from the engine's thread
 };
 Config g_cfg;
 std::atomic<bool> g_stop{false};
@@ -227,11 +228,15 @@ struct Layer {
   std::vector<uint64_t> moff;
   std::vector<uint32_t> midx;
   gsj_layer* h = nullptr;
+  gsj_rowset* rs = nullptr;   // row ids (and members) on the device, for encoding rows there
   double copy_s = 0, prep_s = 0, upload_s = 0;
 
   Members members() const { return deduped ? Members{moff.data(), midx.data()} : Members{}; }
   bool points() const { return kind == "point"; }
-  ~Layer() { if (h) gsj_layer_free(nullptr, h); }
+  ~Layer() {
+    if (rs) gsj_rowset_free(rs);
+    if (h) gsj_layer_free(nullptr, h);
+  }
   std::string json() const {   // Layer::json, gpujoind.cu:81-86
     return Json().str("layer", name).str("kind", kind).str("source", source).u64("rows", rows).u64("skipped", skipped)
         .u64("distinct", n_distinct).u64("gpu_geoms", gpu_geoms).u64("vertices", verts).u64("subdivide", (uint64_t)subdiv)
@@ -336,6 +341,11 @@ std::string build_layer(const std::string& name, const std::string& path, int su
     check(lease.get(), gsj_layer_upload_polygons(lease.get(), bn, bnr, bnv, gro, rvo, xy, subdiv > 0 ? spar.p : nullptr,
                                                  subdiv > 0 ? ssyn.p : nullptr, &L->h), "upload");
     L->upload_s = secs_since(t1);
+  }
+  {
+    Lease lease;
+    check(lease.get(), gsj_rowset_upload(lease.get(), L->n_distinct, L->deduped ? L->moff.data() : nullptr, L->deduped ? L->midx.data() : nullptr,
+                                         L->rows, L->ids.buf.data(), L->ids.off.data(), &L->rs), "row ids upload");
   }
   gsj_layer_info info;
   gsj_layer_get_info(L->h, &info);
@@ -542,6 +552,35 @@ template <class Run, class Enc> uint64_t send_rows_acc(Run& r, Conn& c, uint64_t
 }
 
 constexpr double kNaN = std::numeric_limits<double>::quiet_NaN();
+
+// Rows encoded on the device (gsj_encode_rows: the same rows, whole frames) on the request's context, written as
+// they come back. Used when the engine's sink runs on the request's thread (not with streamed batches, whose
+// sender thread cannot share the context).
+struct GpuWrite { Conn* c; double* wr_s; };
+int gpu_frames_sink(void* u, const uint8_t* bytes, uint64_t nb, uint64_t) {
+  auto* g = static_cast<GpuWrite*>(u);
+  const auto t = Clock::now();
+  const bool ok = g->c->write_full(bytes, nb);
+  *g->wr_s += secs_since(t);
+  return ok ? 0 : 1;
+}
+uint64_t gpu_rows(gsj_ctx* ctx, Conn& c, const Layer& P, const Layer& Q, int mode, bool same, bool distinct, bool swapped, double value,
+                  const std::string& pattern, const uint32_t* p, const double* ar, const uint32_t* code, const uint8_t* wh, uint64_t n,
+                  double* enc_s, double* wr_s) {
+  if (!n || c.broken) return 0;
+  gsj_encode_spec sp;
+  sp.mode = mode; sp.same = same; sp.distinct = distinct; sp.swapped = swapped; sp.point_value = value;
+  std::memset(sp.pattern, 0, sizeof sp.pattern);
+  std::memcpy(sp.pattern, pattern.data(), std::min<size_t>(pattern.size(), 9));
+  GpuWrite g{&c, wr_s};
+  const double w0 = *wr_s;
+  const auto t0 = Clock::now();
+  uint64_t rows = 0;
+  const int rc = gsj_encode_rows(ctx, P.rs, Q.rs, &sp, p, ar, code, wh, n, gpu_frames_sink, &g, &rows);
+  *enc_s += secs_since(t0) - (*wr_s - w0);
+  if (rc && rc != GSJ_ERR_SINK) throw std::runtime_error(std::string("row encoding: ") + gsj_last_error(ctx));
+  return rows;
+}
 // relate(point, polygon) for a point inside / on the boundary (DE9IM_PT_INTERIOR / _BOUNDARY, engine.cuh:337-338)
 constexpr uint32_t kPtInterior = 1u | (3u << 12) | (2u << 14) | (3u << 16);   // 0FFFFF212
 constexpr uint32_t kPtBoundary = (1u << 2) | (3u << 12) | (2u << 14) | (3u << 16);   // F0FFFF212
@@ -571,6 +610,7 @@ struct JoinRun {
   uint64_t total = 0;
   double area_sum = 0, host_s = 0, enc_s = 0, wr_s = 0;
   Streamer* out = nullptr;
+  gsj_ctx* gctx = nullptr;   // set: rows encoded on the device
 };
 
 void join_rows(JoinRun& J, const uint32_t* p, const double* ar, uint64_t n) {
@@ -590,6 +630,12 @@ void join_rows(JoinRun& J, const uint32_t* p, const double* ar, uint64_t n) {
   }
   const Layer& A = *J.A;
   const Layer& B = *J.B;
+  if (J.gctx) {
+    J.total += gpu_rows(J.gctx, *J.c, A, J.same ? A : B, GSJ_ENC_PAIRS, J.same, J.distinct, false, 0.0, "", p, ar, nullptr, nullptr, n,
+                        &J.enc_s, &J.wr_s);
+    J.host_s += secs_since(th);
+    return;
+  }
   J.total += send_rows_acc(J, *J.c, n, [&](uint64_t i, FrameWriter& f) {
     const double area = ar ? ar[i] : kNaN;
     pair_rows(p[2 * i], p[2 * i + 1], MA, MB, J.same, J.distinct, [&](uint32_t ra, uint32_t rb, bool) {
@@ -610,6 +656,12 @@ void join_points_rows(JoinRun& J, const uint32_t* p, uint64_t n) {
   const Members MB = J.B->members();
   if (J.stats_only) {
     for (uint64_t i = 0; i < n; i++) J.total += MB.count(p[2 * i + 1]);
+    J.host_s += secs_since(th);
+    return;
+  }
+  if (J.gctx) {   // engine order: A points, B polygons
+    J.total += gpu_rows(J.gctx, *J.c, *J.A, *J.B, GSJ_ENC_POINTS, false, false, J.swapped, J.want_area ? 0.0 : kNaN, "", p, nullptr, nullptr,
+                        nullptr, n, &J.enc_s, &J.wr_s);
     J.host_s += secs_since(th);
     return;
   }
@@ -655,6 +707,7 @@ void op_join(Conn& c, const std::vector<std::string>& a) {
     if (J.A->points()) join_points_rows(J, p, n); else join_rows(J, p, ar, n);
   });
   J.out = &out;
+  if (!pipe && g_cfg.gpu_encode && A->rs && B->rs) J.gctx = ctx;
   gsj_join_stats st{};
   std::string stats;
   if (A->points()) {
@@ -720,6 +773,7 @@ struct RelateRun {
   uint64_t total = 0;
   double host_s = 0, enc_s = 0, wr_s = 0;
   Streamer* out = nullptr;
+  gsj_ctx* gctx = nullptr;   // set: rows encoded on the device
 };
 
 void put_relate(FrameWriter& f, const RelateRun& R, const Layer& LA, uint32_t ra, const Layer& LB, uint32_t rb, uint32_t code) {
@@ -734,6 +788,12 @@ void relate_rows(RelateRun& R, const uint32_t* p, const uint32_t* code, uint64_t
   const Members MA = R.A->members(), MB = R.B->members();
   const Layer& A = *R.A;
   const Layer& OB = R.same ? *R.A : *R.B;
+  if (R.gctx) {
+    R.total += gpu_rows(R.gctx, *R.c, A, OB, GSJ_ENC_RELATE, R.same, R.distinct, false, 0.0, R.pat, p, nullptr, code, nullptr, n, &R.enc_s,
+                        &R.wr_s);
+    R.host_s += secs_since(th);
+    return;
+  }
   R.total += send_rows_acc(R, *R.c, n, [&](uint64_t i, FrameWriter& f) {
     const uint32_t cd = code[i], ct = gsj_de9im_transpose(cd);
     pair_rows(p[2 * i], p[2 * i + 1], MA, MB, R.same, R.distinct, [&](uint32_t ra, uint32_t rb, bool tr) {
@@ -751,6 +811,12 @@ int relate_sink(void* u, const uint32_t* p, const double*, const uint32_t* code,
 void relate_points_rows(RelateRun& R, const uint32_t* p, const uint8_t* wh, uint64_t n) {
   const auto th = Clock::now();
   const Members MB = R.B->members();
+  if (R.gctx) {   // A points, B polygons
+    R.total += gpu_rows(R.gctx, *R.c, *R.A, *R.B, GSJ_ENC_POINT_RELATE, false, false, R.swapped, 0.0, R.pat, p, nullptr, nullptr, wh, n,
+                        &R.enc_s, &R.wr_s);
+    R.host_s += secs_since(th);
+    return;
+  }
   R.total += send_rows_acc(R, *R.c, n, [&](uint64_t i, FrameWriter& f) {
     const uint32_t code = wh[i] == 2 ? kPtBoundary : kPtInterior;   // relate(point, polygon)
     MB.each(p[2 * i + 1], [&](uint32_t rb) {
@@ -796,6 +862,7 @@ void op_relate(Conn& c, const std::vector<std::string>& a) {
     if (R.A->points()) relate_points_rows(R, p, wh, n); else relate_rows(R, p, code, n);
   });
   R.out = &out;
+  if (!pipe && g_cfg.gpu_encode && A->rs && B->rs) R.gctx = ctx;
   gsj_join_stats st{};
   if (A->points()) {
     const int rc = gsj_join_points(ctx, A->h, B->h, &o, relate_points_sink, &R, &st);
@@ -832,6 +899,7 @@ struct PairsRun {
   uint64_t total = 0;
   double host_s = 0, enc_s = 0, wr_s = 0;
   Streamer* out = nullptr;
+  gsj_ctx* gctx = nullptr;   // set: rows encoded on the device
 };
 
 void pairs_rows(PairsRun& P, const uint32_t* p, uint64_t n) {
@@ -840,6 +908,9 @@ void pairs_rows(PairsRun& P, const uint32_t* p, uint64_t n) {
   if (P.A->points()) {   // (point, polygon parent) pairs
     if (P.stats_only) {
       for (uint64_t i = 0; i < n; i++) P.total += MB.count(p[2 * i + 1]);
+    } else if (P.gctx) {
+      P.total += gpu_rows(P.gctx, *P.c, *P.A, *P.B, GSJ_ENC_POINTS, false, false, P.swapped, kNaN, "", p, nullptr, nullptr, nullptr, n, &P.enc_s,
+                          &P.wr_s);
     } else {
       P.total += send_rows_acc(P, *P.c, n, [&](uint64_t i, FrameWriter& f) {
         MB.each(p[2 * i + 1], [&](uint32_t rb) {
@@ -854,6 +925,9 @@ void pairs_rows(PairsRun& P, const uint32_t* p, uint64_t n) {
 #pragma omp parallel for num_threads(g_cfg.threads) reduction(+ : t)
     for (int64_t i = 0; i < (int64_t)n; i++) t += pair_row_count(p[2 * i], p[2 * i + 1], MA, MB, P.same, P.distinct);
     P.total += t;
+  } else if (P.gctx) {
+    P.total += gpu_rows(P.gctx, *P.c, *P.A, P.same ? *P.A : *P.B, GSJ_ENC_PAIRS, P.same, P.distinct, false, 0.0, "", p, nullptr, nullptr,
+                        nullptr, n, &P.enc_s, &P.wr_s);
   } else {
     const Layer& A = *P.A;
     const Layer& OB = P.same ? *P.A : *P.B;
@@ -910,6 +984,7 @@ void op_dwithin(Conn& c, const std::vector<std::string>& a) {
   if (pipe) o.batch_q = g_cfg.stream_batch;
   Streamer out(pipe, [&](const uint32_t* p, const double*, const uint32_t*, const uint8_t*, uint64_t n) { pairs_rows(P, p, n); });
   P.out = &out;
+  if (!pipe && g_cfg.gpu_encode && A->rs && B->rs) P.gctx = ctx;
   gsj_join_stats st{};
   if (A->points()) {
     const int rc = erode ? gsj_points_erode(ctx, A->h, B->h, rb, &o, pairs_sink, &P, &st) : gsj_points_dwithin(ctx, A->h, B->h, d, &o, pairs_sink, &P, &st);
@@ -1082,7 +1157,7 @@ void on_signal(int) { g_stop = true; }
 
 const char* kUsage =
     "usage: gsjd [--socket PATH] [--tcp HOST:PORT] [--token-file FILE] [--data-dir DIR] [--device N] [--workers N]\n"
-    "            [--threads N] [--mem-budget-gb G] [--refine plain|filtered] [--stream-batch N]\n"
+    "            [--threads N] [--mem-budget-gb G] [--refine plain|filtered] [--stream-batch N] [--gpu-encode 0|1]\n"
     "            [--conninfo STR (accepted, unused: layers load from files)]\n";
 
 }  // namespace
@@ -1104,6 +1179,7 @@ extern "C" int gsjd_main(int argc, char** argv) {
     else if (a == "--threads" && has) g_cfg.threads = std::max(1, atoi(argv[++i]));
     else if (a == "--mem-budget-gb" && has) g_cfg.mem_budget_gb = atof(argv[++i]);
     else if (a == "--stream-batch" && has) g_cfg.stream_batch = (uint32_t)std::max(0, atoi(argv[++i]));
+    else if (a == "--gpu-encode" && has) g_cfg.gpu_encode = atoi(argv[++i]) != 0;
     else if (a == "--refine" && has) {
       const std::string m = argv[++i];
       if (m != "plain" && m != "filtered") { fputs("--refine plain|filtered\n", stderr); return 1; }

@@ -109,12 +109,13 @@ struct gsj_ctx {
   // scratch pools
   gsj::DevBuf counters, cand, flag, area, ev, evb, heavy, scratch, keep, opairs, oarea, oev, oevb, ocode, tmp, keys, keys2, idx,
       idx2, agg_area, agg_ev, agg_evb, agg_flag, qbb, uf, misc1, misc2, misc3,
-      er_pf, er_keep, er_off, er_pairs, er_flag, er_heavy, er_tiles, er_tiles2, er_slab, er_again, er_scr, er_ctr, er_tmp;
+      er_pf, er_keep, er_off, er_pairs, er_flag, er_heavy, er_tiles, er_tiles2, er_slab, er_again, er_scr, er_ctr, er_tmp,
+      enc_in, enc_cnt, enc_pre, enc_blk, enc_out;
   // every scratch pool, e.g. to bind them to the stream or release them before the stream goes
   template <class Fn> void each_buf(Fn&& fn) {
-    for (gsj::DevBuf* b : {&counters, &cand, &flag, &area, &ev, &evb, &heavy, &scratch, &keep, &opairs, &oarea, &oev, &oevb, &ocode, &tmp, &keys, &keys2, &idx, &idx2, &agg_area, &agg_ev, &agg_evb, &agg_flag, &qbb, &uf, &misc1, &misc2, &misc3, &er_pf, &er_keep, &er_off, &er_pairs, &er_flag, &er_heavy, &er_tiles, &er_tiles2, &er_slab, &er_again, &er_scr, &er_ctr, &er_tmp}) fn(*b);
+    for (gsj::DevBuf* b : {&counters, &cand, &flag, &area, &ev, &evb, &heavy, &scratch, &keep, &opairs, &oarea, &oev, &oevb, &ocode, &tmp, &keys, &keys2, &idx, &idx2, &agg_area, &agg_ev, &agg_evb, &agg_flag, &qbb, &uf, &misc1, &misc2, &misc3, &er_pf, &er_keep, &er_off, &er_pairs, &er_flag, &er_heavy, &er_tiles, &er_tiles2, &er_slab, &er_again, &er_scr, &er_ctr, &er_tmp, &enc_in, &enc_cnt, &enc_pre, &enc_blk, &enc_out}) fn(*b);
   }
-  gsj::PinnedBuf h_counters, h_pairs, h_area, h_code, h_where;
+  gsj::PinnedBuf h_counters, h_pairs, h_area, h_code, h_where, h_enc;
 };
 
 namespace gsj {
@@ -147,5 +148,12 @@ gsj_join_opts opts_or_default(const gsj_join_opts* o);
 // per-pair refinement (flag, area, ev, evb); returns the number of pairs that took the oversized path
 uint64_t refine(gsj_ctx* c, const gsj_layer* P, const gsj_layer* R, const uint2* pairs, uint64_t np, const RefineArgs& rp, int mode,
                 uint8_t* flag, double* area, double4* ev, uint32_t* evb);
+
+// device row encoding (encode.cu)
+uint64_t encode_rows(gsj_ctx* c, const gsj_rowset* P, const gsj_rowset* Q, const gsj_encode_spec* spec, const uint32_t* pairs, const double* area,
+                     const uint32_t* code, const uint8_t* where, uint64_t n, gsj_bytes_sink sink, void* user);
+gsj_rowset* rowset_upload(gsj_ctx* c, uint64_t n_geoms, const uint64_t* moff, const uint32_t* midx, uint64_t n_rows, const char* blob,
+                          const uint64_t* off);
+void rowset_free(gsj_rowset* r);
 
 }  // namespace gsj

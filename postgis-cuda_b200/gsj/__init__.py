@@ -24,6 +24,13 @@ _vp = ctypes.c_void_p
 JOIN_SINK = ctypes.CFUNCTYPE(ctypes.c_int, _vp, _u32p, _f64p, _u32p, ctypes.c_uint64)
 POINTS_SINK = ctypes.CFUNCTYPE(ctypes.c_int, _vp, _u32p, _u8p, ctypes.c_uint64)
 PAIRS_SINK = ctypes.CFUNCTYPE(ctypes.c_int, _vp, _u32p, ctypes.c_uint64)
+BYTES_SINK = ctypes.CFUNCTYPE(ctypes.c_int, _vp, _u8p, ctypes.c_uint64, ctypes.c_uint64)
+GSJ_ENC_PAIRS, GSJ_ENC_RELATE, GSJ_ENC_POINTS, GSJ_ENC_POINT_RELATE = 0, 1, 2, 3
+
+
+class EncodeSpec(ctypes.Structure):
+    _fields_ = [("mode", ctypes.c_int), ("same", ctypes.c_int), ("distinct", ctypes.c_int), ("swapped", ctypes.c_int),
+                ("point_value", ctypes.c_double), ("pattern", ctypes.c_char * 10)]
 
 
 class RefineParams(ctypes.Structure):
@@ -98,6 +105,10 @@ SIGNATURES = {
     "gsj_dedup": (ctypes.c_int, [ctypes.c_uint64] * 3 + [_vp] * 3 + [ctypes.c_int] + [ctypes.POINTER(ctypes.c_uint64)] * 3 +
                   [ctypes.POINTER(_vp)] * 5),
     "gsj_host_free": (None, [_vp]),
+    "gsj_rowset_upload": (ctypes.c_int, [_vp, ctypes.c_uint64, _vp, _vp, ctypes.c_uint64, _vp, _vp, ctypes.POINTER(_vp)]),
+    "gsj_rowset_free": (None, [_vp]),
+    "gsj_encode_rows": (ctypes.c_int, [_vp, _vp, _vp, ctypes.POINTER(EncodeSpec), _vp, _vp, _vp, _vp, ctypes.c_uint64, BYTES_SINK, _vp,
+                                       ctypes.POINTER(ctypes.c_uint64)]),
     "gsj_de9im_str": (None, [ctypes.c_uint32, ctypes.c_char_p]),
     "gsj_de9im_transpose": (ctypes.c_uint32, [ctypes.c_uint32]),
     "gsj_de9im_match": (ctypes.c_int, [ctypes.c_uint32, ctypes.c_char_p]),
@@ -182,6 +193,16 @@ def dedup(ps, morton=False):
 
 
 @dataclasses.dataclass
+class _RowsetHandle:
+    def __init__(self, h):
+        self.h = h
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().gsj_rowset_free(self.h)
+            self.h = None
+
+
 class JoinResult:
     pairs: np.ndarray          # (n, 2) uint32: (P parent, R parent)
     area: np.ndarray | None    # (n,) float64
@@ -368,6 +389,42 @@ class Engine:
 
     def points_erode(self, pts: Layer, R: Layer, r: float, refine_mode=GSJ_REFINE_FILTERED):
         return self._pairs_call(lib().gsj_points_erode, pts.h, R.h, float(r), opts=join_opts(refine_mode=refine_mode))
+
+    # ---- row encoding on the device (the daemon's result frames) ----
+    def rowset(self, ids, moff=None, midx=None):
+        """Device row ids (list of bytes) and optional dedup members (moff[n_geoms + 1], midx) for encode_rows."""
+        blob = b"".join(ids)
+        off = np.zeros(len(ids) + 1, np.uint64)
+        off[1:] = np.cumsum([len(x) for x in ids])
+        mo = None if moff is None else np.ascontiguousarray(moff, np.uint64)
+        mi = None if midx is None else np.ascontiguousarray(midx, np.uint32)
+        n_geoms = len(ids) if mo is None else len(mo) - 1
+        h = _vp()
+        bb = ctypes.create_string_buffer(blob, max(1, len(blob)))
+        self._check(lib().gsj_rowset_upload(self.ctx, n_geoms, None if mo is None else mo.ctypes.data, None if mi is None else mi.ctypes.data,
+                                            len(ids), bb, off.ctypes.data, ctypes.byref(h)))
+        return _RowsetHandle(h)
+
+    def encode_rows(self, P, Q, mode, pairs, area=None, code=None, where=None, same=False, distinct=False, swapped=False, point_value=0.0,
+                    pattern=""):
+        """(stream bytes, rows) of gsj_encode_rows."""
+        pairs = np.ascontiguousarray(pairs, np.uint32).reshape(-1, 2)
+        a = None if area is None else np.ascontiguousarray(area, np.float64)
+        c = None if code is None else np.ascontiguousarray(code, np.uint32)
+        w = None if where is None else np.ascontiguousarray(where, np.uint8)
+        sp = EncodeSpec(mode, int(same), int(distinct), int(swapped), float(point_value), pattern.encode())
+        chunks = []
+
+        def sink(user, b, nb, nr):
+            chunks.append(ctypes.string_at(b, nb))
+            return 0
+
+        cb = BYTES_SINK(sink)
+        rows = ctypes.c_uint64()
+        self._check(lib().gsj_encode_rows(self.ctx, P.h, Q.h, ctypes.byref(sp), pairs.ctypes.data, None if a is None else a.ctypes.data,
+                                          None if c is None else c.ctypes.data, None if w is None else w.ctypes.data, len(pairs), cb, None,
+                                          ctypes.byref(rows)))
+        return b"".join(chunks), rows.value
 
     # ---- parity / diagnostics ----
     def candidates(self, P: Layer, R: Layer, upper=False) -> np.ndarray:

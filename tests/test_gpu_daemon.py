@@ -238,18 +238,18 @@ def test_client_gone_and_drop(env):
 
 
 def test_stream_batches_same_rows(env):
-    """Rows streamed from probe batches of 64 query geometries (a sender thread encodes and writes each batch while
-    the engine refines the next) equal the rows of one batch sent after the join, for every streamed op: same
-    pairs, bit-identical areas, same DE-9IM strings."""
+    """The same rows (pairs, bit-identical areas, DE-9IM strings) for every streamed op from: one batch encoded on the
+    device (the default), probe batches of 64 query geometries encoded on the host by a sender thread while the
+    engine refines the next batch, and one batch encoded on the host."""
     def norm(rows):
         return sorted(tuple(-1.0 if isinstance(x, float) and math.isnan(x) else x for x in r) for r in rows)
 
     res, procs = {}, []
     try:
-        for sb in (0, 64):
+        for sb, flags in ((0, []), (64, ["--stream-batch", "64"]), (1, ["--gpu-encode", "0"])):
             sock = str(env.dir / f"gsjd_sb{sb}.sock")
             log = open(env.dir / f"gsjd_sb{sb}.log", "w")
-            procs.append((D.start(sock, str(env.dir), workers=2, log=log, extra=["--stream-batch", str(sb)]), log))
+            procs.append((D.start(sock, str(env.dir), workers=2, log=log, extra=flags), log))
             cl = C.Client(sock)
             cl.load("parcels", "parcels.copy")
             cl.load("parcels_sub", "parcels.copy", subdivide=32)
@@ -267,5 +267,5 @@ def test_stream_batches_same_rows(env):
             D.stop(p)
             log.close()
     assert env.info["points"]["rows"] > 64 * 8 and env.info["parcels"]["rows"] > 64 * 8   # many batches
-    for a, b in zip(res[0], res[64]):
-        assert a == b and len(a) > 0
+    for a, b, c in zip(res[0], res[64], res[1]):
+        assert a == b == c and len(a) > 0
