@@ -15,6 +15,7 @@
 //  - rows are encoded by a pool of --threads encoder threads started once, into per-thread buffers kept across
 //    requests; every engine context is created at start-up.
 #include <arpa/inet.h>
+#include <dirent.h>
 #include <netinet/in.h>
 #include <netinet/tcp.h>
 #include <omp.h>
@@ -24,6 +25,7 @@
 #include <sys/un.h>
 #include <unistd.h>
 
+#include <algorithm>
 #include <atomic>
 #include <cerrno>
 #include <chrono>
@@ -67,6 +69,7 @@ struct Config {
   double mem_budget_gb = 0;   // scratch budget shared by running requests (0: half of the free memory at first use)
   uint32_t stream_batch = 0;   // probe geometries per engine batch when rows are streamed (0: one batch)
   int gpu_encode = 1;           // rows encoded on the device (gsj_encode_rows) when they are sent from the engine's thread
+  std::string snapshot_dir;     // prepared layers saved here after LOAD and restored at start-up (empty: off)
 };
 Config g_cfg;
 std::atomic<bool> g_stop{false};
@@ -281,6 +284,129 @@ template <class T> struct HostArray {   // library-allocated host arrays (gsj_de
   ~HostArray() { if (p) gsj_host_free(p); }
 };
 
+// ---- prepared-layer snapshots: a restart restores every loaded layer without reading, deduplicating or
+// subdividing its source again. One file per layer: header, ids, members, then the arrays as uploaded. ----
+constexpr char kSnapMagic[8] = {'G', 'S', 'J', 'S', 'N', 'A', 'P', '1'};
+struct SnapArrays {   // what gsj_layer_upload_* received
+  uint64_t n = 0, nr = 0, nv = 0;
+  const uint64_t* gro = nullptr; const uint64_t* rvo = nullptr; const double* xy = nullptr;
+  const uint32_t* parent = nullptr; const uint8_t* syn = nullptr;
+};
+std::string snapshot_path(const std::string& name) {
+  static const char* hx = "0123456789abcdef";
+  std::string f;
+  for (unsigned char ch : name) { f += hx[ch >> 4]; f += hx[ch & 15]; }
+  return g_cfg.snapshot_dir + "/" + f + ".gsnap";
+}
+void write_snapshot(const Layer& L, const SnapArrays& A) {
+  const std::string path = snapshot_path(L.name), tmp = path + ".tmp";
+  FILE* f = fopen(tmp.c_str(), "wb");
+  if (!f) { logf("snapshot %s: cannot write %s", L.name.c_str(), tmp.c_str()); return; }
+  bool ok = true;
+  auto put = [&](const void* p, size_t n) { if (ok && n && fwrite(p, 1, n, f) != n) ok = false; };
+  auto put64 = [&](uint64_t v) { put(&v, 8); };
+  auto putstr = [&](const std::string& v) { put64(v.size()); put(v.data(), v.size()); };
+  put(kSnapMagic, 8);
+  put64(L.points() ? 1 : 0); put64((uint64_t)L.subdiv); put64(L.deduped ? 1 : 0);
+  put64(L.rows); put64(L.skipped); put64(L.n_distinct); put64(A.n); put64(A.nr); put64(A.nv);
+  putstr(L.name); putstr(L.source);
+  put64(L.ids.buf.size()); put(L.ids.buf.data(), L.ids.buf.size()); put(L.ids.off.data(), L.ids.off.size() * 8);
+  if (L.deduped) { put(L.moff.data(), L.moff.size() * 8); put(L.midx.data(), L.midx.size() * 4); }
+  if (L.points()) {
+    put(A.xy, A.n * 16);
+  } else {
+    put(A.gro, (A.n + 1) * 8); put(A.rvo, (A.nr + 1) * 8); put(A.xy, A.nv * 16);
+    put64(A.parent ? 1 : 0);
+    if (A.parent) { put(A.parent, A.n * 4); put(A.syn, A.nv); }
+  }
+  ok = fclose(f) == 0 && ok;
+  if (!ok || rename(tmp.c_str(), path.c_str()) != 0) { remove(tmp.c_str()); logf("snapshot %s: write failed", L.name.c_str()); }
+}
+void register_layer(const std::shared_ptr<Layer>& L) {
+  std::shared_ptr<Layer> old;
+  std::lock_guard<std::mutex> g(g_reg);
+  auto& slot = g_layers[L->name];
+  old = slot;
+  slot = L;
+}
+// restores one snapshot; returns "" or the reason it was skipped
+std::string restore_snapshot(const std::string& path) {
+  FILE* f = fopen(path.c_str(), "rb");
+  if (!f) return "cannot open";
+  std::unique_ptr<FILE, int (*)(FILE*)> guard(f, fclose);
+  bool ok = true;
+  auto get = [&](void* p, size_t n) { if (ok && n && fread(p, 1, n, f) != n) ok = false; };
+  auto get64 = [&]() { uint64_t v = 0; get(&v, 8); return v; };
+  auto getstr = [&]() { std::string v(std::min<uint64_t>(get64(), 1 << 20), '\0'); get(&v[0], v.size()); return v; };
+  char mg[8] = {0};
+  get(mg, 8);
+  if (!ok || std::memcmp(mg, kSnapMagic, 8) != 0) return "not a snapshot";
+  auto L = std::make_shared<Layer>();
+  const bool pts = get64() != 0;
+  L->subdiv = (int)get64(); L->deduped = get64() != 0;
+  L->rows = get64(); L->skipped = get64(); L->n_distinct = get64();
+  const uint64_t n = get64(), nr = get64(), nv = get64();
+  L->name = getstr(); L->source = getstr() + " (snapshot)";
+  if (!ok || L->rows == 0 || L->rows > (1ull << 32) || n > (1ull << 32) || nv > (1ull << 40)) return "bad header";
+  const uint64_t blob = get64();
+  if (!ok || blob > (1ull << 36)) return "bad id table";
+  L->ids.buf.resize(blob); get(&L->ids.buf[0], blob);
+  L->ids.off.resize(L->rows + 1); get(L->ids.off.data(), (L->rows + 1) * 8);
+  if (!ok || L->ids.off[0] != 0 || L->ids.off[L->rows] != blob) return "bad id table";
+  if (L->deduped) {
+    L->moff.resize(L->n_distinct + 1); get(L->moff.data(), L->moff.size() * 8);
+    L->midx.resize(L->rows); get(L->midx.data(), L->midx.size() * 4);
+  }
+  std::vector<uint64_t> gro, rvo;
+  std::vector<double> xy;
+  std::vector<uint32_t> parent;
+  std::vector<uint8_t> syn;
+  Lease lease;
+  if (pts) {
+    L->kind = "point"; L->gpu_geoms = L->verts = n;
+    xy.resize(2 * n); get(xy.data(), n * 16);
+    if (!ok) return "truncated";
+    check(lease.get(), gsj_layer_upload_points(lease.get(), n, xy.data(), &L->h), "upload");
+  } else {
+    L->kind = "polygon"; L->gpu_geoms = n; L->verts = nv;
+    gro.resize(n + 1); rvo.resize(nr + 1); xy.resize(2 * nv);
+    get(gro.data(), gro.size() * 8); get(rvo.data(), rvo.size() * 8); get(xy.data(), nv * 16);
+    if (get64()) { parent.resize(n); syn.resize(nv); get(parent.data(), n * 4); get(syn.data(), nv); }
+    if (!ok) return "truncated";
+    if (gro[0] != 0 || gro[n] != nr || rvo[0] != 0 || rvo[nr] != nv) return "inconsistent offsets";
+    check(lease.get(), gsj_layer_upload_polygons(lease.get(), n, nr, nv, gro.data(), rvo.data(), xy.data(), parent.empty() ? nullptr : parent.data(),
+                                                 syn.empty() ? nullptr : syn.data(), &L->h), "upload");
+  }
+  check(lease.get(), gsj_rowset_upload(lease.get(), L->n_distinct, L->deduped ? L->moff.data() : nullptr, L->deduped ? L->midx.data() : nullptr,
+                                       L->rows, L->ids.buf.data(), L->ids.off.data(), &L->rs), "row ids upload");
+  gsj_layer_info info;
+  gsj_layer_get_info(L->h, &info);
+  L->gpu_bytes = info.device_bytes;
+  register_layer(L);
+  logf("restored %s from %s: %s", L->name.c_str(), path.c_str(), L->json().c_str());
+  return "";
+}
+void restore_snapshots() {
+  if (g_cfg.snapshot_dir.empty()) return;
+  DIR* d = opendir(g_cfg.snapshot_dir.c_str());
+  if (!d) { logf("snapshot dir %s: cannot open", g_cfg.snapshot_dir.c_str()); return; }
+  std::vector<std::string> files;
+  while (dirent* e = readdir(d)) {
+    const std::string nm = e->d_name;
+    if (nm.size() > 6 && nm.compare(nm.size() - 6, 6, ".gsnap") == 0) files.push_back(g_cfg.snapshot_dir + "/" + nm);
+  }
+  closedir(d);
+  std::sort(files.begin(), files.end());
+  for (const auto& fpath : files) {
+    try {
+      const std::string why = restore_snapshot(fpath);
+      if (!why.empty()) logf("snapshot %s skipped: %s", fpath.c_str(), why.c_str());
+    } catch (const std::exception& ex) {
+      logf("snapshot %s skipped: %s", fpath.c_str(), ex.what());
+    }
+  }
+}
+
 std::string build_layer(const std::string& name, const std::string& path, int subdiv, bool dedup) {
   auto t0 = Clock::now();
   LoadedLayer ld;
@@ -301,6 +427,10 @@ std::string build_layer(const std::string& name, const std::string& path, int su
     auto t1 = Clock::now();
     check(lease.get(), gsj_layer_upload_points(lease.get(), L->rows, ld.xy.data(), &L->h), "upload");
     L->upload_s = secs_since(t1);
+    if (!g_cfg.snapshot_dir.empty()) {
+      SnapArrays A; A.n = L->rows; A.xy = ld.xy.data();
+      write_snapshot(*L, A);
+    }
   } else {
     L->kind = "polygon";
     const uint64_t n = ld.gro.size() - 1;
@@ -341,6 +471,11 @@ std::string build_layer(const std::string& name, const std::string& path, int su
     check(lease.get(), gsj_layer_upload_polygons(lease.get(), bn, bnr, bnv, gro, rvo, xy, subdiv > 0 ? spar.p : nullptr,
                                                  subdiv > 0 ? ssyn.p : nullptr, &L->h), "upload");
     L->upload_s = secs_since(t1);
+    if (!g_cfg.snapshot_dir.empty()) {   // the arrays as uploaded (after dedup / subdivision), with the ids and members
+      SnapArrays A; A.n = bn; A.nr = bnr; A.nv = bnv; A.gro = gro; A.rvo = rvo; A.xy = xy;
+      if (subdiv > 0) { A.parent = spar.p; A.syn = ssyn.p; }
+      write_snapshot(*L, A);
+    }
   }
   {
     Lease lease;
@@ -352,13 +487,7 @@ std::string build_layer(const std::string& name, const std::string& path, int su
   L->gpu_bytes = info.device_bytes;
   const std::string js = L->json();
   logf("load %s: ready %s", name.c_str(), js.c_str());
-  std::shared_ptr<Layer> old;
-  {
-    std::lock_guard<std::mutex> g(g_reg);
-    auto& slot = g_layers[name];
-    old = slot;
-    slot = L;
-  }
+  register_layer(L);
   return js;
 }
 
@@ -1107,6 +1236,7 @@ void handle(int fd) {
           auto it = g_layers.find(args[0]);
           if (it != g_layers.end()) { old = it->second; g_layers.erase(it); }
         }
+        if (old && !g_cfg.snapshot_dir.empty()) remove(snapshot_path(args[0]).c_str());   // not restored any more
         c.ok_json(old ? "true" : "false");
         break;
       }
@@ -1158,6 +1288,7 @@ void on_signal(int) { g_stop = true; }
 const char* kUsage =
     "usage: gsjd [--socket PATH] [--tcp HOST:PORT] [--token-file FILE] [--data-dir DIR] [--device N] [--workers N]\n"
     "            [--threads N] [--mem-budget-gb G] [--refine plain|filtered] [--stream-batch N] [--gpu-encode 0|1]\n"
+    "            [--snapshot-dir DIR (prepared layers saved after LOAD, restored at start-up)]\n"
     "            [--conninfo STR (accepted, unused: layers load from files)]\n";
 
 }  // namespace
@@ -1180,6 +1311,7 @@ extern "C" int gsjd_main(int argc, char** argv) {
     else if (a == "--mem-budget-gb" && has) g_cfg.mem_budget_gb = atof(argv[++i]);
     else if (a == "--stream-batch" && has) g_cfg.stream_batch = (uint32_t)std::max(0, atoi(argv[++i]));
     else if (a == "--gpu-encode" && has) g_cfg.gpu_encode = atoi(argv[++i]) != 0;
+    else if (a == "--snapshot-dir" && has) g_cfg.snapshot_dir = argv[++i];
     else if (a == "--refine" && has) {
       const std::string m = argv[++i];
       if (m != "plain" && m != "filtered") { fputs("--refine plain|filtered\n", stderr); return 1; }
@@ -1204,6 +1336,7 @@ extern "C" int gsjd_main(int argc, char** argv) {
   g_encode.start(std::max(0, g_cfg.threads - 1));
   g_pool_small.prewarm();   // before the socket exists: a client that can connect finds the contexts ready
   g_pool_large.prewarm();
+  restore_snapshots();
   std::vector<pollfd> fds;
   const int u = listen_unix(g_cfg.socket);
   if (u < 0) return 1;

@@ -269,3 +269,44 @@ def test_stream_batches_same_rows(env):
     assert env.info["points"]["rows"] > 64 * 8 and env.info["parcels"]["rows"] > 64 * 8   # many batches
     for a, b, c in zip(res[0], res[64], res[1]):
         assert a == b == c and len(a) > 0
+
+
+def test_snapshots_restore_layers(env, tmp_path):
+    """--snapshot-dir: a restarted daemon restores every loaded layer (deduplicated, subdivided, points) from its
+    snapshot, without the source files, and answers with the same rows; a dropped layer is not restored."""
+    snap = tmp_path / "snap"
+    snap.mkdir()
+
+    def start(tag):
+        log = open(env.dir / f"gsjd_snap_{tag}.log", "w")
+        sock = str(env.dir / f"gsjd_snap_{tag}.sock")
+        return D.start(sock, str(env.dir), workers=2, log=log, extra=["--snapshot-dir", str(snap)]), log, C.Client(sock)
+
+    def info(cl):
+        return sorted((x["layer"], x["kind"], x["rows"], x["distinct"], x["gpu_geoms"], x["dedup"]) for x in cl.list())
+
+    def queries(cl):   # NaN payloads (dwithin rows) compared as a marker: NaN != NaN
+        return [sorted(tuple(-1.0 if isinstance(v, float) and math.isnan(v) else v for v in r) for r in rows) for rows, _ in (cl.join("parcels", "parcels", True, "all"), cl.join("parcels_sub", "parcels2", True),
+                                             cl.relate("points", "parcels", "", "all"), cl.dwithin("parcels", "parcels2", 5.0))]
+
+    p, log, cl = start("a")
+    try:
+        cl.load("parcels", "parcels.copy")
+        cl.load("parcels_sub", "parcels.copy", subdivide=32)
+        cl.load("parcels2", "parcels2.gset")
+        cl.load("points", "points.pset")
+        cl.load("gone", "parcels2.gset")
+        want = queries(cl)
+        assert cl.drop("gone") is True
+        layers = info(cl)
+    finally:
+        D.stop(p)
+        log.close()
+    assert len(list(snap.glob("*.gsnap"))) == 4
+    p, log, cl = start("b")
+    try:
+        assert info(cl) == layers and [x[0] for x in layers] == ["parcels", "parcels2", "parcels_sub", "points"]
+        assert queries(cl) == want and all(len(w) > 0 for w in want)
+    finally:
+        D.stop(p)
+        log.close()
