@@ -192,7 +192,6 @@ def dedup(ps, morton=False):
     return u, _take(ptrs[3], n.value + 1, np.uint64), _take(ptrs[4], len(gro) - 1, np.uint32)
 
 
-@dataclasses.dataclass
 class _RowsetHandle:
     def __init__(self, h):
         self.h = h
@@ -203,6 +202,7 @@ class _RowsetHandle:
             self.h = None
 
 
+@dataclasses.dataclass
 class JoinResult:
     pairs: np.ndarray          # (n, 2) uint32: (P parent, R parent)
     area: np.ndarray | None    # (n,) float64

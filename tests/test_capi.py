@@ -3,6 +3,8 @@ import ctypes
 import os
 import re
 
+import numpy as np
+
 import gsj
 from gsj._build import lib_path
 
@@ -45,3 +47,8 @@ def test_errors_are_status_codes_not_exits():
     rc = gsj.lib().gsj_ctx_create(0, ctypes.byref(h))
     assert rc != 0 and not h.value
     assert gsj.lib().gsj_join(None, None, None, None, None, gsj.JOIN_SINK(lambda *a: 0), None, None) == 1
+
+
+def test_result_types_construct_without_gpu():
+    r = gsj.JoinResult(np.zeros((0, 2), np.uint32), None, None, {"candidates": 0})
+    assert len(r.pairs) == 0 and r.stats["candidates"] == 0
