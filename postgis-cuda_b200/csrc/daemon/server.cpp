@@ -357,25 +357,25 @@ std::string restore_snapshot(const std::string& path) {
     L->moff.resize(L->n_distinct + 1); get(L->moff.data(), L->moff.size() * 8);
     L->midx.resize(L->rows); get(L->midx.data(), L->midx.size() * 4);
   }
-  std::vector<uint64_t> gro, rvo;
-  std::vector<double> xy;
-  std::vector<uint32_t> parent;
-  std::vector<uint8_t> syn;
+  // the big arrays are read into uninitialised buffers (a zero-filled vector would write them twice)
+  std::unique_ptr<uint64_t[]> gro, rvo;
+  std::unique_ptr<double[]> xy;
+  std::unique_ptr<uint32_t[]> parent;
+  std::unique_ptr<uint8_t[]> syn;
   Lease lease;
   if (pts) {
     L->kind = "point"; L->gpu_geoms = L->verts = n;
-    xy.resize(2 * n); get(xy.data(), n * 16);
+    xy.reset(new double[2 * n]); get(xy.get(), n * 16);
     if (!ok) return "truncated";
-    check(lease.get(), gsj_layer_upload_points(lease.get(), n, xy.data(), &L->h), "upload");
+    check(lease.get(), gsj_layer_upload_points(lease.get(), n, xy.get(), &L->h), "upload");
   } else {
     L->kind = "polygon"; L->gpu_geoms = n; L->verts = nv;
-    gro.resize(n + 1); rvo.resize(nr + 1); xy.resize(2 * nv);
-    get(gro.data(), gro.size() * 8); get(rvo.data(), rvo.size() * 8); get(xy.data(), nv * 16);
-    if (get64()) { parent.resize(n); syn.resize(nv); get(parent.data(), n * 4); get(syn.data(), nv); }
+    gro.reset(new uint64_t[n + 1]); rvo.reset(new uint64_t[nr + 1]); xy.reset(new double[2 * nv]);
+    get(gro.get(), (n + 1) * 8); get(rvo.get(), (nr + 1) * 8); get(xy.get(), nv * 16);
+    if (get64()) { parent.reset(new uint32_t[n]); syn.reset(new uint8_t[nv]); get(parent.get(), n * 4); get(syn.get(), nv); }
     if (!ok) return "truncated";
     if (gro[0] != 0 || gro[n] != nr || rvo[0] != 0 || rvo[nr] != nv) return "inconsistent offsets";
-    check(lease.get(), gsj_layer_upload_polygons(lease.get(), n, nr, nv, gro.data(), rvo.data(), xy.data(), parent.empty() ? nullptr : parent.data(),
-                                                 syn.empty() ? nullptr : syn.data(), &L->h), "upload");
+    check(lease.get(), gsj_layer_upload_polygons(lease.get(), n, nr, nv, gro.get(), rvo.get(), xy.get(), parent.get(), syn.get(), &L->h), "upload");
   }
   check(lease.get(), gsj_rowset_upload(lease.get(), L->n_distinct, L->deduped ? L->moff.data() : nullptr, L->deduped ? L->midx.data() : nullptr,
                                        L->rows, L->ids.buf.data(), L->ids.off.data(), &L->rs), "row ids upload");
