@@ -5,6 +5,7 @@
 #include <cmath>
 #include <cub/cub.cuh>
 #include <omp.h>
+#include <thread>
 #include "engine.h"
 
 namespace gsj {
@@ -64,9 +65,32 @@ void layer_upload_polygons(gsj_ctx* c, uint64_t n, uint64_t nr, uint64_t nv, con
   if (n == 0 || n >= (1ull << 31) || nr >= (1ull << 32)) throw Error(GSJ_ERR_ARG, "layer size out of range (0 < n < 2^31 geometries, rings < 2^32)");
   if (!gro || !rvo || !xy) throw Error(GSJ_ERR_ARG, "gro / rvo / xy must not be NULL");
   if (gro[0] != 0 || gro[n] != nr || rvo[0] != 0 || rvo[nr] != nv) throw Error(GSJ_ERR_ARG, "offset arrays are inconsistent with n / nr / nv");
-  for (uint64_t g = 0; g < n; g++) if (gro[g + 1] < gro[g]) throw Error(GSJ_ERR_ARG, "gro must be non-decreasing");
-  for (uint64_t r = 0; r < nr; r++) if (rvo[r + 1] < rvo[r]) throw Error(GSJ_ERR_ARG, "rvo must be non-decreasing");
-  if (parent) for (uint64_t g = 1; g < n; g++) if (parent[g] < parent[g - 1]) throw Error(GSJ_ERR_ARG, "parent must be non-decreasing");
+  int bad_g = 0, bad_r = 0, bad_p = 0;
+#pragma omp parallel for reduction(| : bad_g) schedule(static)
+  for (int64_t g = 0; g < (int64_t)n; g++) bad_g |= gro[g + 1] < gro[g];
+#pragma omp parallel for reduction(| : bad_r) schedule(static)
+  for (int64_t r = 0; r < (int64_t)nr; r++) bad_r |= rvo[r + 1] < rvo[r];
+  if (parent) {
+#pragma omp parallel for reduction(| : bad_p) schedule(static)
+    for (int64_t g = 1; g < (int64_t)n; g++) bad_p |= parent[g] < parent[g - 1];
+  }
+  if (bad_g) throw Error(GSJ_ERR_ARG, "gro must be non-decreasing");
+  if (bad_r) throw Error(GSJ_ERR_ARG, "rvo must be non-decreasing");
+  if (bad_p) throw Error(GSJ_ERR_ARG, "parent must be non-decreasing");
+  // real boundary length per geometry for relate (engine.cuh:69-82): host std::hypot, as the reference; computed
+  // on a helper thread while the arrays are copied and the LBVH is built
+  std::vector<double> glen(n, 0.0);
+  std::thread glen_th([&] {
+#pragma omp parallel for schedule(dynamic, 4096)
+    for (int64_t g = 0; g < (int64_t)n; g++) {
+      double len = 0;
+      for (uint64_t r = gro[g]; r < gro[g + 1]; r++)
+        for (uint64_t v = rvo[r]; v + 1 < rvo[r + 1]; v++)
+          if (!syn || !syn[v]) len += std::hypot(xy[2 * v + 2] - xy[2 * v], xy[2 * v + 3] - xy[2 * v + 1]);
+      glen[g] = len;
+    }
+  });
+  struct Joiner { std::thread& t; ~Joiner() { if (t.joinable()) t.join(); } } glen_join{glen_th};   // also on an exception
   L->is_points = 0;
   L->d.n = (uint32_t)n; L->d.nr = (uint32_t)nr; L->d.nv = nv;
   cudaStream_t s = c->stream;
@@ -94,23 +118,8 @@ void layer_upload_polygons(gsj_ctx* c, uint64_t n, uint64_t nr, uint64_t nv, con
   k_prep_polygons<<<grid_for((uint64_t)n * 32, 256), 256, 0, s>>>((uint32_t)n, d_gro, d_rvo, d_xy, d_origin, d_ext, d_bb);
   GSJ_CK(cudaGetLastError());
   L->d.gro = d_gro; L->d.rvo = d_rvo; L->d.xy = d_xy; L->d.origin = d_origin; L->d.ext = d_ext; L->d.bb = d_bb;
-  // real boundary length per parent for relate (engine.cuh:69-82): host std::hypot, as the reference
   uint32_t np = parent ? parent[n - 1] + 1 : (uint32_t)n;
   L->nparent = np;
-  std::vector<double> glen(n, 0.0);
-#pragma omp parallel for schedule(dynamic, 4096)
-  for (int64_t g = 0; g < (int64_t)n; g++) {
-    double len = 0;
-    for (uint64_t r = gro[g]; r < gro[g + 1]; r++)
-      for (uint64_t v = rvo[r]; v + 1 < rvo[r + 1]; v++)
-        if (!syn || !syn[v]) len += std::hypot(xy[2 * v + 2] - xy[2 * v], xy[2 * v + 3] - xy[2 * v + 1]);
-    glen[g] = len;
-  }
-  std::vector<double> bl(np, 0.0);
-  for (uint64_t g = 0; g < n; g++) bl[parent ? parent[g] : g] += glen[g];
-  double* d_blen = dmalloc<double>(L, np);
-  GSJ_CK(cudaMemcpyAsync(d_blen, bl.data(), np * 8, cudaMemcpyHostToDevice, s));
-  L->d.blen = d_blen;
   std::vector<uint32_t> bits;
   if (syn) {
     bits.assign((nv + 31) / 32, 0);
@@ -128,6 +137,13 @@ void layer_upload_polygons(gsj_ctx* c, uint64_t n, uint64_t nr, uint64_t nv, con
   // host staging vectors above are released at return: the copies must have finished
   GSJ_CK(cudaStreamSynchronize(s));
   build_bvh(c, L);
+  glen_th.join();
+  std::vector<double> bl(np, 0.0);   // per parent, pieces in order (the reference's summation order)
+  for (uint64_t g = 0; g < n; g++) bl[parent ? parent[g] : g] += glen[g];
+  double* d_blen = dmalloc<double>(L, np);
+  GSJ_CK(cudaMemcpyAsync(d_blen, bl.data(), np * 8, cudaMemcpyHostToDevice, s));
+  L->d.blen = d_blen;
+  GSJ_CK(cudaStreamSynchronize(s));
 }
 
 void layer_upload_points(gsj_ctx* c, uint64_t n, const double* xy, gsj_layer* L) {
