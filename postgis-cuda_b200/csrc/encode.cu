@@ -96,6 +96,8 @@ __device__ __forceinline__ const RowsDev& yset(const Spec& S, const RowsDev& P, 
   return (S.swapped && (S.mode == GSJ_ENC_POINTS || S.mode == GSJ_ENC_POINT_RELATE)) ? P : Q;
 }
 
+}  // namespace
+
 __global__ void k_enc_count(Spec S, const uint2* __restrict__ pairs, const uint32_t* __restrict__ code, const uint8_t* __restrict__ where,
                             uint64_t n, RowsDev P, RowsDev Q, unsigned long long* rows, unsigned long long* bytes) {
   const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -161,6 +163,8 @@ __global__ void k_enc_write(Spec S, const uint2* __restrict__ pairs, const doubl
     }
   });
 }
+
+namespace {
 
 RowsDev dev_of(const gsj_rowset* r) { return RowsDev{r->moff, r->midx, r->blob, r->off}; }
 
