@@ -199,7 +199,9 @@ int gsj_refine_pairs_noalloc(gsj_ctx* ctx, const gsj_layer* P, const gsj_layer* 
  *                   transposed when swapped, kept when it matches pattern
  * P holds the ids of the pairs' first members, Q of the second (for same, pass the same rowset twice).
  * Frames hold whole pairs' rows, ~1 MiB each for ids up to ~16 bytes; frame boundaries are not the host
- * encoder's, the rows are the same. Runs on the context's stream; returns after the sink returned. */
+ * encoder's, the rows are the same. Runs on the context's stream; returns after the sink returned. It may be called
+ * from inside a join's sink on the same context (its scratch is its own; the join continues after it on the stream).
+ * Ids longer than 65535 bytes are cut to 65535, as the host encoder does. */
 typedef struct gsj_rowset gsj_rowset;
 enum { GSJ_ENC_PAIRS = 0, GSJ_ENC_RELATE = 1, GSJ_ENC_POINTS = 2, GSJ_ENC_POINT_RELATE = 3 };
 typedef struct {

@@ -165,3 +165,13 @@ def test_bad_arguments(engine, sets):
     with pytest.raises(gsj.GsjError):
         engine.encode_rows(sets["U"], sets["U"], gsj.GSJ_ENC_RELATE, np.array([[0, 0]], np.uint32), code=np.zeros(1, np.uint32),
                            pattern="T*")
+
+
+def test_long_ids_are_cut_like_the_host_encoder(engine):
+    """An id longer than a u16 length can say is sent as its first 65535 bytes (FrameWriter::id does the same)."""
+    ids = [b"a" * 70000, b"b", b"c" * 65535]
+    S = engine.rowset(ids)
+    pairs = np.array([[0, 1], [2, 0], [1, 1]], np.uint32)
+    buf, n = engine.encode_rows(S, S, gsj.GSJ_ENC_PAIRS, pairs, area=np.array([1.0, 2.0, 3.0]))
+    got = decode(buf, 8)
+    assert n == 3 and [(len(a), len(b)) for a, b, _ in got] == [(65535, 1), (65535, 65535), (1, 1)]
