@@ -294,6 +294,8 @@ def run_op(args, rank, local, ws):
     eng = gsj.Engine(local)
     ext = torch.cuda.ExternalStream(eng.stream_handle(), device=local)
     op = args.op
+    # cluster across GPUs: one layer, each rank its probe shard, forests all-gathered and joined (gsj.dist)
+    cl_shard = op == "cluster" and args.shard and ws > 1
     t0 = time.time()
     pts = None
     if op == "area":
@@ -310,7 +312,7 @@ def run_op(args, rank, local, ws):
         n = args.seeds or 20_000_000
         side = 2.0 * (n / 2e6) ** 0.5
         box = (-119.0, 33.0, -119.0 + side, 33.0 + side)
-        A = B = gen.layer_cfg5(n, box, seed=rank)
+        A = B = gen.layer_cfg5(n, box, seed=0 if cl_shard else rank)
         if op == "erode":
             workload = f"ST_Intersects(ST_Buffer(a,-1m), ST_Buffer(b,-1m)) self-join (self_pairs all), {n / 1e6:g}M parcels, ~30 vertices/ring"
             metric, unit = "join pairs/s (negative-buffer intersects self-join, ra = rb = 1 m)", "pairs/s"
@@ -332,6 +334,10 @@ def run_op(args, rank, local, ws):
         if op == "erode":   # self_pairs 'all': a parcel's pair with itself is kept when its eroded form is not empty
             p, st = eng.erode(LA, LA, 1.0, 1.0, same=True, refine_mode=mode)
             return len(p), st
+        if cl_shard:
+            from gsj import dist as gd
+            root, st = gd.cluster_sharded(eng, LA, refine_mode=mode)
+            return (len(root) if rank == 0 else 0), st   # the layer counted once
         root, st = eng.cluster(LA, refine_mode=mode)
         return len(root), st
 
@@ -377,6 +383,10 @@ def run_op(args, rank, local, ws):
             u = len(eng.points_dwithin(xp, xb, 5.0)[0])
         elif op == "erode":
             u = len(eng.erode(xa, xa, 1.0, 1.0, same=True)[0])
+        elif cl_shard:
+            from gsj import dist as gd
+            root_all = gd.cluster_sharded(eng, xa)[0]
+            u = len(root_all) if rank == 0 else 0   # the layer counted once
         else:
             u = len(eng.cluster(xa)[0])
         for x in {id(v): v for v in (xa, xb, xp) if v is not None}.values():
@@ -420,10 +430,11 @@ def run_op(args, rank, local, ws):
                "sample": f"CPU FP64 oracle (OpenMP) on {sample} ({dt:.1f} s)"}
     line = {
         "metric": metric, "value": value, "unit": unit, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": tot_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic (seeded Voronoi parcels / uniform points)",
+        "ms_per_step": tot_ms / args.steps, "higher_is_better": True, "scaling": "strong" if cl_shard else "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic (seeded Voronoi parcels / uniform points)",
         "config": {"workload": workload, "units_per_step": int(f["units"] / args.steps), "candidates": int(st[0]["candidates"]),
-                   "parallelism": f"replicas x{ws}", "gen_s": round(t_gen, 1)},
+                   "parallelism": (f"probe shards x{ws}, forests all-gathered and joined" if cl_shard else f"replicas x{ws}"),
+                   "gen_s": round(t_gen, 1)},
         "phases_ms": {k: float(np.mean([s_[k] for s_ in st])) for k in ("traverse_ms", "refine_ms", "compact_ms", "copy_ms")},
         "e2e": {"value": e2e_value, "unit": unit, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": int(8 * e2e_units / max(1, args.steps)),
                 "ms_per_step": e2e_tot / args.steps},

@@ -118,6 +118,11 @@ int gsj_join_points(gsj_ctx* ctx, const gsj_layer* pts, const gsj_layer* R, cons
  * parent's connected component in the intersects graph. */
 int gsj_cluster(gsj_ctx* ctx, const gsj_layer* P, uint32_t nparent, const gsj_join_opts* o, uint32_t* root,
                 gsj_join_stats* stats);
+/* Clustering across GPUs: each GPU runs gsj_cluster on the same layer with o->shard / o->nshards (its probe shard;
+ * every intersecting pair is found by exactly one shard), the root arrays are gathered, and this joins them:
+ * roots[nforests * nparent] (forest f at f * nparent) -> root[nparent], the smallest parent index of each parent's
+ * component in the union, i.e. gsj_cluster's answer for the whole layer. Runs on the context's GPU. */
+int gsj_cluster_merge(gsj_ctx* ctx, uint32_t nparent, uint32_t nforests, const uint32_t* roots, uint32_t* root);
 
 /* Host-side layer preparation (no device involved). Outputs are allocated by the library; free each with
  * gsj_host_free. Both return GSJ_OK or an error code.

@@ -9,6 +9,7 @@ void join_host(gsj_ctx* c, const gsj_layer* P, const gsj_layer* R, const gsj_ref
 void points_host(gsj_ctx* c, const gsj_layer* pts, const gsj_layer* R, const gsj_join_opts* op, gsj_points_sink sink, void* user,
                  gsj_join_stats* stp);
 void cluster_host(gsj_ctx* c, const gsj_layer* P, uint32_t nparent, const gsj_join_opts* op, uint32_t* root, gsj_join_stats* stp);
+void cluster_merge_host(gsj_ctx* c, uint32_t nparent, uint32_t nforests, const uint32_t* roots, uint32_t* out);
 void candidates_host(gsj_ctx* c, const gsj_layer* P, const gsj_layer* R, int upper, gsj_pairs_sink sink, void* user);
 void refine_pairs_host(gsj_ctx* c, const gsj_layer* P, const gsj_layer* R, const uint32_t* pairs, uint64_t np, const gsj_refine_params* rpp,
                        int mode, uint8_t* flag, double* area, double* ev, uint32_t* evb);
@@ -199,6 +200,10 @@ int gsj_join_points(gsj_ctx* c, const gsj_layer* pts, const gsj_layer* R, const 
 int gsj_cluster(gsj_ctx* c, const gsj_layer* P, uint32_t nparent, const gsj_join_opts* o, uint32_t* root, gsj_join_stats* st) {
   if (!c || !P || !root) return GSJ_ERR_ARG;
   return guard(c, [&] { gsj::cluster_host(c, P, nparent, o, root, st); });
+}
+int gsj_cluster_merge(gsj_ctx* c, uint32_t nparent, uint32_t nforests, const uint32_t* roots, uint32_t* root) {
+  if (!c || (nparent && (!root || (nforests && !roots)))) return GSJ_ERR_ARG;
+  return guard(c, [&] { gsj::cluster_merge_host(c, nparent, nforests, roots, root); });
 }
 
 int gsj_dwithin(gsj_ctx* c, const gsj_layer* P, const gsj_layer* R, double d, int same, const gsj_join_opts* o, gsj_pairs_sink sink, void* user,

@@ -420,6 +420,19 @@ __global__ void k_uf_flatten(uint32_t* par, uint32_t n) {   // concurrent reader
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) par[i] = uf_find(par, i);
 }
+// one forest of a probe shard's cluster (root[i] = smallest index of i's component there): joined into par
+__global__ void k_uf_union_roots(const uint32_t* __restrict__ root, uint32_t n, uint32_t* par) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  uint32_t a = i, b = root[i];
+  if (a == b) return;
+  for (;;) {
+    uint32_t ra = uf_find(par, a), rb = uf_find(par, b);
+    if (ra == rb) return;
+    if (ra > rb) { uint32_t t = ra; ra = rb; rb = t; }
+    if (atomicCAS(&par[rb], rb, ra) == rb) return;
+  }
+}
 __global__ void k_uf_roots(uint32_t* par, uint32_t n, uint32_t* root) {
   uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) root[i] = uf_find(par, i);
@@ -553,6 +566,28 @@ void cluster_host(gsj_ctx* c, const gsj_layer* P, uint32_t nparent, const gsj_jo
   st.launches = c->launches - l0;
   st.node_visits = c->node_visits - v0;
   if (stp) *stp = st;
+}
+
+// Components of the union of several forests (the clusters of the probe shards of one layer, computed by
+// cluster_host with shard / nshards on several GPUs and gathered): every i joined with its root in every forest.
+void cluster_merge_host(gsj_ctx* c, uint32_t nparent, uint32_t nforests, const uint32_t* roots, uint32_t* out) {
+  if (!nparent) return;
+  for (uint64_t k = 0; k < (uint64_t)nforests * nparent; k++)
+    if (roots[k] >= nparent) throw Error(GSJ_ERR_ARG, "a root index is out of range");
+  cudaStream_t s = c->stream;
+  uint32_t* par = c->uf.as<uint32_t>(2 * (size_t)nparent);
+  uint32_t* droot = par + nparent;
+  uint32_t* din = c->misc1.as<uint32_t>(nparent);
+  k_uf_init<<<grid_for(nparent, 256), 256, 0, s>>>(par, nparent); c->launches++;
+  for (uint32_t f = 0; f < nforests; f++) {
+    GSJ_CK(cudaMemcpyAsync(din, roots + (uint64_t)f * nparent, (size_t)nparent * 4, cudaMemcpyHostToDevice, s));
+    k_uf_union_roots<<<grid_for(nparent, 256), 256, 0, s>>>(din, nparent, par); c->launches++;
+    k_uf_flatten<<<grid_for(nparent, 256), 256, 0, s>>>(par, nparent); c->launches++;
+  }
+  k_uf_roots<<<grid_for(nparent, 256), 256, 0, s>>>(par, nparent, droot); c->launches++;
+  GSJ_CK(cudaGetLastError());
+  GSJ_CK(cudaMemcpyAsync(out, droot, (size_t)nparent * 4, cudaMemcpyDeviceToHost, s));
+  GSJ_CK(cudaStreamSynchronize(s));
 }
 
 // the intersects + area join with device-side results: pass 1 of the erosion join

@@ -91,6 +91,7 @@ SIGNATURES = {
     "gsj_join": (ctypes.c_int, [_vp, _vp, _vp, ctypes.POINTER(RefineParams), ctypes.POINTER(JoinOpts), JOIN_SINK, _vp, ctypes.POINTER(JoinStats)]),
     "gsj_join_points": (ctypes.c_int, [_vp, _vp, _vp, ctypes.POINTER(JoinOpts), POINTS_SINK, _vp, ctypes.POINTER(JoinStats)]),
     "gsj_cluster": (ctypes.c_int, [_vp, _vp, ctypes.c_uint32, ctypes.POINTER(JoinOpts), _vp, ctypes.POINTER(JoinStats)]),
+    "gsj_cluster_merge": (ctypes.c_int, [_vp, ctypes.c_uint32, ctypes.c_uint32, _vp, _vp]),
     "gsj_dwithin": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_double, ctypes.c_int, ctypes.POINTER(JoinOpts), PAIRS_SINK, _vp,
                                    ctypes.POINTER(JoinStats)]),
     "gsj_erode": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_double, ctypes.c_double, ctypes.c_int, _vp, ctypes.POINTER(JoinOpts), PAIRS_SINK,
@@ -353,13 +354,20 @@ class Engine:
         where = np.concatenate(cw) if cw else np.zeros(0, np.uint8)
         return pairs, where, st.as_dict()
 
-    def cluster(self, P: Layer, nparent: int | None = None, refine_mode=GSJ_REFINE_FILTERED):
+    def cluster(self, P: Layer, nparent: int | None = None, refine_mode=GSJ_REFINE_FILTERED, shard=0, nshards=1):
         nparent = P.info["nparent"] if nparent is None else nparent
         root = np.empty(nparent, np.uint32)
         st = JoinStats()
-        o = join_opts(refine_mode=refine_mode)
+        o = join_opts(refine_mode=refine_mode, shard=shard, nshards=nshards)
         self._check(lib().gsj_cluster(self.ctx, P.h, nparent, ctypes.byref(o), root.ctypes.data, ctypes.byref(st)))
         return root, st.as_dict()
+
+    def cluster_merge(self, roots) -> np.ndarray:
+        """Roots of the union of the given forests (probe-shard clusters of one layer): gsj_cluster_merge."""
+        r = np.ascontiguousarray(np.stack([np.asarray(x, np.uint32) for x in roots]), np.uint32)
+        out = np.empty(r.shape[1], np.uint32)
+        self._check(lib().gsj_cluster_merge(self.ctx, r.shape[1], r.shape[0], r.ctypes.data, out.ctypes.data))
+        return out
 
     def _pairs_call(self, fn, *args, opts=None):
         chunks = []

@@ -1,5 +1,6 @@
 """bench.py's multi-rank path on CPU: two gloo ranks on 127.0.0.1 (replicas; only the timing and counts are
-reduced), and the reference arm under torchrun (rank 0 prints the one JSON line, the others exit 0)."""
+reduced), the reference arm under torchrun (rank 0 prints the one JSON line, the others exit 0), and the exchange of
+the sharded cluster (each rank's forest gathered in rank order)."""
 import json
 import os
 import socket
@@ -52,3 +53,46 @@ def test_reference_arm_under_torchrun():
     d = json.loads(lines[0])
     assert d["impl"] == "reference" and d["n_gpus"] == 2 and d["value"] > 0 and d["cpu_baseline"]["kind"] == "port"
     assert d["e2e"]["h2d_bytes_per_step"] == 0 and d["higher_is_better"] is True
+
+
+def _forest(rank, port, out):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank), WORLD_SIZE="2", LOCAL_RANK=str(rank))
+    sys.path.insert(0, os.path.join(ROOT, "postgis-cuda_b200"))
+    import numpy as np
+    import torch.distributed as dist
+    from gsj import dist as gd
+    dist.init_process_group("gloo", rank=rank, world_size=2)
+    rng = np.random.default_rng(rank)
+    n = 1000
+    root = np.arange(n, dtype=np.uint32)   # a forest: each i points at a smaller index of its component (a root)
+    for i in rng.choice(n, 300, replace=False):
+        root[i] = rng.integers(0, i + 1)
+    for i in range(n):                     # flattened to component minima, as gsj_cluster returns them
+        root[i] = root[root[i]]
+    parts = gd.gather_forests(root)
+    np.save(os.path.join(out, f"f{rank}.npy"), np.stack(parts))
+    dist.destroy_process_group()
+
+
+def test_cluster_forests_gathered_in_rank_order(tmp_path):
+    """The one exchange of the sharded cluster on two gloo ranks: every rank receives every rank's forest, in rank
+    order; joining them (union-find restated here) gives the components of all the ranks' edges."""
+    import numpy as np
+    mp.start_processes(_forest, args=(free_port(), str(tmp_path)), nprocs=2, start_method="spawn")
+    a, b = np.load(tmp_path / "f0.npy"), np.load(tmp_path / "f1.npy")
+    assert np.array_equal(a, b) and a.shape == (2, 1000)
+    par = list(range(1000))
+
+    def find(x):
+        while par[x] != x:
+            par[x] = par[par[x]]
+            x = par[x]
+        return x
+    for forest in a:
+        for i, r in enumerate(forest):
+            x, y = find(i), find(int(r))
+            if x != y:
+                par[max(x, y)] = min(x, y)
+    merged = [find(i) for i in range(1000)]
+    assert all(merged[i] <= min(a[0][i], a[1][i]) for i in range(1000))   # joining can only lower a root
+    assert len(set(merged)) < min(len(set(a[0].tolist())), len(set(a[1].tolist())))

@@ -295,3 +295,17 @@ def test_probe_shards_partition_the_join(engine, layers, pieces, nshards):
     a, aw = srt(fp, fw)
     b, bw = srt(np.concatenate([x[0] for x in parts]), np.concatenate([x[1] for x in parts]))
     assert np.array_equal(a, b) and np.array_equal(aw, bw)
+
+
+@pytest.mark.parametrize("mode", MODES)
+def test_cluster_probe_shards_merge(engine, mode):
+    """Clustering across GPUs, on one: the clusters of 3 probe shards (each finds its own intersecting pairs) joined
+    by gsj_cluster_merge equal the single-pass roots, on a layer with components of every size and on its pieces."""
+    ps = shrunk_parcels(30000, (-118.3, 33.95, -118.15, 34.1), seed=12)
+    for layer, nparent in ((ps, ps.n), (gsj.subdivide(ps, 16), ps.n)):
+        L = engine.upload_polygons(layer)
+        whole, _ = engine.cluster(L, nparent, refine_mode=mode)
+        forests = [engine.cluster(L, nparent, refine_mode=mode, shard=k, nshards=3)[0] for k in range(3)]
+        assert not any(np.array_equal(f, whole) for f in forests)   # each shard alone misses connections
+        assert np.array_equal(engine.cluster_merge(forests), whole)
+        assert np.array_equal(whole, O.cluster(O.OSet(layer), nparent))
