@@ -71,8 +71,9 @@ typedef struct gsj_refine_params {
 } gsj_refine_params;
 void gsj_refine_params_default(gsj_refine_params* p);
 
-/* Refinement variants: GSJ_REFINE_PLAIN = FP64 everywhere (the reference's scheme); GSJ_REFINE_FILTERED = FP32
- * certified filters in front of the FP64 predicates plus size-binned scheduling. Same results bit for bit. */
+/* Refinement variants, the same results bit for bit: GSJ_REFINE_PLAIN = the reference's scheme (a warp per pair, every
+ * lane sweeping all of the other polygon's local edges in FP64); GSJ_REFINE_FILTERED = the same FP64 decisions
+ * reorganised around per-pair candidate edge-pair lists (only edge pairs whose boxes come within 2 tol are visited). */
 #define GSJ_REFINE_PLAIN 0
 #define GSJ_REFINE_FILTERED 1
 
@@ -124,8 +125,9 @@ int gsj_cluster(gsj_ctx* ctx, const gsj_layer* P, uint32_t nparent, const gsj_jo
  * component in the union, i.e. gsj_cluster's answer for the whole layer. Runs on the context's GPU. */
 int gsj_cluster_merge(gsj_ctx* ctx, uint32_t nparent, uint32_t nforests, const uint32_t* roots, uint32_t* root);
 
-/* Host-side layer preparation (no device involved). Outputs are allocated by the library; free each with
- * gsj_host_free. Both return GSJ_OK or an error code.
+/* Layer preparation. Outputs are host arrays allocated by the library; free each with gsj_host_free. Both run on the
+ * calling thread's current CUDA device (a context is made for the call; gsj_subdivide_gpu / gsj_dedup_gpu below take
+ * one) and return GSJ_OK or an error code.
  * Subdivision (engine/subdivide.h:71-129): geometries with more than maxv vertices are cut recursively at the middle
  * of their bbox's longer side (Sutherland-Hodgman, FP64); parent[piece] = geometry, syn[v] = 1 for edges created
  * by a cut (ignored for boundary contact). Feed the result to gsj_layer_upload_polygons with parent and syn. */
@@ -139,13 +141,12 @@ int gsj_dedup(uint64_t n, uint64_t nr, uint64_t nv, const uint64_t* gro, const u
               uint64_t* out_n, uint64_t* out_nr, uint64_t* out_nv, uint64_t** out_gro, uint64_t** out_rvo, double** out_xy,
               uint64_t** out_moff, uint32_t** out_midx);
 void gsj_host_free(void* p);
-/* gsj_dedup computed on the context's GPU (hash, radix sort, exact comparison within equal-hash runs, gathers):
- * the same output arrays, bit for bit; the host arrays are copied to the device and the results back. */
+/* gsj_dedup on the context's GPU (hash, radix sort, exact comparison within equal-hash runs, gathers); the host
+ * arrays are copied to the device and the results back. */
 int gsj_dedup_gpu(gsj_ctx* ctx, uint64_t n, uint64_t nr, uint64_t nv, const uint64_t* gro, const uint64_t* rvo, const double* xy, int morton,
                   uint64_t* out_n, uint64_t* out_nr, uint64_t* out_nv, uint64_t** out_gro, uint64_t** out_rvo, double** out_xy,
                   uint64_t** out_moff, uint32_t** out_midx);
-/* gsj_subdivide computed on the context's GPU (breadth-first cut rounds, pieces sorted by geometry and cut path):
- * the same output arrays, bit for bit. */
+/* gsj_subdivide on the context's GPU (breadth-first cut rounds, pieces sorted by geometry and cut path). */
 int gsj_subdivide_gpu(gsj_ctx* ctx, uint64_t n, uint64_t nr, uint64_t nv, const uint64_t* gro, const uint64_t* rvo, const double* xy, int maxv,
                       uint64_t* out_n, uint64_t* out_nr, uint64_t* out_nv, uint64_t** out_gro, uint64_t** out_rvo, double** out_xy,
                       uint32_t** out_parent, uint8_t** out_syn);
@@ -183,7 +184,8 @@ int gsj_refine_pairs(gsj_ctx* ctx, const gsj_layer* P, const gsj_layer* R, const
  * every GPU that loads the library, until exit); layers whose largest geometry needs a larger per-warp slab
  * (more than ~466k edges) are rejected with GSJ_ERR_ARG. All calls share that array: calls that overlap on the GPU
  * race and must be serialised. The first call on a device looks up the array's address; make it before any
- * stream capture. Runs on the context's stream and returns after it finished. */
+ * stream capture. The address is kept until the process exits: do not call this on a device after resetting it
+ * (cudaDeviceReset). Runs on the context's stream and returns after it finished. */
 #define GSJ_NOALLOC_SCRATCH_BYTES (32u << 20)
 int gsj_refine_pairs_noalloc(gsj_ctx* ctx, const gsj_layer* P, const gsj_layer* R, const uint32_t* d_pairs, uint64_t np,
                              const gsj_refine_params* rp, uint8_t* d_flag, double* d_area, double* d_ev, uint32_t* d_evb);

@@ -73,6 +73,15 @@ int64_t orc_pt_erode(const double* pts, uint64_t npts, const orc_set* R, double 
 int64_t orc_erode(const orc_set* P, const orc_set* R, double ra, double rb, int same, const uint8_t* need_self, int nthreads,
                   uint32_t** out_pairs);
 
+/* Layer preparation restated on the CPU (oracle_prep.cpp). Subdivision (engine/subdivide.h:14-129): pieces of at most
+ * ~maxv vertices, parent[piece] = geometry, syn[v] = 1 for an edge on a cut line; returns the piece count.
+ * Deduplication (engine/dedup.h:22-124): distinct geometries in order of first occurrence (morton: Z-order of their
+ * bbox centres), members midx[moff[d] .. moff[d+1]); returns the distinct count. Arrays freed with orc_free. */
+int64_t orc_subdivide(uint64_t n, const uint64_t* gro, const uint64_t* rvo, const double* xy, int maxv, uint64_t** out_gro, uint64_t** out_rvo,
+                      double** out_xy, uint32_t** out_parent, uint8_t** out_syn, uint64_t* out_nr, uint64_t* out_nv);
+int64_t orc_dedup(uint64_t n, const uint64_t* gro, const uint64_t* rvo, const double* xy, int morton, uint64_t** out_gro, uint64_t** out_rvo,
+                  double** out_xy, uint64_t** out_moff, uint32_t** out_midx, uint64_t* out_nr, uint64_t* out_nv);
+
 void orc_free(void* p);
 
 #ifdef __cplusplus

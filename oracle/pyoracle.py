@@ -72,6 +72,13 @@ def lib():
         if hasattr(L, "orc_erode"):
             L.orc_erode.restype = ctypes.c_int64
             L.orc_erode.argtypes = [vp, vp, ctypes.c_double, ctypes.c_double, ctypes.c_int, vp, ctypes.c_int, ctypes.POINTER(u32p)]
+        u64pp = ctypes.POINTER(ctypes.POINTER(ctypes.c_uint64))
+        L.orc_subdivide.restype = ctypes.c_int64
+        L.orc_subdivide.argtypes = [ctypes.c_uint64, vp, vp, vp, ctypes.c_int, u64pp, u64pp, ctypes.POINTER(f64p), ctypes.POINTER(u32p),
+                                    ctypes.POINTER(u8p), ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64)]
+        L.orc_dedup.restype = ctypes.c_int64
+        L.orc_dedup.argtypes = [ctypes.c_uint64, vp, vp, vp, ctypes.c_int, u64pp, u64pp, ctypes.POINTER(f64p), u64pp, ctypes.POINTER(u32p),
+                                ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64)]
         L.orc_free.argtypes = [vp]
         _lib = L
     return _lib
@@ -184,6 +191,36 @@ def erode(P: OSet, R: OSet, ra: float, rb: float, same=False, need_self=None, nt
     ns = None if need_self is None else np.ascontiguousarray(need_self, dtype=np.uint8)
     n = lib().orc_erode(P.h, R.h, ra, rb, int(same), None if ns is None else ns.ctypes.data, nthreads, ctypes.byref(op))
     return _take(op, 2 * n, np.uint32, (n, 2))
+
+
+def _host_set(ps):
+    return (np.ascontiguousarray(ps.gro, np.uint64), np.ascontiguousarray(ps.rvo, np.uint64), np.ascontiguousarray(ps.xy, np.float64))
+
+
+def subdivide(ps, maxv: int):
+    """Pieces of at most ~maxv vertices (a PolygonSet-like object with .parent and .syn), restated on the CPU."""
+    from gsj.gen import PolygonSet
+    gro, rvo, xy = _host_set(ps)
+    u64 = ctypes.POINTER(ctypes.c_uint64)
+    og, orv, oxy, opar, osyn = u64(), u64(), f64p(), u32p(), u8p()
+    nr, nv = ctypes.c_uint64(), ctypes.c_uint64()
+    n = lib().orc_subdivide(len(gro) - 1, gro.ctypes.data, rvo.ctypes.data, xy.ctypes.data, int(maxv), ctypes.byref(og), ctypes.byref(orv),
+                            ctypes.byref(oxy), ctypes.byref(opar), ctypes.byref(osyn), ctypes.byref(nr), ctypes.byref(nv))
+    return PolygonSet(_take(og, n + 1, np.uint64), _take(orv, nr.value + 1, np.uint64), _take(oxy, 2 * nv.value, np.float64, (nv.value, 2)),
+                      parent=_take(opar, n, np.uint32), syn=_take(osyn, nv.value, np.uint8))
+
+
+def dedup(ps, morton=False):
+    """(distinct PolygonSet, moff, midx), restated on the CPU."""
+    from gsj.gen import PolygonSet
+    gro, rvo, xy = _host_set(ps)
+    u64 = ctypes.POINTER(ctypes.c_uint64)
+    og, orv, oxy, omo, omi = u64(), u64(), f64p(), u64(), u32p()
+    nr, nv = ctypes.c_uint64(), ctypes.c_uint64()
+    n = lib().orc_dedup(len(gro) - 1, gro.ctypes.data, rvo.ctypes.data, xy.ctypes.data, int(morton), ctypes.byref(og), ctypes.byref(orv),
+                        ctypes.byref(oxy), ctypes.byref(omo), ctypes.byref(omi), ctypes.byref(nr), ctypes.byref(nv))
+    u = PolygonSet(_take(og, n + 1, np.uint64), _take(orv, nr.value + 1, np.uint64), _take(oxy, 2 * nv.value, np.float64, (nv.value, 2)))
+    return u, _take(omo, n + 1, np.uint64), _take(omi, len(gro) - 1, np.uint32)
 
 
 def de9im_str(code: int) -> str:

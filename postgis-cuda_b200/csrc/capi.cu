@@ -1,5 +1,7 @@
 // The C ABI (include/gsj.h): status codes instead of exits, exceptions stop here.
+#include <cstdlib>
 #include <cstring>
+#include <functional>
 #include "engine.h"
 
 namespace gsj {
@@ -123,6 +125,35 @@ int gsj_subdivide_gpu(gsj_ctx* c, uint64_t n, uint64_t nr, uint64_t nv, const ui
   if (!c) return GSJ_ERR_ARG;
   return guard(c, [&] { gsj::subdivide_gpu(c, n, nr, nv, gro, rvo, xy, maxv, out_n, out_nr, out_nv, out_gro, out_rvo, out_xy, out_parent, out_syn); });
 }
+
+// The context-free forms run on the calling thread's current CUDA device, with a context made for the call.
+static int on_current_device(const std::function<int(gsj_ctx*)>& fn) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) { (void)cudaGetLastError(); return GSJ_ERR_CUDA; }
+  gsj_ctx* c = nullptr;
+  const int rc = ctx_create(dev, 0, &c);
+  if (rc) return rc;
+  const int r = fn(c);
+  gsj_ctx_destroy(c);
+  return r;
+}
+
+int gsj_subdivide(uint64_t n, uint64_t nr, uint64_t nv, const uint64_t* gro, const uint64_t* rvo, const double* xy, int maxv, uint64_t* out_n,
+                  uint64_t* out_nr, uint64_t* out_nv, uint64_t** out_gro, uint64_t** out_rvo, double** out_xy, uint32_t** out_parent,
+                  uint8_t** out_syn) {
+  return on_current_device([&](gsj_ctx* c) {
+    return gsj_subdivide_gpu(c, n, nr, nv, gro, rvo, xy, maxv, out_n, out_nr, out_nv, out_gro, out_rvo, out_xy, out_parent, out_syn);
+  });
+}
+
+int gsj_dedup(uint64_t n, uint64_t nr, uint64_t nv, const uint64_t* gro, const uint64_t* rvo, const double* xy, int morton, uint64_t* out_n,
+              uint64_t* out_nr, uint64_t* out_nv, uint64_t** out_gro, uint64_t** out_rvo, double** out_xy, uint64_t** out_moff, uint32_t** out_midx) {
+  return on_current_device([&](gsj_ctx* c) {
+    return gsj_dedup_gpu(c, n, nr, nv, gro, rvo, xy, morton, out_n, out_nr, out_nv, out_gro, out_rvo, out_xy, out_moff, out_midx);
+  });
+}
+
+void gsj_host_free(void* p) { free(p); }
 
 int gsj_ctx_mem_info(gsj_ctx* c, uint64_t* fr, uint64_t* tot, int* sms) {
   if (!c) return GSJ_ERR_ARG;

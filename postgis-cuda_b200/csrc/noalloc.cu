@@ -11,7 +11,9 @@
 // geometry edge count rounded up to 8; calls whose one-warp slab does not fit are rejected with GSJ_ERR_ARG.
 // Every call on a device uses the same array: calls that overlap on the GPU (other streams, other contexts on
 // the device, other host threads) race on it and must be serialised by the caller. The first call on a device
-// looks the array's device address up (cudaGetSymbolAddress); make that first call before any stream capture.
+// looks the array's device address up (cudaGetSymbolAddress); make that first call before any stream capture. The
+// address is kept for the life of the process: a host application that resets a device (cudaDeviceReset) must not
+// call this entry point on that device afterwards.
 #include <mutex>
 #include "engine.h"
 
@@ -43,7 +45,12 @@ __global__ void __launch_bounds__(32) k_refine_static(DLayer P, DLayer R, const 
   for (uint64_t p = blockIdx.x; p < np; p += gridDim.x) {
     const uint2 pr = pairs[p];
     if (pr.x >= P.n || pr.y >= R.n) {   // a caller's index out of range: record it, skip the pair
-      if (lane == 0) { atomicExch(err, 2); flag[p] = 0; }
+      if (lane == 0) {
+        atomicExch(err, 2);
+        flag[p] = 0;
+        if (area) area[p] = 0.0;
+        if (ev) { ev[p] = make_double4(0, 0, 0, 0); evb[p] = 0u; }
+      }
       continue;
     }
     uint8_t f; double ar; double4 e4; uint32_t b4;

@@ -164,7 +164,7 @@ def _take(ptr, count, dtype):
 
 
 def subdivide(ps, maxv: int):
-    """Pieces of at most ~maxv vertices (gsj_subdivide): a PolygonSet with .parent and .syn set."""
+    """Pieces of at most ~maxv vertices (gsj_subdivide, on the current CUDA device): a PolygonSet with .parent and .syn set."""
     from .gen import PolygonSet
     gro = np.ascontiguousarray(ps.gro, np.uint64); rvo = np.ascontiguousarray(ps.rvo, np.uint64); xy = np.ascontiguousarray(ps.xy, np.float64)
     n, nr, nv = ctypes.c_uint64(), ctypes.c_uint64(), ctypes.c_uint64()
@@ -179,7 +179,7 @@ def subdivide(ps, maxv: int):
 
 
 def dedup(ps, morton=False):
-    """(distinct PolygonSet, moff, midx) (gsj_dedup)."""
+    """(distinct PolygonSet, moff, midx) (gsj_dedup, on the current CUDA device)."""
     from .gen import PolygonSet
     gro = np.ascontiguousarray(ps.gro, np.uint64); rvo = np.ascontiguousarray(ps.rvo, np.uint64); xy = np.ascontiguousarray(ps.xy, np.float64)
     n, nr, nv = ctypes.c_uint64(), ctypes.c_uint64(), ctypes.c_uint64()
@@ -245,6 +245,7 @@ class Engine:
         if rc:
             raise GsjError(rc, "cannot create a context (no CUDA device?)")
         self.ctx = h
+        self.device = device
 
     def close(self):
         if self.ctx:

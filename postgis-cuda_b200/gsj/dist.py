@@ -9,12 +9,16 @@ from __future__ import annotations
 import numpy as np
 
 
-def gather_forests(root: np.ndarray) -> list[np.ndarray]:
-    """Every rank's root array, in rank order (all-gather over the default process group)."""
+def gather_forests(root: np.ndarray, device: int | None = None) -> list[np.ndarray]:
+    """Every rank's root array, in rank order (all-gather over the default process group). With NCCL the exchange
+    runs on CUDA device ``device`` (default: the current one), which must be this rank's GPU."""
     import torch
     import torch.distributed as dist
     ws = dist.get_world_size()
-    dev = torch.device("cuda", torch.cuda.current_device()) if dist.get_backend() == "nccl" else torch.device("cpu")
+    if dist.get_backend() == "nccl":
+        dev = torch.device("cuda", torch.cuda.current_device() if device is None else device)
+    else:
+        dev = torch.device("cpu")
     t = torch.from_numpy(root.astype(np.int64, copy=False)).to(dev)
     parts = [torch.empty_like(t) for _ in range(ws)]
     dist.all_gather(parts, t)
@@ -26,4 +30,4 @@ def cluster_sharded(engine, layer, nparent: int | None = None, refine_mode=1):
     import torch.distributed as dist
     rank, ws = dist.get_rank(), dist.get_world_size()
     root, st = engine.cluster(layer, nparent, refine_mode=refine_mode, shard=rank, nshards=ws)
-    return engine.cluster_merge(gather_forests(root)), st
+    return engine.cluster_merge(gather_forests(root, engine.device)), st

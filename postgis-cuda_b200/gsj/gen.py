@@ -141,3 +141,19 @@ def layer_parcels(n, box, seed=0) -> PolygonSet:
     """Jittered-grid parcels, 4-256 vertices per ring (log-uniform), 5% MultiPolygons (2-4 parts), 2% holes."""
     return voronoi(n, box, seed, jitter_grid=True, jitter=0.4, vmin=4, vmax=256, log_uniform=True,
                    mp_frac=0.05, mp_parts=(2, 4), hole_frac=0.02)
+
+
+def shrunk(ps: PolygonSet, seed: int, frac=0.55, f=0.9) -> PolygonSet:
+    """A seeded fraction ``frac`` of the geometries shrunk by ``f`` toward their bbox centre. Only neighbours that both
+    keep their size touch, so the intersects graph of a tiling falls into components of every size (site
+    percolation): the clustering workload with many components."""
+    shrink = np.random.default_rng(seed).random(ps.n) < frac
+    v0 = ps.rvo[ps.gro[:-1]].astype(np.int64)
+    cnt = np.diff(np.append(v0, ps.nv))
+    lo = np.minimum.reduceat(ps.xy, v0, axis=0)
+    hi = np.maximum.reduceat(ps.xy, v0, axis=0)
+    c = np.repeat(0.5 * (lo + hi), cnt, axis=0)
+    m = np.repeat(shrink, cnt)
+    xy = ps.xy.copy()
+    xy[m] = c[m] + f * (xy[m] - c[m])
+    return PolygonSet(ps.gro, ps.rvo, xy)

@@ -94,5 +94,25 @@ def test_cluster_forests_gathered_in_rank_order(tmp_path):
             if x != y:
                 par[max(x, y)] = min(x, y)
     merged = [find(i) for i in range(1000)]
-    assert all(merged[i] <= min(a[0][i], a[1][i]) for i in range(1000))   # joining can only lower a root
+    # independently: connected components of the edges (i, root_f[i]) of both forests by breadth-first search,
+    # labelled by their smallest member
+    adj = [[] for _ in range(1000)]
+    for forest in a:
+        for i, r in enumerate(forest):
+            adj[i].append(int(r)); adj[int(r)].append(i)
+    comp = [-1] * 1000
+    for s in range(1000):
+        if comp[s] < 0:
+            todo, members = [s], []
+            comp[s] = s
+            while todo:
+                x = todo.pop()
+                members.append(x)
+                for y in adj[x]:
+                    if comp[y] < 0:
+                        comp[y] = s; todo.append(y)
+            m = min(members)
+            for x in members:
+                comp[x] = m
+    assert merged == comp
     assert len(set(merged)) < min(len(set(a[0].tolist())), len(set(a[1].tolist())))

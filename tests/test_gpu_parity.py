@@ -118,20 +118,8 @@ def test_cluster(engine, layers):
 
 
 def shrunk_parcels(n, box, seed, frac=0.55, f=0.9):
-    """Parcels with a seeded fraction shrunk by f toward their bbox centre. Only neighbours that both keep their
-    size touch, so the intersects graph falls into components of every size (site percolation)."""
-    ps = gen.layer_parcels(n, box, seed=seed)
-    shrink = np.random.default_rng(seed).random(ps.n) < frac
-    ring_g = np.repeat(np.arange(ps.n), np.diff(ps.gro).astype(np.int64))
-    vg = ring_g[np.repeat(np.arange(len(ps.rvo) - 1), np.diff(ps.rvo).astype(np.int64))]
-    lo, hi = np.full((ps.n, 2), np.inf), np.full((ps.n, 2), -np.inf)
-    np.minimum.at(lo, vg, ps.xy)
-    np.maximum.at(hi, vg, ps.xy)
-    c = 0.5 * (lo + hi)
-    m = shrink[vg]
-    xy = ps.xy.copy()
-    xy[m] = c[vg[m]] + f * (xy[m] - c[vg[m]])
-    return gen.PolygonSet(ps.gro, ps.rvo, xy)
+    """Parcels with a seeded fraction shrunk toward their bbox centre: components of every size."""
+    return gen.shrunk(gen.layer_parcels(n, box, seed=seed), seed, frac, f)
 
 
 @pytest.mark.parametrize("mode", MODES)
@@ -193,13 +181,13 @@ def test_subdivided_points_cluster_dwithin(engine, pieces):
 
 
 @pytest.mark.parametrize("morton", [False, True])
-def test_dedup_gpu_matches_host(engine, morton):
-    """gsj_dedup_gpu gives the host routine's arrays bit for bit: distinct set, member offsets and indices."""
+def test_dedup_gpu_matches_oracle(engine, morton):
+    """gsj_dedup_gpu gives the oracle's arrays bit for bit: distinct set, member offsets and indices."""
     import test_gpu_daemon as TD
     base = gen.layer_parcels(30000, (-118.3, 33.95, -118.2, 34.05), seed=4)
     rng = np.random.default_rng(5)
     ps = TD.with_duplicates(base, rng.choice(base.n, 3000, replace=True))   # groups of 2+ copies, some repeated
-    hu, hmo, hmi = gsj.dedup(ps, morton=morton)
+    hu, hmo, hmi = O.dedup(ps, morton=morton)
     gu, gmo, gmi = engine.dedup(ps, morton=morton)
     assert np.array_equal(hmo, gmo) and np.array_equal(hmi, gmi)
     assert np.array_equal(hu.gro, gu.gro) and np.array_equal(hu.rvo, gu.rvo) and np.array_equal(hu.xy.view(np.uint64), gu.xy.view(np.uint64))
@@ -265,12 +253,12 @@ def test_empty_and_tiny_layers(engine):
 
 
 @pytest.mark.parametrize("maxv", [12, 24, 64])
-def test_subdivide_gpu_matches_host(engine, maxv):
-    """gsj_subdivide_gpu gives the host routine's pieces bit for bit: order, rings, vertices, cut flags, parents."""
+def test_subdivide_gpu_matches_oracle(engine, maxv):
+    """gsj_subdivide_gpu gives the oracle's pieces bit for bit: order, rings, vertices, cut flags, parents."""
     layers = [gen.layer_parcels(20000, (-118.3, 33.95, -118.2, 34.05), seed=5), gen.voronoi(50, gen.LA_BOX, 1, vmin=40, vmax=80),
               shapes.make_set(degenerate_geometries())]
     for ps in layers:
-        h = gsj.subdivide(ps, maxv)
+        h = O.subdivide(ps, maxv)
         g = engine.subdivide(ps, maxv)
         assert g.n == h.n and np.array_equal(g.gro, h.gro) and np.array_equal(g.rvo, h.rvo)
         assert np.array_equal(g.xy.view(np.uint64), h.xy.view(np.uint64))

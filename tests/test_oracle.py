@@ -117,12 +117,12 @@ def test_golden_dwithin(golden_layers):
 
 @pytest.fixture(scope="module")
 def sub32(golden_layers):
-    import gsj
-    return gsj.subdivide(golden_layers["parcels"], 32)
+    return O.subdivide(golden_layers["parcels"], 32)
 
 
 def test_subdivision_matches_reference_pieces(golden_layers, sub32):
-    """Pieces from gsj_subdivide give the reference engine's subdivided results (same cut points, cut flags)."""
+    """The oracle's pieces give the reference engine's subdivided results (same cut points, cut flags); the GPU
+    subdivision is checked against these pieces bit for bit in the GPU tests."""
     assert sub32.n == 11203 and int(sub32.parent.max()) == golden_layers["parcels"].n - 1
     S = O.OSet(sub32)
     p, a, c, _ = O.join(S, S, O.params(1, 0), upper=True)
@@ -165,9 +165,9 @@ def test_dedup_members():
             xy.append(v); rvo.append(rvo[-1] + len(v))
         gro.append(len(rvo) - 1)
     dup = gen.PolygonSet(np.array(gro, np.uint64), np.array(rvo, np.uint64), np.concatenate(xy))
-    u, moff, midx = gsj.dedup(dup)
+    u, moff, midx = O.dedup(dup)
     assert u.n == ps.n and list(midx[moff[5]:moff[6]]) == [5, 300, 302] and list(midx[moff[7]:moff[8]]) == [7, 301]
-    um, moffm, midxm = gsj.dedup(dup, morton=True)
+    um, moffm, midxm = O.dedup(dup, morton=True)
     assert um.n == ps.n and sorted(np.diff(moffm).tolist()) == sorted(np.diff(moff).tolist())
 
 
@@ -204,8 +204,8 @@ def test_golden_two_layer_cases(golden_layers):
     check_pairs("pq_relate", p, c, "relate")
     for case, ra, rb in (("pq_erode1", 1.0, 1.0), ("pq_erode1_3", 1.0, 3.0), ("pq_erode5", 5.0, 5.0)):
         assert rowset(O.erode(P, Q, ra, rb)) == rowset(np.load(f"{MG.HERE}/{case}.npz")["pairs"]), case
-    SP = O.OSet(gsj.subdivide(golden_layers["parcels"], 32))
-    SQ = O.OSet(gsj.subdivide(golden_layers["parcels2"], 32))
+    SP = O.OSet(O.subdivide(golden_layers["parcels"], 32))
+    SQ = O.OSet(O.subdivide(golden_layers["parcels2"], 32))
     assert rowset(O.erode(SP, SQ, 1.0, 1.0)) == rowset(np.load(f"{MG.HERE}/pq_erode1_sub32.npz")["pairs"])
     p, _ = O.dwithin(P, Q, 5.0)
     assert rowset(p) == rowset(np.load(f"{MG.HERE}/pq_dwithin5.npz")["pairs"])
