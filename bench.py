@@ -15,10 +15,16 @@ erode = ST_Intersects(ST_Buffer(a, -1 m), ST_Buffer(b, -1 m)) self-join and clus
 on a parcel layer with ~30 vertices per ring (20M parcels by default; --seeds to change).
 
 A step is one full self-join of the resident layer. value = intersecting pairs / device time (CUDA events on the
-engine's stream). e2e = the same join through the C ABI from pinned host buffers: upload (H2D) + LBVH build +
-join + result D2H, every step. N > 1 (torchrun): every rank joins its own 2M-parcel layer (seed = rank), no
-data-path collective; value = all ranks' pairs / max-over-ranks time (weak scaling). --impl reference times the
-CPU FP64 restatement of the same predicates on the host cores (the reference engine has no CPU path).
+engine's stream; the rows reach pinned host buffers every step). e2e = the same join through the C ABI from pinned
+host buffers: upload (H2D) + LBVH build + join + result D2H, every step. N > 1 (torchrun): every rank joins its own
+2M-parcel layer (seed = rank), no data-path collective; value = all ranks' pairs / max-over-ranks time (weak
+scaling). After the timed steps the filtered and the plain variant's rows are compared with each other and, row by
+row, with the reference engine's own driver run on the same layer (pair_diffs_vs_reference, code_diffs_vs_reference).
+
+--impl reference runs the reference engine itself (landstats-us/postgis-cuda engine/harness.cu, unmodified, built
+for sm_100a into oracle/_ref/harness) on the same seeded layer on this GPU: value = its intersecting pairs / its GPU
+phase time (traverse + refine + compact, its own stats) of the last of warmup + steps repetitions; e2e = the same
+pairs / its upload + BVH + join + D2H time. The CPU FP64 oracle stays the cpu_baseline of this arm's line.
 """
 from __future__ import annotations
 
@@ -38,7 +44,12 @@ sys.path.insert(0, os.path.join(ROOT, "postgis-cuda_b200"))
 
 BOX = (-119.0, 33.0, -117.0, 35.0)
 N_SEEDS = 2_000_000
-METRIC = "join pairs/s (DE-9IM relate self-join, filtered+batched FP64)"
+METRIC = "join pairs/s (DE-9IM relate self-join, filtered FP64 refinement)"
+# B200 FP64 (non-tensor) peak per GPU from NVIDIA's HGX B200 specification (296 TFLOPS for 8 GPUs); no measured copy
+FP64_PEAK_TFLOPS = 37.0
+# algorithmic FP64 work of the reference's refinement per local edge pair (i, j): the contact test's 4 orientations
+# x 10 flops, plus ~30 flops of the Green's-theorem / relate pass (edge_contrib_loc, engine.cuh:416-515)
+FLOPS_PER_EDGE_PAIR = 70.0
 WORKLOAD = "relate self-join, 2M jittered-grid Voronoi parcels, 2x2 deg, 4-256 vertices/ring, 5% multipolygons, 2% holes"
 
 
@@ -458,25 +469,74 @@ def run_op(args, rank, local, ws):
         print(json.dumps(line), flush=True)
 
 
+def reference_check(ps, filt, tmpdir):
+    """Row-by-row comparison with the reference engine's own driver on the same layer (checker, untimed)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import refharness as RH
+    from gsj import gen
+    if not RH.available():
+        return {"available": False, "why": "oracle/_ref/harness is not built"}
+    g = os.path.join(tmpdir, "parcels.gset")
+    gen.write_gset(g, ps)
+    out = os.path.join(tmpdir, "reference_rows.csv")
+    t = time.time()
+    r = RH.run([g, g, "--relate"], reps=1, out_csv=out)
+    rows, codes = RH.read_pairs_csv(out)
+    os.remove(out)
+    want_p, want_c = RH.upper_rows(rows, codes)
+    got_p, got_c = RH.sorted_rows(filt.pairs, filt.code)
+    same = got_p.shape == want_p.shape and np.array_equal(got_p, want_p)
+    if same:
+        pair_diffs, code_diffs = 0, int((got_c != want_c).sum())
+    else:
+        a, b = set(map(tuple, got_p.tolist())), set(map(tuple, want_p.tolist()))
+        pair_diffs, code_diffs = len(a ^ b), None
+    return {"available": True, "pair_diffs": pair_diffs, "code_diffs": code_diffs, "reference_rows": int(len(rows)),
+            "reference_pairs": int(len(want_p)), "reference_phases_ms": r["ms"], "seconds": round(time.time() - t, 1)}
+
+
 def run_reference(args, rank, ws):
-    """--impl reference: the CPU FP64 port of the reference's predicates, timed on the host cores."""
+    """--impl reference: the reference engine's own driver (unmodified, sm_100a) on the same seeded layer and GPU."""
+    import shutil
+    import tempfile
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import refharness as RH
     from gsj import gen
     if rank != 0:
         return
+    if not RH.available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/harness (the reference engine's driver) is not built"}), flush=True)
+        return
     ps = gen.layer_parcels(args.seeds, BOX, seed=0)
-    target = args.cpu_sample_s or max(4.0, min(15.0, 90.0 / max(1, args.steps + args.warmup)))
-    S, sub, w = cpu_sample(ps, target_s=target)
-    runs = [cpu_time(S) for _ in range(args.warmup + args.steps)][args.warmup:]
-    n = runs[0][0]
-    secs = float(np.sum([r[1] for r in runs]))
-    value = n * len(runs) / secs
+    d = tempfile.mkdtemp(prefix="gsj_ref_")
+    try:
+        g = os.path.join(d, "parcels.gset")
+        gen.write_gset(g, ps)
+        reps = args.warmup + args.steps
+        with Clocks(0) as clk:
+            r = RH.run([g, g, "--relate"], reps=reps)
+    finally:
+        shutil.rmtree(d, ignore_errors=True)
+    ms = RH.gpu_ms(r)
+    pairs = r["count"]["gpu_hits"]
+    value = pairs / (ms / 1000.0)
+    e2e_ms = r["ms"]["upload"] + r["ms"]["bvh"] + ms + r["ms"].get("d2h", 0.0)
+    h2d = int(ps.gro.nbytes + ps.rvo.nbytes + ps.xy.nbytes)
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "pairs/s", "n_gpus": args.gpus, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": 1000.0 * secs / len(runs), "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded Voronoi parcels)",
-            "config": {"workload": WORKLOAD, "sample": f"{sub.n} parcels in a {w:.3f} deg corner sub-box of the layer"},
-            "cpu_baseline": {"value": value, "unit": "pairs/s", "cores": os.cpu_count(), "kind": "port",
-                             "sample": f"CPU FP64 oracle (OpenMP), relate self-join of {sub.n} parcels ({n} pairs) per step"},
-            "e2e": {"value": value, "unit": "pairs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded Voronoi parcels; the reference's parcel datasets are private)",
+            "config": {"workload": WORKLOAD, "parcels": int(ps.n), "vertices": int(ps.nv), "candidates": int(r["count"]["cand"]),
+                       "pairs_per_step": int(pairs), "parallelism": "replicas x1 (own layer per rank)", "l2": "inputs > L2 (2.2 GB resident layer)"},
+            "reference_engine": {"driver": "landstats-us/postgis-cuda engine/harness.cu, unmodified, nvcc -arch=sm_100a",
+                                 "command": "harness parcels.gset parcels.gset --relate --reps %d" % reps,
+                                 "phases_ms": r["ms"], "counts": r["count"],
+                                 "timing": "the driver's own stats of its last repetition: GPU phases traverse + refine + compact"},
+            "e2e": {"value": pairs / (e2e_ms / 1000.0), "unit": "pairs/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": int(pairs * 12),
+                    "ms_per_step": e2e_ms, "what": "upload (host prep + H2D) + BVH + join + D2H, the driver's own timers"},
+            "cpu_baseline": {"value": value, "unit": "pairs/s", "cores": os.cpu_count(), "kind": "reference",
+                             "sample": f"the reference engine's driver on this box's GPU (host threads for its prep: {os.cpu_count()}); "
+                                       f"relate self-join of {ps.n} parcels, last of {reps} repetitions"},
+            "clocks": clk.summary()}
     print(json.dumps(line), flush=True)
 
 
@@ -490,6 +550,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-sample-s", type=float, default=0.0, help="CPU seconds per reference-arm step (0: sized from --steps)")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving-latency leg (gsjd under a Poisson request stream)")
+    ap.add_argument("--no-reference-check", action="store_true", help="skip the row-by-row comparison with the reference engine's driver")
     ap.add_argument("--op", default="relate", choices=["relate", "area", "dwithin", "erode", "cluster"])
     ap.add_argument("--arms", default="filtered,plain", help="refinement variants an --op run times (filtered first; for profiling one)")
     ap.add_argument("--shard", action="store_true",
@@ -529,7 +590,7 @@ def main():
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         with torch.cuda.stream(ext):
             e0.record()
-        r = eng.join(L, L, want_area=False, want_relate=True, upper=True, refine_mode=mode, **shard)
+        r = eng.join(L, L, want_area=False, want_relate=True, upper=True, refine_mode=mode, collect=False, **shard)
         with torch.cuda.stream(ext):
             e1.record()
         e1.synchronize()
@@ -547,16 +608,27 @@ def main():
         with Clocks(local) as clk:
             for _ in range(args.steps):
                 r, t = timed_join(mode)
-                ms.append(t); pairs += len(r.pairs); stats.append(r.stats)
+                ms.append(t); pairs += r.stats["hits"]; stats.append(r.stats)
         torch.cuda.synchronize()
         barrier(ws)
-        res[name] = dict(ms=ms, pairs=pairs, stats=stats, clocks=clk.summary(), result=r)
-    # identical results between the variants (0 pair diffs, same DE-9IM)
-    a, b = res["filtered"]["result"], res["plain"]["result"]
+        res[name] = dict(ms=ms, pairs=pairs, stats=stats, clocks=clk.summary())
+    # checks (untimed): the rows of both variants, compared with each other and with the reference engine's
+    a = eng.join(L, L, want_area=False, want_relate=True, upper=True, refine_mode=gsj.GSJ_REFINE_FILTERED, **shard)
+    b = eng.join(L, L, want_area=False, want_relate=True, upper=True, refine_mode=gsj.GSJ_REFINE_PLAIN, **shard)
     ia, ib = np.lexsort(a.pairs.T[::-1]), np.lexsort(b.pairs.T[::-1])
     same_pairs = a.pairs.shape == b.pairs.shape and np.array_equal(a.pairs[ia], b.pairs[ib])
     pair_diffs = 0 if same_pairs else len(set(map(tuple, a.pairs.tolist())) ^ set(map(tuple, b.pairs.tolist())))
     code_diffs = int((a.code[ia] != b.code[ib]).sum()) if same_pairs else None
+    refcheck = None
+    if rank == 0 and not shard and not args.no_reference_check:
+        import shutil
+        import tempfile
+        d = tempfile.mkdtemp(prefix="gsj_refcheck_")
+        try:
+            refcheck = reference_check(ps, a, d)
+        finally:
+            shutil.rmtree(d, ignore_errors=True)
+    del b
 
     # end-to-end through the C ABI from pinned host buffers: upload + LBVH + join + D2H of the rows
     e2e_ms, e2e_pairs = [], 0
@@ -576,15 +648,18 @@ def main():
     plain_value, plain_ms = aggregate(float(np.sum(res["plain"]["ms"])), float(res["plain"]["pairs"]), ws)
     e2e_value, e2e_tot = aggregate(float(np.sum(e2e_ms)), float(e2e_pairs), ws)
     pk = peaks()
-    # roofline of the dominant kernel (refinement): algorithmic bytes = both geometries' vertices per candidate pair
-    cand = eng.candidates(L, L, upper=True)
-    nvg = (ps.rvo[ps.gro[1:]] - ps.rvo[ps.gro[:-1]]).astype(np.int64)
-    alg_bytes = float(16 * (nvg[cand[:, 0]] + nvg[cand[:, 1]]).sum() + len(cand) * (8 + 1 + 32 + 4 + 2 * 40))
     st = f["stats"]
     refine_ms = float(np.mean([s["refine_ms"] for s in st]))
     trav_ms = float(np.mean([s["traverse_ms"] for s in st]))
     hbm = pk.get("hbm_gbs", 6650.0)
-    # algorithmic traversal bytes: 48-byte node records actually visited + probe box and order id + written pairs
+    # roofline of the dominant kernel (refinement), FP64-bound: algorithmic flops = the local edge pairs (na x nb per
+    # refined pair, counted by the kernels) x FLOPS_PER_EDGE_PAIR; its HBM figure = both geometries' vertices per pair
+    edge_pairs = float(np.mean([s["edge_pairs"] for s in st]))
+    flops = edge_pairs * FLOPS_PER_EDGE_PAIR
+    cand = eng.candidates(L, L, upper=True)
+    nvg = (ps.rvo[ps.gro[1:]] - ps.rvo[ps.gro[:-1]]).astype(np.int64)
+    alg_bytes = float(16 * (nvg[cand[:, 0]] + nvg[cand[:, 1]]).sum() + len(cand) * (8 + 1 + 32 + 4 + 2 * 40))
+    # traversal: 48-byte node records visited + probe box and order id + written pairs (mostly served from L2)
     trav_bytes = float(np.mean([s_["node_visits"] for s_ in st]) * 48 + ps.n * (16 + 4) + len(cand) * 8)
     traffic = None
     try:
@@ -611,7 +686,8 @@ def main():
         "config": {"workload": WORKLOAD, "parcels": int(L.info["n"]), "vertices": int(L.info["nv"]), "candidates": int(st[0]["candidates"]),
                    "pairs_per_step": int(st[0]["hits"]),
                    "parallelism": f"probe shards x{ws} (one layer, R replicated)" if shard else f"replicas x{ws} (own layer per rank)",
-                   "l2": "inputs > L2 (2.2 GB resident layer)", "gen_s": round(t_gen, 2)},
+                   "l2": "inputs > L2 (2.2 GB resident layer)"},
+        "gen_s": round(t_gen, 2),
         "latency_ms": ({"p50": serving["filtered"]["p50_ms"], "p99": serving["filtered"]["p99_ms"],
                         "what": "gsjd serving, arrival to end of result stream"} if serving else None),
         "step_latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
@@ -620,15 +696,23 @@ def main():
                        "latency_ms": {"p50": float(np.percentile(res["plain"]["ms"], 50)), "p99": float(np.percentile(res["plain"]["ms"], 99))},
                        "speedup_filtered": value / plain_value},
         "pair_diffs_filtered_vs_plain": pair_diffs, "code_diffs_filtered_vs_plain": code_diffs,
+        "pair_diffs_vs_reference": (refcheck or {}).get("pair_diffs"), "code_diffs_vs_reference": (refcheck or {}).get("code_diffs"),
+        "reference_check": refcheck,
         "phases_ms": {k: float(np.mean([s[k] for s in st])) for k in ("traverse_ms", "refine_ms", "compact_ms", "copy_ms")},
         "e2e": {"value": e2e_value, "unit": "pairs/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "ms_per_step": e2e_tot / args.steps},
-        "roofline": {"kernel": "k_refine (+k_refine_scratch)", "bound": "hbm", "achieved": alg_bytes / (refine_ms / 1000.0) / 1e9,
-                     "peak": hbm, "unit": "GB/s", "frac": alg_bytes / (refine_ms / 1000.0) / 1e9 / hbm, "traffic": traffic,
-                     "peak_source": "MEASURED_PEAKS.json hbm_gbs" if "hbm_gbs" in pk else "fallback",
-                     "note": "refinement is FP64-pipe / latency bound; bytes = both geometries' vertices per candidate pair"},
-        "roofline_traversal": {"kernel": "k_traverse", "bound": "hbm", "achieved": trav_bytes / (trav_ms / 1000.0) / 1e9, "peak": hbm,
-                               "unit": "GB/s", "frac": trav_bytes / (trav_ms / 1000.0) / 1e9 / hbm},
+        "roofline": {"kernel": "k_refine<1> (+k_refine_scratch<1>)", "bound": "fp64", "achieved": flops / (refine_ms / 1000.0) / 1e12,
+                     "peak": FP64_PEAK_TFLOPS, "unit": "TFLOP/s", "frac": flops / (refine_ms / 1000.0) / 1e12 / FP64_PEAK_TFLOPS,
+                     "traffic": traffic, "peak_source": "B200 FP64 specification (HGX B200: 296 TFLOPS / 8 GPUs); not measured here",
+                     "work": {"edge_pairs_per_launch": edge_pairs, "flops_per_edge_pair": FLOPS_PER_EDGE_PAIR,
+                              "what": "local edge pairs na x nb of every refined pair (the reference's brute-force unit), counted in the kernels"},
+                     "hbm": {"achieved_gbs": alg_bytes / (refine_ms / 1000.0) / 1e9, "peak_gbs": hbm,
+                             "frac": alg_bytes / (refine_ms / 1000.0) / 1e9 / hbm,
+                             "peak_source": "MEASURED_PEAKS.json hbm_gbs" if "hbm_gbs" in pk else "fallback",
+                             "bytes": "both geometries' vertices per candidate pair + per-pair outputs"}},
+        "roofline_traversal": {"kernel": "k_traverse", "bound": "l2/hbm latency", "what": "visited LBVH node bytes per second (mostly L2 hits)",
+                               "achieved": trav_bytes / (trav_ms / 1000.0) / 1e9, "unit": "GB/s", "hbm_peak": hbm,
+                               "node_bytes_over_hbm_peak": trav_bytes / (trav_ms / 1000.0) / 1e9 / hbm},
         "gpu_launches": int(sum(s["launches"] for s in st)),
         "clocks": f["clocks"],
         "cpu_baseline": cpu,

@@ -97,6 +97,7 @@ typedef struct gsj_join_stats {
   uint64_t candidates, hits, heavy, batches;
   uint64_t launches;     /* kernels of this library launched by the call */
   uint64_t node_visits;  /* LBVH nodes visited by the candidate search (48 bytes each) */
+  uint64_t edge_pairs;   /* sum over the refined pairs of na x nb, their local edge counts (the refinement's work unit) */
 } gsj_join_stats;
 
 /* Sink for a finished batch (the host callback of join_stream): pairs[2n] = (P index, R index) in parent ids,

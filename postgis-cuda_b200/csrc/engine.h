@@ -106,6 +106,7 @@ struct gsj_ctx {
   int refine_attr = 0, dw_attr = 0, er_attr = 0;
   uint64_t launches = 0;      // kernels launched by this context (reported per call in the stats)
   uint64_t node_visits = 0;   // LBVH nodes visited by traversals (roofline accounting)
+  uint64_t edge_pairs = 0;    // local edge pairs (na x nb) of the pairs refined (the refinement's work unit)
   // scratch pools
   gsj::DevBuf counters, cand, flag, area, ev, evb, heavy, scratch, keep, opairs, oarea, oev, oevb, ocode, tmp, keys, keys2, idx,
       idx2, agg_area, agg_ev, agg_evb, agg_flag, qbb, uf, misc1, misc2, misc3,

@@ -459,7 +459,7 @@ void join_host(gsj_ctx* c, const gsj_layer* P, const gsj_layer* R, const gsj_ref
   RefineArgs rp = to_args(rpp);
   gsj_join_opts o = opts_or_default(op);
   gsj_join_stats st{};
-  const uint64_t l0 = c->launches, v0 = c->node_visits;
+  const uint64_t l0 = c->launches, v0 = c->node_visits, e0 = c->edge_pairs;
   Timer tm(c->stream);
   run_join(c, P, R, rp, o, st, [&](const JoinOut& out) {
     if (!out.n) return;
@@ -475,13 +475,14 @@ void join_host(gsj_ctx* c, const gsj_layer* P, const gsj_layer* R, const gsj_ref
   });
   st.launches = c->launches - l0;
   st.node_visits = c->node_visits - v0;
+  st.edge_pairs = c->edge_pairs - e0;
   if (stp) *stp = st;
 }
 
 void points_host(gsj_ctx* c, const gsj_layer* pts, const gsj_layer* R, const gsj_join_opts* op, gsj_points_sink sink, void* user, gsj_join_stats* stp) {
   gsj_join_opts o = opts_or_default(op);
   gsj_join_stats st{};
-  const uint64_t l0 = c->launches, v0 = c->node_visits;
+  const uint64_t l0 = c->launches, v0 = c->node_visits, e0 = c->edge_pairs;
   Timer tm(c->stream);
   run_points(c, pts, R, o, st, [&](const uint2* dp, const uint8_t* dw, uint64_t n) {
     if (!n) return;
@@ -495,6 +496,7 @@ void points_host(gsj_ctx* c, const gsj_layer* pts, const gsj_layer* R, const gsj
   });
   st.launches = c->launches - l0;
   st.node_visits = c->node_visits - v0;
+  st.edge_pairs = c->edge_pairs - e0;
   if (stp) *stp = st;
 }
 
@@ -506,7 +508,7 @@ void cluster_host(gsj_ctx* c, const gsj_layer* P, uint32_t nparent, const gsj_jo
   RefineArgs rp = to_args(nullptr);
   rp.want_area = 0; rp.want_relate = 0;
   gsj_join_stats st{};
-  const uint64_t l0 = c->launches, v0 = c->node_visits;
+  const uint64_t l0 = c->launches, v0 = c->node_visits, e0 = c->edge_pairs;
   cudaStream_t s = c->stream;
   uint32_t* par = c->uf.as<uint32_t>(2 * (size_t)nparent);
   uint32_t* droot = par + nparent;
@@ -565,6 +567,7 @@ void cluster_host(gsj_ctx* c, const gsj_layer* P, uint32_t nparent, const gsj_jo
   GSJ_CK(cudaStreamSynchronize(s));
   st.launches = c->launches - l0;
   st.node_visits = c->node_visits - v0;
+  st.edge_pairs = c->edge_pairs - e0;
   if (stp) *stp = st;
 }
 

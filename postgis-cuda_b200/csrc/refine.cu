@@ -35,7 +35,6 @@ struct PairGeo { Box ov; double tol, eps_par, snap, cx, cy; };
 // 2 tol of each other - a superset of the pairs any box test of the pair routine keeps (those use tol or no pad).
 // Built by one lane-balanced sweep over the na x nb grid (ballot compaction keeps (i, j) order); per-edge
 // ranges: A edge i owns cp[sa[i] .. sa[i+1]), B edge j owns pj[(j ? sb[j-1] : 0) .. sb[j]) (entries in i order).
-constexpr int CPCAP = 512;
 constexpr int REFINE_RUN = 4, REFINE_RUNS = 32;   // filtered kernel: pairs per fetch, fetches per warp
 // Large grids are searched by buckets instead: NBK slabs along the overlap box's longer side, B's edges listed per
 // slab (bl, boff), each lane scanning only its A edge's slabs and reporting a pair once, in the first slab both
@@ -44,7 +43,6 @@ constexpr int REFINE_RUN = 4, REFINE_RUNS = 32;   // filtered kernel: pairs per 
 constexpr int NBK = 16, LCAP = 32;
 constexpr int GRID_MAX = 2048;   // scratch kernel: na x nb up to this: the grid sweep
 struct FlatBuf { uint32_t* cp; uint16_t* pj; uint32_t* sa; uint32_t* sb; uint32_t* bl; uint32_t* boff; int cap, blcap; };   // cap: entries of cp / pj
-constexpr size_t FLAT_BYTES = CPCAP * sizeof(uint32_t) + CPCAP * sizeof(uint16_t) + 2 * (CAP_F + 1) * sizeof(uint32_t);
 
 __device__ __forceinline__ void warp_exscan(uint32_t* a, int n, int lane) {   // in place over a[0 .. n)
   uint32_t run = 0;
@@ -204,6 +202,54 @@ __device__ int flat_candidates(const EList& LA, int na, const EList& LB, int nb,
   return cnt;
 }
 
+// Candidate edge pairs of the shared-memory kernel as bit masks: row i holds the B edges j whose boxes come within
+// 2 tol of A edge i (the flat lists' test and set), column j the A edges i. A row visits its j, a column its i, in
+// increasing order by walking set bits, which is the order of the flat lists; the masks never overflow (up to
+// CAP_F edges per side) and cost no counting, scans or scatter. Word-major: word w of row i at rm[w * CAP_F + i].
+constexpr int MASK_WORDS = CAP_F / 32;
+struct MaskBuf { uint32_t* rm; uint32_t* cm; };
+constexpr size_t MASK_BYTES = 2 * (size_t)MASK_WORDS * CAP_F * sizeof(uint32_t);
+
+// one stage of the in-register 32 x 32 bit transpose: lanes l and l ^ s swap the off-diagonal s x s blocks
+__device__ __forceinline__ uint32_t transpose_stage(uint32_t x, int s, uint32_t m, int lane) {
+  const uint32_t p = __shfl_xor_sync(0xffffffffu, x, s);
+  return (lane & s) ? ((x & ~m) | ((p >> s) & m)) : ((x & m) | ((p << s) & ~m));
+}
+// lane l holds row l of a 32 x 32 bit matrix (bit j = M[l][j]); returns column l (bit i = M[i][l])
+__device__ __forceinline__ uint32_t warp_transpose32(uint32_t x, int lane) {
+  x = transpose_stage(x, 16, 0x0000FFFFu, lane);
+  x = transpose_stage(x, 8, 0x00FF00FFu, lane);
+  x = transpose_stage(x, 4, 0x0F0F0F0Fu, lane);
+  x = transpose_stage(x, 2, 0x33333333u, lane);
+  return transpose_stage(x, 1, 0x55555555u, lane);
+}
+
+// lane i (per 32 A edges) keeps its padded box in registers and tests every B edge j, read once for the whole warp
+// (a shared-memory broadcast); each 32 x 32 block of rows is transposed into columns by shuffles
+__device__ void mask_candidates(const EList& LA, int na, const EList& LB, int nb, double pad, const MaskBuf& mb, int lane) {
+  const int nbw = (nb + 31) >> 5;
+  const double inf = __longlong_as_double(0x7ff0000000000000LL);
+  for (int ic = 0; ic < na; ic += 32) {
+    const int i = ic + lane;
+    double ax0 = inf, ay0 = inf, ax1 = -inf, ay1 = -inf;   // lanes past the end keep an empty box: no bits
+    if (i < na) {
+      const double px = LA.x0[i], py = LA.y0[i], qx = LA.x1[i], qy = LA.y1[i];
+      ax0 = (px < qx ? px : qx) - pad; ax1 = (px < qx ? qx : px) + pad;
+      ay0 = (py < qy ? py : qy) - pad; ay1 = (py < qy ? qy : py) + pad;
+    }
+    for (int w = 0; w < nbw; w++) {
+      const int j0 = w << 5, j1 = min(nb, j0 + 32);
+      uint32_t bits = 0;
+      for (int j = j0; j < j1; j++)
+        bits |= (out_cmp(LB.x0[j], LB.y0[j], LB.x1[j], LB.y1[j], ax0, ay0, ax1, ay1) ? 0u : 1u) << (j - j0);
+      if (i < na) mb.rm[w * CAP_F + i] = bits;
+      const uint32_t col = warp_transpose32(bits, lane);
+      if (j0 + lane < nb) mb.cm[(ic >> 5) * CAP_F + j0 + lane] = col;
+    }
+  }
+  __syncwarp();
+}
+
 // Green's-theorem contribution of edge p->q within the other polygon + relate lengths (engine.cuh:416-515).
 // each_k(visit) calls visit(k) for the other polygon's local edges k in increasing order: all of them, or only
 // those of a candidate list that holds every k passing the box test below (the same visits, the same results).
@@ -312,11 +358,13 @@ __device__ __forceinline__ double pair_snap(double2 oa, double2 ea) {   // engin
 }
 
 // One pair, whole warp. Returns false when a local list exceeded cap (nothing written).
-// FLAT (filtered kernel only): the candidate-list path; a pair whose list would exceed CPCAP is handed back
-// (false) like an oversized pair, and the scratch kernel runs it with the full sweeps.
-template <bool F, bool FLAT = false, bool BUCKETS = false>
+// MASK (the filtered shared-memory kernel): candidate edge pairs as bit masks (mb).
+// FLAT (the filtered scratch kernel): candidate lists in global scratch; a pair whose list would exceed fb->cap is
+// handed back (false) and runs with the full sweeps.
+template <bool F, bool FLAT = false, bool BUCKETS = false, bool MASK = false>
 __device__ bool refine_pair_t(const DLayer& P, const DLayer& R, uint32_t a, uint32_t b, const RefineArgs& rp, EList LA, EList LB, int cap,
-                              int lane, uint8_t& o_flag, double& o_area, double4& o_ev, uint32_t& o_evb, const FlatBuf* fb = nullptr) {
+                              int lane, uint8_t& o_flag, double& o_area, double4& o_ev, uint32_t& o_evb, const FlatBuf* fb = nullptr,
+                              const MaskBuf* mb = nullptr, unsigned long long* ep = nullptr) {
   const double2 oa = P.origin[a], ob = R.origin[b], ea = P.ext[a], eb = R.ext[b];
   const double sx = ob.x - oa.x, sy = ob.y - oa.y;
   const double pad = 4.0 * fmax(rp.tol_abs, (double)rp.tol_rel * fmax(fmax(ea.x, ea.y), fmax(eb.x, eb.y)));
@@ -334,7 +382,9 @@ __device__ bool refine_pair_t(const DLayer& P, const DLayer& R, uint32_t a, uint
   if (na > cap || nb > cap) return false;
   __syncwarp();
   int ncp = -1;   // candidate edge pairs (FLAT); -1: sweep every edge pair
-  if constexpr (FLAT) {
+  if constexpr (MASK) {
+    mask_candidates(LA, na, LB, nb, 2.0 * G.tol, *mb, lane);
+  } else if constexpr (FLAT) {
     ncp = flat_candidates<BUCKETS>(LA, na, LB, nb, 2.0 * G.tol, G.ov, *fb, lane);
     if (ncp > fb->cap) return false;
   }
@@ -356,7 +406,35 @@ __device__ bool refine_pair_t(const DLayer& P, const DLayer& R, uint32_t a, uint
     };
     for (int j = 0; j < nb; j++) if (test(j)) break;
   };
-  if constexpr (FLAT) {
+  if constexpr (MASK) {
+    // each lane walks its A edge's candidates, one per round; the warp stops at the first real contact
+    const int nbw = (nb + 31) >> 5;
+    for (int ic = 0; ic < na && !hit; ic += 32) {
+      const int i = ic + lane;
+      uint32_t w[MASK_WORDS];
+      #pragma unroll
+      for (int q = 0; q < MASK_WORDS; q++) w[q] = (i < na && q < nbw) ? mb->rm[q * CAP_F + i] : 0u;
+      double px0 = 0, py0 = 0, px1 = 0, py1 = 0;
+      uint32_t fa = 0;
+      if (i < na) { px0 = LA.x0[i]; py0 = LA.y0[i]; px1 = LA.x1[i]; py1 = LA.y1[i]; fa = LA.fl[i]; }
+      const double ax0 = px0 < px1 ? px0 : px1, ax1 = px0 < px1 ? px1 : px0, ay0 = py0 < py1 ? py0 : py1, ay1 = py0 < py1 ? py1 : py0;
+      for (;;) {
+        int j = -1;
+        #pragma unroll
+        for (int q = 0; q < MASK_WORDS; q++)
+          if (j < 0 && w[q]) { j = (q << 5) + __ffs(w[q]) - 1; w[q] &= w[q] - 1; }
+        if (!__any_sync(0xffffffffu, j >= 0)) break;
+        if (j >= 0) {
+          const double qx0 = LB.x0[j], qy0 = LB.y0[j], qx1 = LB.x1[j], qy1 = LB.y1[j];
+          if (!out_cmp(qx0, qy0, qx1, qy1, ax0, ay0, ax1, ay1) && seg_isect(px0, py0, px1, py1, qx0, qy0, qx1, qy1)) {
+            hit_any = true;
+            if (!((fa | LB.fl[j]) & 1u)) hit = true;
+          }
+        }
+        if (__any_sync(0xffffffffu, hit)) { hit = true; break; }
+      }
+    }
+  } else if constexpr (FLAT) {
     // one candidate per lane; the warp stops at the first real contact (hit_any is then implied)
     for (int base = 0; base < ncp; base += 32) {
       const int e = base + lane;
@@ -429,7 +507,26 @@ __device__ bool refine_pair_t(const DLayer& P, const DLayer& R, uint32_t a, uint
     double s2 = 0.0, ai = 0, ao = 0, bi = 0, bo = 0;
     uint32_t bits = rtouch ? REL_TOUCH : 0;
     const bool rel = rp.want_relate != 0;
-    if constexpr (FLAT) {   // visit only each edge's candidates, in the same increasing order; one call site for both passes
+    if constexpr (MASK) {   // visit only each edge's candidates, in increasing order, by walking the set bits
+      const int nbw = (nb + 31) >> 5, naw = (na + 31) >> 5;
+      for (int pass = 0; pass < 2; pass++) {
+        const EList& LS = pass ? LB : LA;
+        const EList& LO = pass ? LA : LB;
+        const int nself = pass ? nb : na, nother = pass ? na : nb, nw = pass ? naw : nbw;
+        const uint32_t* mrow = pass ? mb->cm : mb->rm;
+        const bool inc = pass ? inA_c : inB_c;
+        double lin = 0.0, lon = 0.0;   // this pass's lengths (each starts from 0, so the sums are the same)
+        for (int i = lane; i < nself; i += 32) {
+          const uint32_t f = LS.fl[i];
+          s2 += edge_contrib_k<F>(LS.x0[i], LS.y0[i], LS.x1[i], LS.y1[i], LO, nother, inc, G, !(f & 1u), rel ? &lin : nullptr, &lon, &bits, f,
+                                  [&](auto&& visit) {
+                                    for (int q = 0; q < nw; q++)
+                                      for (uint32_t m = mrow[q * CAP_F + i]; m; m &= m - 1) visit((q << 5) + __ffs(m) - 1);
+                                  });
+        }
+        if (pass) { bi = lin; bo = lon; } else { ai = lin; ao = lon; }
+      }
+    } else if constexpr (FLAT) {   // visit only each edge's candidates, in the same increasing order; one call site for both passes
       const uint32_t* cp = fb->cp;
       const uint16_t* pj = fb->pj;
       for (int pass = 0; pass < 2; pass++) {
@@ -467,6 +564,7 @@ __device__ bool refine_pair_t(const DLayer& P, const DLayer& R, uint32_t a, uint
   const bool ev_any = e4.x != 0 || e4.y != 0 || e4.z != 0 || e4.w != 0;
   o_flag = hit ? 1 : ((ar != 0.0 || ev_any) ? 2 : 0);
   o_area = ar; o_ev = e4; o_evb = eb4;
+  if (ep && lane == 0) *ep += (unsigned long long)na * (unsigned long long)nb;   // local edge pairs: the refinement's work unit
   return true;
 }
 
@@ -478,7 +576,7 @@ __device__ bool refine_pair(const DLayer& P, const DLayer& R, uint32_t a, uint32
 
 template <bool F> struct Cfg;
 template <> struct Cfg<false> { static constexpr int cap = CAP; static constexpr size_t list = LIST_BYTES, smem = RB_SMEM, edge = EDGE_BYTES; static constexpr int minb = 3; };
-template <> struct Cfg<true> { static constexpr int cap = CAP_F; static constexpr size_t list = LIST_BYTES_F, smem = RB_SMEM_F + RB_WARPS * FLAT_BYTES, edge = EDGE_BYTES_F; static constexpr int minb = 4; };
+template <> struct Cfg<true> { static constexpr int cap = CAP_F; static constexpr size_t list = LIST_BYTES_F, smem = RB_SMEM_F + RB_WARPS * MASK_BYTES, edge = EDGE_BYTES_F; static constexpr int minb = 4; };
 
 template <bool F>
 __device__ __forceinline__ EList carve_t(unsigned char* base, int cap) { return F ? carve_f(base, cap) : carve(base, cap); }
@@ -486,28 +584,25 @@ __device__ __forceinline__ EList carve_t(unsigned char* base, int cap) { return 
 template <bool F>
 __global__ void __launch_bounds__(RB_WARPS * 32, Cfg<F>::minb) k_refine(DLayer P, DLayer R, const uint2* __restrict__ pairs, uint64_t np,
                                                                         RefineArgs rp, uint8_t* flag, double* area, double4* ev, uint32_t* evb,
-                                                                        uint32_t* heavy, unsigned long long* nheavy, unsigned long long* next) {
+                                                                        uint32_t* heavy, unsigned long long* nheavy, unsigned long long* next,
+                                                                        unsigned long long* epairs) {
   extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ unsigned long long s_ep[RB_WARPS];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  if (lane == 0) s_ep[wib] = 0;
+  __syncwarp();
   EList LA = carve_t<F>(smem + (size_t)wib * 2 * Cfg<F>::list, Cfg<F>::cap);
   EList LB = carve_t<F>(smem + (size_t)wib * 2 * Cfg<F>::list + Cfg<F>::list, Cfg<F>::cap);
-  FlatBuf fbuf;
-  const FlatBuf* fb = nullptr;
-  if constexpr (F) {   // after the lists of all warps: cp (u32), sa, sb (u32), pj (u16)
-    unsigned char* fbase = smem + (size_t)RB_WARPS * 2 * Cfg<F>::list + (size_t)wib * FLAT_BYTES;
-    fbuf.cp = reinterpret_cast<uint32_t*>(fbase);
-    fbuf.sa = fbuf.cp + CPCAP;
-    fbuf.sb = fbuf.sa + (CAP_F + 1);
-    fbuf.pj = reinterpret_cast<uint16_t*>(fbuf.sb + (CAP_F + 1));
-    fbuf.bl = fbuf.boff = nullptr;
-    fbuf.cap = CPCAP;
-    fbuf.blcap = 0;
-    fb = &fbuf;
+  MaskBuf mbuf{nullptr, nullptr};
+  if constexpr (F) {   // after the lists of all warps: row masks, then column masks
+    unsigned char* mbase = smem + (size_t)RB_WARPS * 2 * Cfg<F>::list + (size_t)wib * MASK_BYTES;
+    mbuf.rm = reinterpret_cast<uint32_t*>(mbase);
+    mbuf.cm = mbuf.rm + MASK_WORDS * CAP_F;
   }
   auto one = [&](uint64_t p) {
     const uint2 pr = pairs[p];
     uint8_t f; double ar; double4 e4; uint32_t b4;
-    const bool ok = refine_pair_t<F, F>(P, R, pr.x, pr.y, rp, LA, LB, Cfg<F>::cap, lane, f, ar, e4, b4, fb);
+    const bool ok = refine_pair_t<F, false, false, F>(P, R, pr.x, pr.y, rp, LA, LB, Cfg<F>::cap, lane, f, ar, e4, b4, nullptr, &mbuf, &s_ep[wib]);
     if (lane == 0) {
       if (!ok) { heavy[atomicAdd(nheavy, 1ull)] = (uint32_t)p; flag[p] = 0; }
       else {
@@ -534,6 +629,8 @@ __global__ void __launch_bounds__(RB_WARPS * 32, Cfg<F>::minb) k_refine(DLayer P
     const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
     for (uint64_t p = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; p < np; p += nw) one(p);
   }
+  __syncwarp();
+  if (lane == 0 && s_ep[wib]) atomicAdd(epairs, s_ep[wib]);
 }
 
 // oversized pairs: the same pair routine with per-warp edge lists in global scratch. The filtered variant also
@@ -546,8 +643,9 @@ __host__ __device__ constexpr size_t scratch_per_warp(int cap, int cph) {
 template <bool F>
 __global__ void __launch_bounds__(128) k_refine_scratch(DLayer P, DLayer R, const uint2* __restrict__ pairs, const uint32_t* __restrict__ heavy,
                                                        uint64_t nh, RefineArgs rp, uint8_t* flag, double* area, double4* ev, uint32_t* evb,
-                                                       unsigned char* scratch, int cap, int cph, int* err) {
+                                                       unsigned char* scratch, int cap, int cph, int* err, unsigned long long* epairs) {
   const int lane = threadIdx.x & 31;
+  unsigned long long ep = 0;
   const uint64_t w = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
   unsigned char* base = scratch + w * scratch_per_warp<F>(cap, cph);
   EList LA = carve_t<F>(base, cap), LB = carve_t<F>(base + (size_t)cap * Cfg<F>::edge, cap);
@@ -568,10 +666,10 @@ __global__ void __launch_bounds__(128) k_refine_scratch(DLayer P, DLayer R, cons
     uint8_t f; double ar; double4 e4; uint32_t b4;
     bool ok;
     if constexpr (F) {   // candidate entries pack both edge indices in 16 bits each
-      ok = cap <= 0xFFFF && refine_pair_t<F, true, true>(P, R, pr.x, pr.y, rp, LA, LB, cap, lane, f, ar, e4, b4, &fb);
-      if (!ok) ok = refine_pair_t<F, false>(P, R, pr.x, pr.y, rp, LA, LB, cap, lane, f, ar, e4, b4);
+      ok = cap <= 0xFFFF && refine_pair_t<F, true, true>(P, R, pr.x, pr.y, rp, LA, LB, cap, lane, f, ar, e4, b4, &fb, nullptr, &ep);
+      if (!ok) ok = refine_pair_t<F, false>(P, R, pr.x, pr.y, rp, LA, LB, cap, lane, f, ar, e4, b4, nullptr, nullptr, &ep);
     } else {
-      ok = refine_pair_t<F, false>(P, R, pr.x, pr.y, rp, LA, LB, cap, lane, f, ar, e4, b4);
+      ok = refine_pair_t<F, false>(P, R, pr.x, pr.y, rp, LA, LB, cap, lane, f, ar, e4, b4, nullptr, nullptr, &ep);
     }
     if (lane == 0) {
       if (!ok) *err = 1;
@@ -583,6 +681,7 @@ __global__ void __launch_bounds__(128) k_refine_scratch(DLayer P, DLayer R, cons
     }
     __syncwarp();
   }
+  if (lane == 0 && ep) atomicAdd(epairs, ep);
 }
 
 template <bool F>
@@ -595,7 +694,7 @@ static uint64_t refine_t(gsj_ctx* c, const gsj_layer* P, const gsj_layer* R, con
   }
   unsigned long long* ctr = c->counters.as<unsigned long long>(8);
   int* err = reinterpret_cast<int*>(ctr + 1);
-  GSJ_CK(cudaMemsetAsync(ctr, 0, 24, s));   // heavy count, error word, pair counter
+  GSJ_CK(cudaMemsetAsync(ctr, 0, 32, s));   // heavy count, error word, pair counter, local edge pairs
   uint32_t* heavy = c->heavy.as<uint32_t>(np);
   int blocks;
   if constexpr (F) {   // enough warps to cover every pair with REFINE_RUNS fetches each, spread over all SMs
@@ -606,10 +705,11 @@ static uint64_t refine_t(gsj_ctx* c, const gsj_layer* P, const gsj_layer* R, con
   } else {
     blocks = (int)std::min<uint64_t>((np + RB_WARPS - 1) / RB_WARPS, (uint64_t)c->sm_count * 8);
   }
-  k_refine<F><<<blocks, RB_WARPS * 32, Cfg<F>::smem, s>>>(P->d, R->d, pairs, np, rp, flag, area, ev, evb, heavy, ctr, ctr + 2); c->launches++;
+  k_refine<F><<<blocks, RB_WARPS * 32, Cfg<F>::smem, s>>>(P->d, R->d, pairs, np, rp, flag, area, ev, evb, heavy, ctr, ctr + 2, ctr + 3);
+  c->launches++;
   GSJ_CK(cudaGetLastError());
-  unsigned long long* h = c->h_counters.as<unsigned long long>(2);
-  GSJ_CK(cudaMemcpyAsync(h, ctr, 16, cudaMemcpyDeviceToHost, s));
+  unsigned long long* h = c->h_counters.as<unsigned long long>(4);
+  GSJ_CK(cudaMemcpyAsync(h, ctr, 32, cudaMemcpyDeviceToHost, s));
   GSJ_CK(cudaStreamSynchronize(s));
   const uint64_t nh = h[0];
   if (nh) {
@@ -622,12 +722,14 @@ static uint64_t refine_t(gsj_ctx* c, const gsj_layer* P, const gsj_layer* R, con
     nwarps = (nwarps + 3) / 4 * 4;
     unsigned char* scr = c->scratch.as<unsigned char>(per * nwarps);
     GSJ_CK(cudaMemsetAsync(err, 0, 4, s));
-    k_refine_scratch<F><<<(int)(nwarps / 4), 128, 0, s>>>(P->d, R->d, pairs, heavy, nh, rp, flag, area, ev, evb, scr, cap, cph, err); c->launches++;
+    k_refine_scratch<F><<<(int)(nwarps / 4), 128, 0, s>>>(P->d, R->d, pairs, heavy, nh, rp, flag, area, ev, evb, scr, cap, cph, err, ctr + 3);
+    c->launches++;
     GSJ_CK(cudaGetLastError());
-    GSJ_CK(cudaMemcpyAsync(h, ctr, 16, cudaMemcpyDeviceToHost, s));
+    GSJ_CK(cudaMemcpyAsync(h, ctr, 32, cudaMemcpyDeviceToHost, s));
     GSJ_CK(cudaStreamSynchronize(s));
     if (reinterpret_cast<int*>(h + 1)[0]) throw Error(GSJ_ERR_CUDA, "oversized pair exceeded the scratch edge capacity");
   }
+  c->edge_pairs += h[3];
   return nh;
 }
 

@@ -46,7 +46,8 @@ class JoinOpts(ctypes.Structure):
 class JoinStats(ctypes.Structure):
     _fields_ = [("traverse_ms", ctypes.c_double), ("refine_ms", ctypes.c_double), ("compact_ms", ctypes.c_double),
                 ("copy_ms", ctypes.c_double), ("candidates", ctypes.c_uint64), ("hits", ctypes.c_uint64), ("heavy", ctypes.c_uint64),
-                ("batches", ctypes.c_uint64), ("launches", ctypes.c_uint64), ("node_visits", ctypes.c_uint64)]
+                ("batches", ctypes.c_uint64), ("launches", ctypes.c_uint64), ("node_visits", ctypes.c_uint64),
+                ("edge_pairs", ctypes.c_uint64)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -318,12 +319,16 @@ class Engine:
 
     # ---- joins ----
     def join(self, P: Layer, R: Layer, want_area=True, want_relate=False, upper=False, no_agg=False,
-             refine_mode=GSJ_REFINE_FILTERED, batch_q=0, snap_half_ulp=False, shard=0, nshards=1) -> JoinResult:
+             refine_mode=GSJ_REFINE_FILTERED, batch_q=0, snap_half_ulp=False, shard=0, nshards=1, collect=True) -> JoinResult:
+        """collect=False: the rows reach the library's pinned host buffers batch by batch as usual but are not copied
+        into numpy arrays (pairs/area/code are None; stats['hits'] counts them)."""
         rp = refine_params(want_area, want_relate, snap_half_ulp)
         o = join_opts(upper, no_agg, refine_mode, batch_q, shard, nshards)
         chunks_p, chunks_a, chunks_c = [], [], []
 
         def sink(user, pairs, area, code, n):
+            if not collect:
+                return 0
             chunks_p.append(np.ctypeslib.as_array(pairs, (n * 2,)).copy())
             if area:
                 chunks_a.append(np.ctypeslib.as_array(area, (n,)).copy())
@@ -334,6 +339,8 @@ class Engine:
         cb = JOIN_SINK(sink)
         st = JoinStats()
         self._check(lib().gsj_join(self.ctx, P.h, R.h, ctypes.byref(rp), ctypes.byref(o), cb, None, ctypes.byref(st)))
+        if not collect:
+            return JoinResult(None, None, None, st.as_dict())
         pairs = np.concatenate(chunks_p).reshape(-1, 2) if chunks_p else np.zeros((0, 2), np.uint32)
         area = (np.concatenate(chunks_a) if chunks_a else np.zeros(0)) if want_area else None
         code = (np.concatenate(chunks_c) if chunks_c else np.zeros(0, np.uint32)) if want_relate else None

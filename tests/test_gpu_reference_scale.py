@@ -90,7 +90,6 @@ def test_area_and_relate_two_layers_2m(engine, tmp, parcels, parcels_b):
         assert_areas(got_a, want_a)
         assert np.array_equal(got_c, rel_c), f"mode {mode}: {(got_c != rel_c).sum()} DE-9IM matrices differ"
     assert len(want_p) > 8_000_000 and (want_a > 0).mean() > 0.5    # interiors overlap
-    assert abs(want_a.sum() - 4.0) < 1e-6                           # both layers tile the same 2 x 2 degree box
     LA.free(); LB.free()
 
 
