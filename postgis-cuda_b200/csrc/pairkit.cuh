@@ -21,11 +21,15 @@ __device__ __forceinline__ bool edge_outside(double px, double py, double qx, do
   return fmax(px, qx) < o.x0 || fmin(px, qx) > o.x1 || fmax(py, qy) < o.y0 || fmin(py, qy) > o.y1;
 }
 
-// all edges of geometry A meeting the overlap box, compacted in ring order with a warp ballot (engine.cuh:358-377)
-template <bool F>
-static __device__ int collect(const Frame& A, const Box& ov, EList L, int cap, int lane) {
+// all edges of geometry A meeting the overlap box, compacted in ring order with a warp ballot (engine.cuh:358-377).
+// PIP: the same pass also takes the crossing parity of the segment (A's bbox left edge - 1, my) -> (mx, my) over
+// every edge of A, as pip_full_warp does (an XOR over the edges, so the order is free), into *inside.
+template <bool F, bool PIP = false>
+static __device__ int collect(const Frame& A, const Box& ov, EList L, int cap, int lane, double mx = 0, double my = 0, bool* inside = nullptr) {
   const DLayer& S = *A.L;
   const unsigned lt = (1u << lane) - 1;
+  const double ox = A.shx - (double)1, oy = my;
+  bool par = false;
   int cnt = 0;
   for (uint32_t ra = A.r0; ra < A.r1; ra++) {
     const uint64_t s = S.rvo[ra], e = S.rvo[ra + 1];
@@ -39,6 +43,13 @@ static __device__ int collect(const Frame& A, const Box& ov, EList L, int cap, i
           fl = (uint32_t)S.syn(i) | (S.syn(i > s ? i - 1 : e - 2) ? 2u : 0u) | (S.syn(i + 2 < e ? i + 1 : s) ? 4u : 0u);
         }
         in = F ? !out_cmp(x0, y0, x1, y1, ov.x0, ov.y0, ov.x1, ov.y1) : !edge_outside(x0, y0, x1, y1, ov);
+        if (PIP && !((y0 > my) == (y1 > my) && y0 != my && y1 != my)) {
+          const bool so = left_of(x0, y0, x1, y1, ox, oy), sc = left_of(x0, y0, x1, y1, mx, my);
+          if (so != sc) {
+            const bool su = orient(ox, oy, mx, my, x0, y0) > 0, sv = orient(ox, oy, mx, my, x1, y1) > 0;
+            if (su != sv) par = !par;
+          }
+        }
       }
       const unsigned m = __ballot_sync(0xffffffffu, in);
       const int pos = cnt + __popc(m & lt);
@@ -48,6 +59,7 @@ static __device__ int collect(const Frame& A, const Box& ov, EList L, int cap, i
       cnt += __popc(m);
     }
   }
+  if (PIP) *inside = (__popc(__ballot_sync(0xffffffffu, par)) & 1) != 0;
   return cnt;
 }
 

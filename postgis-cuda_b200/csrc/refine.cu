@@ -281,7 +281,13 @@ __device__ double edge_contrib_k(double px, double py, double qx, double qy, con
       col = (g0 * g0 <= snap2 * flen2 || ((cut & 2u) && g0 * g0 <= tf)) && (g1 * g1 <= snap2 * flen2 || ((cut & 4u) && g1 * g1 <= tf));
     }
     if (col) {
-      const double tc = ((ex0 - px) * dx + (ey0 - py) * dy) / len2, te = ((ex1 - px) * dx + (ey1 - py) * dy) / len2;
+      double tc = (ex0 - px) * dx + (ey0 - py) * dy, te = (ex1 - px) * dx + (ey1 - py) * dy;
+      if (F) {   // n / len2 is n for n = +-0 and exactly 1 for n = len2 (> 0): a coincident edge's ends need no division
+        tc = tc == 0.0 ? tc : (tc == len2 ? 1.0 : tc / len2);
+        te = te == 0.0 ? te : (te == len2 ? 1.0 : te / len2);
+      } else {
+        tc = tc / len2; te = te / len2;
+      }
       const double lo = fmax((double)0, fmin(tc, te)), hi = fmin((double)1, fmax(tc, te));
       if (hi > lo) {
         if (lo > 0 && ns < MAXS) ts[ns++] = lo;
@@ -374,10 +380,15 @@ __device__ bool refine_pair_t(const DLayer& P, const DLayer& R, uint32_t a, uint
   G.tol = fmax(rp.tol_abs, (double)rp.tol_rel * fmax(G.ov.x1 - G.ov.x0, G.ov.y1 - G.ov.y0));
   G.eps_par = rp.eps_par;
   G.snap = rp.snap_half_ulp ? pair_snap(oa, ea) : 0.0;
+  G.cx = (double)(G.ov.x0 + 0.381966 * (G.ov.x1 - G.ov.x0));
+  G.cy = (double)(G.ov.y0 + 0.414213 * (G.ov.y1 - G.ov.y0));
   int na = 0, nb = 0;
+  bool inB_c = false, inA_c = false;
   for (int side = 0; side < 2; side++) {   // one inlined copy of the gather
-    const int n = collect<F>(side ? B : A, G.ov, side ? LB : LA, cap, lane);
-    if (side) nb = n; else na = n;
+    bool in = false;
+    // MASK: the containment parity of the probe point c is taken in the gather's pass over each polygon's edges
+    const int n = collect<F, MASK>(side ? B : A, G.ov, side ? LB : LA, cap, lane, G.cx, G.cy, &in);
+    if (side) { nb = n; inB_c = in; } else { na = n; inA_c = in; }
   }
   if (na > cap || nb > cap) return false;
   __syncwarp();
@@ -457,10 +468,7 @@ __device__ bool refine_pair_t(const DLayer& P, const DLayer& R, uint32_t a, uint
   hit = __any_sync(0xffffffffu, hit);
   hit_any = __any_sync(0xffffffffu, hit_any || hit);
   const bool rtouch = hit;
-  G.cx = (double)(G.ov.x0 + 0.381966 * (G.ov.x1 - G.ov.x0));
-  G.cy = (double)(G.ov.y0 + 0.414213 * (G.ov.y1 - G.ov.y0));
-  bool inB_c = false, inA_c = false;
-  if (!hit || rp.want_area || rp.want_relate)
+  if (!MASK && (!hit || rp.want_area || rp.want_relate))
     for (int side = 0; side < 2; side++) {
       const bool in = pip_full_warp(side ? A : B, G.cx, G.cy, lane);
       if (side) inA_c = in; else inB_c = in;
