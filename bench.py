@@ -201,24 +201,30 @@ def cpu_oracle_rate(ps, target_s=15.0):
     return n / dt, dict(pairs=n, seconds=dt, parcels=sub.n, box_deg=w, threads=os.cpu_count())
 
 
-SERVE_RATE, SERVE_REQUESTS, SERVE_WARMUP = 50.0, 500, 50
-SERVE_SIZES = (1e2, 1e5)   # query geometries per request, log-uniform
+# Serving: resident 10M Voronoi polygons (4-512 vertices, log-uniform) + 5M points; a seeded Poisson stream of 50 req/s,
+# each a join of 10^2-10^6 query polygons (log-uniform) of mixed type; then the same requests by closed-loop clients
+# (the daemon at saturation). SERVE_SMALL is a scaled-down copy for quick runs (--serve-small).
+SERVE = dict(name="cfg4", resident=10_000_000, box=(-120.0, 32.0, -115.5, 36.5), vmin=4, vmax=512, points=5_000_000, rate=50.0,
+             requests=1100, warmup=100, sizes=(1e2, 1e6), queries=24, closed_clients=8, closed_s=15.0)
+SERVE_SMALL = dict(name="cfg4 scaled down", resident=1_000_000, box=(-119.0, 33.0, -117.6, 34.4), vmin=4, vmax=512, points=500_000,
+                   rate=50.0, requests=300, warmup=30, sizes=(1e2, 1e5), queries=12, closed_clients=8, closed_s=8.0)
 
 
-def serving_schedule(rng, qpoly, qpts):
-    """Poisson arrivals at SERVE_RATE; ops: intersects+area 50%, relate 20%, dwithin 5 m 20%, point in polygon 10%."""
+def serving_schedule(rng, qpoly, n, rate):
+    """Poisson arrivals at rate; ops: intersects+area 50%, relate 20%, dwithin 5 m 20%, point in polygon 10% (the query
+    polygons against the resident points)."""
     lines, t = [], 0.0
-    for _ in range(SERVE_REQUESTS):
-        t += rng.exponential(1.0 / SERVE_RATE)
-        u = rng.random()
+    for _ in range(n):
+        t += rng.exponential(1.0 / rate)
+        u, q = rng.random(), rng.choice(qpoly)
         if u < 0.5:
-            lines.append(f"{t:.6f}\tJOIN\t{rng.choice(qpoly)}\tresident\t1\tall")
+            lines.append(f"{t:.6f}\tJOIN\t{q}\tresident\t1\tall")
         elif u < 0.7:
-            lines.append(f"{t:.6f}\tRELATE\t{rng.choice(qpoly)}\tresident\t\tall")
+            lines.append(f"{t:.6f}\tRELATE\t{q}\tresident\t\tall")
         elif u < 0.9:
-            lines.append(f"{t:.6f}\tDWITHIN\t{rng.choice(qpoly)}\tresident\tdwithin\t5\t0\tall")
+            lines.append(f"{t:.6f}\tDWITHIN\t{q}\tresident\tdwithin\t5\t0\tall")
         else:
-            lines.append(f"{t:.6f}\tJOIN\t{rng.choice(qpts)}\tresident\t0\tall")
+            lines.append(f"{t:.6f}\tJOIN\t{q}\tpoints\t0\tall")
     return "\n".join(lines) + "\n"
 
 
@@ -228,9 +234,9 @@ SERVE_ARMS = (   # name -> gsjd flags; the same daemon, schedule and priming, on
 )
 
 
-def serving_leg(ps, n_points=1_000_000, workers=4):
-    """gsjd serving a Poisson request stream against the resident layer, filtered and plain FP64 refinement on the
-    same schedule, each after an untimed priming pass over the schedule's distinct requests."""
+def serving_leg(cfg, workers=4):
+    """gsjd serving the request stream against the resident layers, filtered and plain FP64 refinement on the same
+    schedule, each after an untimed priming pass over the schedule's distinct requests; then closed-loop clients."""
     import shutil
     import tempfile
     from gsj import client as C
@@ -240,28 +246,31 @@ def serving_leg(ps, n_points=1_000_000, workers=4):
     d = tempfile.mkdtemp(prefix="gsjd_bench_")
     try:
         t0 = time.time()
-        gen.write_gset(os.path.join(d, "resident.gset"), ps)
+        box = cfg["box"]
+        area = (box[2] - box[0]) * (box[3] - box[1])
+        params = dict(jitter_grid=True, jitter=0.4, vmin=cfg["vmin"], vmax=cfg["vmax"], log_uniform=True)
+        res_layer = gen.voronoi(cfg["resident"], box, 0, **params)
+        n_res, nv_res = res_layer.n, res_layer.nv
+        gen.write_gset(os.path.join(d, "resident.gset"), res_layer)
+        del res_layer
+        gen.write_pset(os.path.join(d, "points.pset"), gen.points(cfg["points"], box, 7))
         rng = np.random.default_rng(42)
-        density = ps.n / ((BOX[2] - BOX[0]) * (BOX[3] - BOX[1]))
-        qpoly, qpts, qsizes = [], [], []
-        for i in range(32):
-            n = int(np.exp(rng.uniform(np.log(SERVE_SIZES[0]), np.log(SERVE_SIZES[1]))))
-            side = min(BOX[2] - BOX[0], (n / density) ** 0.5)
-            x0 = rng.uniform(BOX[0], BOX[2] - side)
-            y0 = rng.uniform(BOX[1], BOX[3] - side)
-            box = (x0, y0, x0 + side, y0 + side)
-            if i < 24:
-                gen.write_gset(os.path.join(d, f"q{i}.gset"), gen.layer_parcels(max(n, 4), box, seed=1000 + i))
-                qpoly.append(f"q{i}")
-            else:
-                gen.write_pset(os.path.join(d, f"t{i}.pset"), gen.points(n, box, 1000 + i))
-                qpts.append(f"t{i}")
-            qsizes.append(n)
+        density = cfg["resident"] / area
+        qpoly, qsizes = [], []
+        lo, hi = cfg["sizes"]
+        for i in range(cfg["queries"]):
+            n = int(np.exp(rng.uniform(np.log(lo), np.log(hi))))
+            side = min(box[2] - box[0], (n / density) ** 0.5)
+            x0 = rng.uniform(box[0], box[2] - side)
+            y0 = rng.uniform(box[1], box[3] - side)
+            gen.write_gset(os.path.join(d, f"q{i}.gset"), gen.voronoi(max(n, 4), (x0, y0, x0 + side, y0 + side), 1000 + i, **params))
+            qpoly.append(f"q{i}")
+            qsizes.append(max(n, 4))
         sched = os.path.join(d, "schedule.tsv")
-        open(sched, "w").write(serving_schedule(rng, qpoly, qpts))
+        open(sched, "w").write(serving_schedule(rng, qpoly, cfg["requests"], cfg["rate"]))
         distinct = sorted({ln.split("\t", 1)[1] for ln in open(sched).read().splitlines() if ln})
         prime = os.path.join(d, "prime.tsv")
-        open(prime, "w").write("".join(f"{0.02 * (i // 8):.3f}\t{req}\n" for i, req in enumerate(distinct * 2)))
+        open(prime, "w").write("".join(f"{0.05 * (i // 4):.3f}\t{req}\n" for i, req in enumerate(distinct)))
         prep_s = time.time() - t0
         out = {}
         for mode, flags in SERVE_ARMS:
@@ -270,25 +279,39 @@ def serving_leg(ps, n_points=1_000_000, workers=4):
             p = D.start(sock, d, workers=workers, threads=max(4, (os.cpu_count() or 8) // 2), log=log, extra=flags)
             try:
                 cl = C.Client(sock)
+                tl = time.time()
                 cl.load("resident", "resident.gset", dedup=False)
+                cl.load("points", "points.pset")
                 for q in qpoly:
                     cl.load(q, q + ".gset", dedup=False)
-                for q in qpts:
-                    cl.load(q, q + ".pset")
-                # untimed priming: every distinct request of the schedule, 8 at a time, so each context has grown
+                load_s = time.time() - tl
+                # untimed priming: every distinct request of the schedule once, 4 at a time, so each context has grown
                 # its scratch for the largest requests before the measured replay (steady-state serving)
-                subprocess.run([lib_path("gsjd_loadgen"), "--socket", sock, "--schedule", prime], capture_output=True, text=True, timeout=900)
-                r = subprocess.run([lib_path("gsjd_loadgen"), "--socket", sock, "--schedule", sched, "--warmup", str(SERVE_WARMUP)],
-                                   capture_output=True, text=True, timeout=900)
+                subprocess.run([lib_path("gsjd_loadgen"), "--socket", sock, "--schedule", prime], capture_output=True, text=True, timeout=1800)
+                r = subprocess.run([lib_path("gsjd_loadgen"), "--socket", sock, "--schedule", sched, "--warmup", str(cfg["warmup"])],
+                                   capture_output=True, text=True, timeout=3600)
                 res = json.loads(r.stdout.strip().splitlines()[-1])
                 res["rows_per_s"] = res["rows"] / res["span_s"]
+                res["load_s"] = round(load_s, 1)
+                r = subprocess.run([lib_path("gsjd_loadgen"), "--socket", sock, "--schedule", sched, "--closed", str(cfg["closed_clients"]),
+                                    "--duration", str(cfg["closed_s"])], capture_output=True, text=True, timeout=3600)
+                res["saturated"] = json.loads(r.stdout.strip().splitlines()[-1])
                 out[mode] = res
             finally:
                 D.stop(p)
                 log.close()
-        out["config"] = {"resident_parcels": int(ps.n), "rate_per_s": SERVE_RATE, "requests": SERVE_REQUESTS, "warmup_requests": SERVE_WARMUP,
-                         "query_sizes": "log-uniform 1e2-1e5", "mix": "join+area 50%, relate 20%, dwithin 5 m 20%, pip 10%",
-                         "workers": workers, "prep_s": round(prep_s, 1)}
+        out["pairs_per_s_saturated"] = {m: out[m]["saturated"]["rows_per_s"] for m, _ in SERVE_ARMS}
+        out["p99_ratio_plain_over_filtered"] = out["plain"]["p99_ms"] / out["filtered"]["p99_ms"] if out["filtered"]["p99_ms"] else None
+        out["saturated_ratio_filtered_over_plain"] = (out["pairs_per_s_saturated"]["filtered"] / out["pairs_per_s_saturated"]["plain"]
+                                                     if out["pairs_per_s_saturated"]["plain"] else None)
+        out["config"] = {"workload": cfg["name"], "resident_polygons": int(n_res), "resident_vertices": int(nv_res),
+                         "resident_points": cfg["points"], "vertices_per_ring": f"{cfg['vmin']}-{cfg['vmax']} log-uniform",
+                         "box_deg": list(box), "rate_per_s": cfg["rate"], "requests": cfg["requests"], "warmup_requests": cfg["warmup"],
+                         "query_sizes": f"log-uniform {lo:g}-{hi:g} polygons", "query_layers": cfg["queries"],
+                         "query_polygons_total": int(sum(qsizes)),
+                         "mix": "join+area 50%, relate 20%, dwithin 5 m 20%, point in polygon 10% (query polygons x resident points)",
+                         "workers": workers, "closed_clients": cfg["closed_clients"], "closed_s": cfg["closed_s"],
+                         "rows": "rows are pairs (no duplicate geometries in these layers)", "prep_s": round(prep_s, 1)}
         return out
     finally:
         shutil.rmtree(d, ignore_errors=True)
@@ -551,6 +574,7 @@ def main():
     ap.add_argument("--cpu-sample-s", type=float, default=0.0, help="CPU seconds per reference-arm step (0: sized from --steps)")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving-latency leg (gsjd under a Poisson request stream)")
     ap.add_argument("--no-reference-check", action="store_true", help="skip the row-by-row comparison with the reference engine's driver")
+    ap.add_argument("--serve-small", action="store_true", help="the serving leg on a scaled-down copy of its workload (quick runs)")
     ap.add_argument("--op", default="relate", choices=["relate", "area", "dwithin", "erode", "cluster"])
     ap.add_argument("--arms", default="filtered,plain", help="refinement variants an --op run times (filtered first; for profiling one)")
     ap.add_argument("--shard", action="store_true",
@@ -678,7 +702,7 @@ def main():
     lat = sorted(f["ms"])
     serving = None
     if rank == 0 and not args.no_serve:
-        serving = serving_leg(ps)
+        serving = serving_leg(SERVE_SMALL if args.serve_small else SERVE)
     line = {
         "metric": METRIC, "value": value, "unit": "pairs/s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": tot_ms / args.steps, "higher_is_better": True, "scaling": "strong" if shard else "weak", "vs_baseline": None,
@@ -689,7 +713,8 @@ def main():
                    "l2": "inputs > L2 (2.2 GB resident layer)"},
         "gen_s": round(t_gen, 2),
         "latency_ms": ({"p50": serving["filtered"]["p50_ms"], "p99": serving["filtered"]["p99_ms"],
-                        "what": "gsjd serving, arrival to end of result stream"} if serving else None),
+                        "plain_p50": serving["plain"]["p50_ms"], "plain_p99": serving["plain"]["p99_ms"],
+                        "what": "gsjd serving the request stream, arrival to end of result stream"} if serving else None),
         "step_latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
         "serving": serving,
         "plain_fp64": {"value": plain_value, "ms_per_step": plain_ms / args.steps,

@@ -1,9 +1,11 @@
-// gsjd_loadgen: open-loop load generator for the daemon. Replays a schedule of requests (arrival time, op, args)
-// against a gsjd (or gpujoind) socket, one connection per request started at its arrival time, reads every
+// gsjd_loadgen: load generator for the daemon. Replays a schedule of requests (arrival time, op, args) against a
+// gsjd (or gpujoind) socket, one connection per request started at its arrival time (open loop), reads every
 // result stream to its end, and prints a JSON summary of the latencies (arrival to end of stream, so time spent
-// queueing in the daemon counts) and row counts.
+// queueing in the daemon counts) and row counts. With --closed N the arrival times are ignored: N clients each send
+// the schedule's requests in turn (shared order), the next as soon as the previous result stream ended, for
+// --duration seconds, and the summary adds the served rows per second (the daemon at saturation).
 //
-//   gsjd_loadgen --socket PATH [--token TOKEN] --schedule FILE [--warmup N] [--detail FILE]
+//   gsjd_loadgen --socket PATH [--token TOKEN] --schedule FILE [--warmup N] [--detail FILE] [--closed N --duration S]
 //
 // --detail writes one TSV line per request: index, op, first argument (the query layer), arrival s, latency ms
 // (-1 on error), rows, first-row ms (arrival to the first frame header), and the daemon's stats JSON.
@@ -170,11 +172,50 @@ uint32_t op_code(const std::string& s) {
   return it == m.end() ? 0 : it->second;
 }
 
+// closed loop: N clients, each starting the next request of the shared order when its previous one ended
+std::string closed_loop(const std::vector<Req>& reqs, int clients, double duration) {
+  std::atomic<uint64_t> next{0};
+  std::mutex mu;
+  std::vector<double> lat;
+  uint64_t rows = 0, done = 0, errors = 0;
+  std::string first_err;
+  const auto t0 = Clock::now();
+  const auto until = t0 + std::chrono::duration_cast<Clock::duration>(std::chrono::duration<double>(duration));
+  std::vector<std::thread> th;
+  for (int c = 0; c < clients; c++)
+    th.emplace_back([&] {
+      while (Clock::now() < until) {
+        const Req& q = reqs[next.fetch_add(1) % reqs.size()];
+        const Result r = run(q, Clock::now());
+        std::lock_guard<std::mutex> g(mu);
+        if (!r.ok) { errors++; if (first_err.empty()) first_err = r.err; continue; }
+        lat.push_back(r.latency_s);
+        rows += r.rows;
+        done++;
+      }
+    });
+  for (auto& t : th) t.join();
+  const double span = std::chrono::duration<double>(Clock::now() - t0).count();
+  char b[512];
+  snprintf(b, sizeof b, "{\"mode\":\"closed\",\"clients\":%d,\"requests\":%llu,\"errors\":%llu,\"rows\":%llu,\"span_s\":%.6g,"
+           "\"rows_per_s\":%.6g,\"requests_per_s\":%.6g,\"p50_ms\":%.6g,\"p99_ms\":%.6g", clients, (unsigned long long)done,
+           (unsigned long long)errors, (unsigned long long)rows, span, rows / span, done / span, 1e3 * pct(lat, 50), 1e3 * pct(lat, 99));
+  std::string js = b;
+  if (!first_err.empty()) {
+    std::string e;
+    for (char ch : first_err) { if (ch == '"' || ch == '\\') e += '\\'; if ((unsigned char)ch >= 0x20) e += ch; }
+    js += ",\"first_error\":\"" + e + "\"";
+  }
+  return js + "}";
+}
+
 }  // namespace
 
 int main(int argc, char** argv) {
   std::string sched, detail;
   size_t warmup = 0;
+  int closed = 0;
+  double duration = 10.0;
   for (int i = 1; i < argc; i++) {
     const std::string a = argv[i];
     if (a == "--socket" && i + 1 < argc) g_socket = argv[++i];
@@ -182,7 +223,12 @@ int main(int argc, char** argv) {
     else if (a == "--schedule" && i + 1 < argc) sched = argv[++i];
     else if (a == "--warmup" && i + 1 < argc) warmup = (size_t)atol(argv[++i]);
     else if (a == "--detail" && i + 1 < argc) detail = argv[++i];
-    else { fprintf(stderr, "usage: gsjd_loadgen --socket PATH [--token T] --schedule FILE [--warmup N] [--detail FILE]\n"); return 2; }
+    else if (a == "--closed" && i + 1 < argc) closed = atoi(argv[++i]);
+    else if (a == "--duration" && i + 1 < argc) duration = atof(argv[++i]);
+    else {
+      fprintf(stderr, "usage: gsjd_loadgen --socket PATH [--token T] --schedule FILE [--warmup N] [--detail FILE] [--closed N --duration S]\n");
+      return 2;
+    }
   }
   std::ifstream f(sched);
   if (!f) { fprintf(stderr, "cannot read schedule %s\n", sched.c_str()); return 2; }
@@ -200,6 +246,12 @@ int main(int argc, char** argv) {
     if (!q.op) { fprintf(stderr, "unknown op %s\n", col[1].c_str()); return 2; }
     q.args.assign(col.begin() + 2, col.end());
     reqs.push_back(q);
+  }
+  if (reqs.empty()) { fprintf(stderr, "empty schedule\n"); return 2; }
+  if (closed > 0) {
+    const std::string js = closed_loop(reqs, closed, duration);
+    puts(js.c_str());
+    return js.find("\"errors\":0,") == std::string::npos ? 1 : 0;
   }
   std::vector<Result> res(reqs.size());
   std::vector<std::thread> th;

@@ -47,9 +47,14 @@ __global__ void k_prep_points(uint64_t n, const double2* __restrict__ xy, float4
   bb[i] = make_float4(__double2float_rd(p.x), __double2float_rd(p.y), __double2float_ru(p.x), __double2float_ru(p.y));
 }
 
-template <class T> static T* dmalloc(gsj_layer* L, size_t count) {
+// a layer's arrays come from the device's stream-ordered pool (the contexts keep it cached, so re-uploading a layer
+// of the same size allocates nothing new); the upload ends with a stream synchronisation, after which every
+// context's stream may use them
+template <class T> static T* dmalloc(gsj_layer* L, size_t count, cudaStream_t s = nullptr) {
   void* p = nullptr;
-  GSJ_CK(cudaMalloc(&p, std::max<size_t>(count * sizeof(T), 16)));
+  const size_t b = std::max<size_t>(count * sizeof(T), 16);
+  if (s) GSJ_CK(cudaMallocAsync(&p, b, s));
+  else GSJ_CK(cudaMalloc(&p, b));
   L->allocs.push_back(p);
   L->bytes += count * sizeof(T);
   return reinterpret_cast<T*>(p);
@@ -58,6 +63,47 @@ template <class T> static T* dmalloc(gsj_layer* L, size_t count) {
 void layer_free(gsj_layer* L) {
   for (void* p : L->allocs) cudaFree(p);
   L->allocs.clear();
+}
+
+// cut-edge flags (one byte per vertex) packed into bits, one warp per 32 vertices
+__global__ void k_pack_syn(uint64_t nv, const uint8_t* __restrict__ syn, uint32_t* bits) {
+  const uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const unsigned m = __ballot_sync(0xffffffffu, v < nv && syn[v] != 0);
+  if ((threadIdx.x & 31) == 0 && v < nv) bits[v >> 5] = m;
+}
+
+// thread per geometry: 32-bit ring offsets, edge count (the largest goes to *maxe), and the length of its real
+// boundary (edges not made by subdivision) summed edge by edge in ring order from the world coordinates, as the
+// reference's host loop does (engine.cuh:69-82)
+__global__ void k_geom_setup(uint32_t n, const uint64_t* __restrict__ gro, const uint64_t* __restrict__ rvo, const double2* __restrict__ xy,
+                             const uint32_t* __restrict__ synb, uint32_t* gro32, double* glen, unsigned int* maxe) {
+  const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g > n) return;
+  gro32[g] = (uint32_t)gro[g];
+  if (g == n) return;
+  uint64_t e = 0;
+  double len = 0;
+  for (uint64_t r = gro[g]; r < gro[g + 1]; r++) {
+    const uint64_t v0 = rvo[r], v1 = rvo[r + 1];
+    e += v1 > v0 ? v1 - v0 - 1 : 0;
+    for (uint64_t v = v0; v + 1 < v1; v++) {
+      if (synb && ((synb[v >> 5] >> (v & 31)) & 1u)) continue;
+      const double2 p = xy[v], q = xy[v + 1];
+      len += hypot(q.x - p.x, q.y - p.y);
+    }
+  }
+  glen[g] = len;
+  atomicMax(maxe, (unsigned int)(e < 0xFFFFFFFFull ? e : 0xFFFFFFFFull));
+}
+
+// per parent geometry: its pieces' lengths summed in piece order (pieces of a parent are contiguous)
+__global__ void k_parent_len(uint32_t n, const uint32_t* __restrict__ parent, const double* __restrict__ glen, double* blen) {
+  const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= n || (g > 0 && parent[g] == parent[g - 1])) return;
+  const uint32_t p = parent[g];
+  double s = 0;
+  for (uint32_t h = g; h < n && parent[h] == p; h++) s += glen[h];
+  blen[p] = s;
 }
 
 void layer_upload_polygons(gsj_ctx* c, uint64_t n, uint64_t nr, uint64_t nv, const uint64_t* gro, const uint64_t* rvo, const double* xy,
@@ -77,73 +123,56 @@ void layer_upload_polygons(gsj_ctx* c, uint64_t n, uint64_t nr, uint64_t nv, con
   if (bad_g) throw Error(GSJ_ERR_ARG, "gro must be non-decreasing");
   if (bad_r) throw Error(GSJ_ERR_ARG, "rvo must be non-decreasing");
   if (bad_p) throw Error(GSJ_ERR_ARG, "parent must be non-decreasing");
-  // real boundary length per geometry for relate (engine.cuh:69-82): host std::hypot, as the reference; computed
-  // on a helper thread while the arrays are copied and the LBVH is built
-  std::vector<double> glen(n, 0.0);
-  std::thread glen_th([&] {
-#pragma omp parallel for schedule(dynamic, 4096)
-    for (int64_t g = 0; g < (int64_t)n; g++) {
-      double len = 0;
-      for (uint64_t r = gro[g]; r < gro[g + 1]; r++)
-        for (uint64_t v = rvo[r]; v + 1 < rvo[r + 1]; v++)
-          if (!syn || !syn[v]) len += std::hypot(xy[2 * v + 2] - xy[2 * v], xy[2 * v + 3] - xy[2 * v + 1]);
-      glen[g] = len;
-    }
-  });
-  struct Joiner { std::thread& t; ~Joiner() { if (t.joinable()) t.join(); } } glen_join{glen_th};   // also on an exception
   L->is_points = 0;
   L->d.n = (uint32_t)n; L->d.nr = (uint32_t)nr; L->d.nv = nv;
   cudaStream_t s = c->stream;
-  std::vector<uint32_t> gro32(n + 1);
-  uint32_t maxe = 0;
-#pragma omp parallel for reduction(max : maxe) schedule(static)
-  for (int64_t g = 0; g <= (int64_t)n; g++) {
-    gro32[g] = (uint32_t)gro[g];
-    if (g < (int64_t)n) {
-      uint64_t e = 0;
-      for (uint64_t r = gro[g]; r < gro[g + 1]; r++) e += rvo[r + 1] > rvo[r] ? rvo[r + 1] - rvo[r] - 1 : 0;
-      maxe = std::max<uint32_t>(maxe, (uint32_t)std::min<uint64_t>(e, 0xFFFFFFFFu));
-    }
-  }
-  L->max_geom_edges = maxe;
-  uint32_t* d_gro = dmalloc<uint32_t>(L, n + 1);
-  uint64_t* d_rvo = dmalloc<uint64_t>(L, nr + 1);
-  double2* d_xy = dmalloc<double2>(L, nv);
-  double2* d_origin = dmalloc<double2>(L, n);
-  double2* d_ext = dmalloc<double2>(L, n);
-  float4* d_bb = dmalloc<float4>(L, n);
-  GSJ_CK(cudaMemcpyAsync(d_gro, gro32.data(), (n + 1) * 4, cudaMemcpyHostToDevice, s));
+  const uint32_t np = parent ? parent[n - 1] + 1 : (uint32_t)n;
+  L->nparent = np;
+  // every copy starts from the caller's arrays; the rest of the preparation runs on the device
+  uint32_t* d_gro = dmalloc<uint32_t>(L, n + 1, s);
+  uint64_t* d_rvo = dmalloc<uint64_t>(L, nr + 1, s);
+  double2* d_xy = dmalloc<double2>(L, nv, s);
+  double2* d_origin = dmalloc<double2>(L, n, s);
+  double2* d_ext = dmalloc<double2>(L, n, s);
+  float4* d_bb = dmalloc<float4>(L, n, s);
+  double* d_len = dmalloc<double>(L, n, s);   // per geometry; also the per-parent lengths of a layer without parents
+  DevBuf t_gro, t_syn, t_max;
+  t_gro.s = t_syn.s = t_max.s = s;
+  uint64_t* d_gro64 = t_gro.as<uint64_t>(n + 1);
+  unsigned int* d_maxe = t_max.as<unsigned int>(1);
+  GSJ_CK(cudaMemcpyAsync(d_gro64, gro, (n + 1) * 8, cudaMemcpyHostToDevice, s));
   GSJ_CK(cudaMemcpyAsync(d_rvo, rvo, (nr + 1) * 8, cudaMemcpyHostToDevice, s));
   GSJ_CK(cudaMemcpyAsync(d_xy, xy, nv * 16, cudaMemcpyHostToDevice, s));
-  k_prep_polygons<<<grid_for((uint64_t)n * 32, 256), 256, 0, s>>>((uint32_t)n, d_gro, d_rvo, d_xy, d_origin, d_ext, d_bb);
+  GSJ_CK(cudaMemsetAsync(d_maxe, 0, 4, s));
+  uint32_t* d_synb = nullptr;
+  if (syn) {
+    uint8_t* d_syn8 = t_syn.as<uint8_t>(nv);
+    GSJ_CK(cudaMemcpyAsync(d_syn8, syn, nv, cudaMemcpyHostToDevice, s));
+    d_synb = dmalloc<uint32_t>(L, (nv + 31) / 32, s);
+    k_pack_syn<<<grid_for(nv, 256), 256, 0, s>>>(nv, d_syn8, d_synb); c->launches++;
+    L->d.synb = d_synb;
+  }
+  k_geom_setup<<<grid_for(n + 1, 128), 128, 0, s>>>((uint32_t)n, d_gro64, d_rvo, d_xy, d_synb, d_gro, d_len, d_maxe); c->launches++;
+  k_prep_polygons<<<grid_for((uint64_t)n * 32, 256), 256, 0, s>>>((uint32_t)n, d_gro, d_rvo, d_xy, d_origin, d_ext, d_bb); c->launches++;
   GSJ_CK(cudaGetLastError());
   L->d.gro = d_gro; L->d.rvo = d_rvo; L->d.xy = d_xy; L->d.origin = d_origin; L->d.ext = d_ext; L->d.bb = d_bb;
-  uint32_t np = parent ? parent[n - 1] + 1 : (uint32_t)n;
-  L->nparent = np;
-  std::vector<uint32_t> bits;
-  if (syn) {
-    bits.assign((nv + 31) / 32, 0);
-    for (uint64_t v = 0; v < nv; v++) if (syn[v]) bits[v >> 5] |= 1u << (v & 31);
-    uint32_t* d_syn = dmalloc<uint32_t>(L, bits.size());
-    GSJ_CK(cudaMemcpyAsync(d_syn, bits.data(), bits.size() * 4, cudaMemcpyHostToDevice, s));
-    L->d.synb = d_syn;
-  }
   if (parent) {
-    uint32_t* d_par = dmalloc<uint32_t>(L, n);
+    uint32_t* d_par = dmalloc<uint32_t>(L, n, s);
     GSJ_CK(cudaMemcpyAsync(d_par, parent, n * 4, cudaMemcpyHostToDevice, s));
     L->d.parent = d_par;
     L->h_parent.assign(parent, parent + n);
+    double* d_blen = dmalloc<double>(L, np, s);
+    GSJ_CK(cudaMemsetAsync(d_blen, 0, (size_t)np * 8, s));
+    k_parent_len<<<grid_for(n, 256), 256, 0, s>>>((uint32_t)n, d_par, d_len, d_blen); c->launches++;
+    L->d.blen = d_blen;
+  } else {
+    L->d.blen = d_len;
   }
-  // host staging vectors above are released at return: the copies must have finished
-  GSJ_CK(cudaStreamSynchronize(s));
   build_bvh(c, L);
-  glen_th.join();
-  std::vector<double> bl(np, 0.0);   // per parent, pieces in order (the reference's summation order)
-  for (uint64_t g = 0; g < n; g++) bl[parent ? parent[g] : g] += glen[g];
-  double* d_blen = dmalloc<double>(L, np);
-  GSJ_CK(cudaMemcpyAsync(d_blen, bl.data(), np * 8, cudaMemcpyHostToDevice, s));
-  L->d.blen = d_blen;
-  GSJ_CK(cudaStreamSynchronize(s));
+  unsigned int* h = c->h_counters.as<unsigned int>(1);
+  GSJ_CK(cudaMemcpyAsync(h, d_maxe, 4, cudaMemcpyDeviceToHost, s));
+  GSJ_CK(cudaStreamSynchronize(s));   // the caller's arrays may go when this returns; other streams may use the layer
+  L->max_geom_edges = h[0];
 }
 
 void layer_upload_points(gsj_ctx* c, uint64_t n, const double* xy, gsj_layer* L) {
@@ -152,13 +181,14 @@ void layer_upload_points(gsj_ctx* c, uint64_t n, const double* xy, gsj_layer* L)
   cudaStream_t s = c->stream;
   L->is_points = 1;
   L->d.n = (uint32_t)n; L->d.nv = n; L->nparent = (uint32_t)n;
-  double2* d_xy = dmalloc<double2>(L, n);
-  float4* d_bb = dmalloc<float4>(L, n);
+  double2* d_xy = dmalloc<double2>(L, n, s);
+  float4* d_bb = dmalloc<float4>(L, n, s);
   GSJ_CK(cudaMemcpyAsync(d_xy, xy, n * 16, cudaMemcpyHostToDevice, s));
-  k_prep_points<<<grid_for(n, 256), 256, 0, s>>>(n, d_xy, d_bb);
+  k_prep_points<<<grid_for(n, 256), 256, 0, s>>>(n, d_xy, d_bb); c->launches++;
   GSJ_CK(cudaGetLastError());
   L->d.xy = d_xy; L->d.bb = d_bb; L->pts = d_xy;
   build_bvh(c, L);
+  GSJ_CK(cudaStreamSynchronize(s));   // the caller's array may go when this returns; other streams may use the layer
 }
 
 // ---- LBVH ---------------------------------------------------------------------------------------------------
@@ -260,8 +290,8 @@ __global__ void k_single_leaf(const float4* bb, BNode* nodes, uint32_t* order) {
 void build_bvh(gsj_ctx* c, gsj_layer* L) {
   cudaStream_t s = c->stream;
   const int n = (int)L->d.n;
-  BNode* nodes = dmalloc<BNode>(L, std::max(n - 1, 1));
-  uint32_t* order = dmalloc<uint32_t>(L, n);
+  BNode* nodes = dmalloc<BNode>(L, std::max(n - 1, 1), s);
+  uint32_t* order = dmalloc<uint32_t>(L, n, s);
   L->bvh.nodes = nodes; L->bvh.order = order; L->bvh.n = (uint32_t)n;
   if (n == 1) {
     k_single_leaf<<<1, 1, 0, s>>>(L->d.bb, nodes, order);
@@ -269,12 +299,15 @@ void build_bvh(gsj_ctx* c, gsj_layer* L) {
     GSJ_CK(cudaStreamSynchronize(s));
     return;
   }
-  DevBuf keys, keys2, tmp, par, flags, nbb, cmm;
+  DevBuf keys, keys2, tmp, par, flags, nbb, cmm;   // stream-ordered temporaries: freed behind the build on the stream
+  for (DevBuf* b : {&keys, &keys2, &tmp, &par, &flags, &nbb, &cmm}) b->s = s;
   int* d_cmm = cmm.as<int>(4);
   int init[4];
   { auto ord = [](float f) { int i; memcpy(&i, &f, 4); return i >= 0 ? i : i ^ 0x7FFFFFFF; };
     init[0] = init[1] = ord(INFINITY); init[2] = init[3] = ord(-INFINITY); }
-  GSJ_CK(cudaMemcpyAsync(d_cmm, init, 16, cudaMemcpyHostToDevice, s));
+  int* h_init = c->h_counters.as<int>(4);   // pinned: the copy may still be pending when this returns
+  memcpy(h_init, init, 16);
+  GSJ_CK(cudaMemcpyAsync(d_cmm, h_init, 16, cudaMemcpyHostToDevice, s));
   k_centroid_bounds<<<std::min(grid_for(n, 256), c->sm_count * 8), 256, 0, s>>>(L->d.bb, n, d_cmm);
   unsigned long long* k1 = keys.as<unsigned long long>(n);
   unsigned long long* k2 = keys2.as<unsigned long long>(n);
@@ -291,8 +324,8 @@ void build_bvh(gsj_ctx* c, gsj_layer* L) {
   float4* d_nbb = nbb.as<float4>(n);
   k_karras<<<grid_for(n, 256), 256, 0, s>>>(k2, n, nodes, par_int, par_leaf, order);
   k_refit<<<grid_for(n, 256), 256, 0, s>>>(n, L->d.bb, nodes, d_nbb, par_int, par_leaf, d_flags);
+  c->launches += 4;
   GSJ_CK(cudaGetLastError());
-  GSJ_CK(cudaStreamSynchronize(s));
 }
 
 }  // namespace gsj

@@ -207,16 +207,27 @@ def test_reference_golden_rows(env):
     assert max(abs(got[k] - want[k]) / abs(want[k]) for k in big) <= 1e-9
 
 
+def same_value(a, b):
+    """Row payloads equal bit for bit (areas as float64 words, NaN for rows without an area; DE-9IM strings)."""
+    if isinstance(a, float) and isinstance(b, float):
+        return struct.pack("<d", a) == struct.pack("<d", b) or (math.isnan(a) and math.isnan(b))
+    return a == b
+
+
 def test_concurrent_requests(env):
+    """Each result is the same alone and in the mix: the same rows with the same areas and DE-9IM matrices, bit for
+    bit, whether a request runs by itself or while 15 others of every kind run on the device beside it."""
     calls = [lambda: env.cl.join("parcels", "parcels2", True, "all"), lambda: env.cl.relate("parcels", "parcels", "", "distinct"),
-             lambda: env.cl.dwithin("parcels", "parcels2", 5.0), lambda: env.cl.join("points", "parcels", False)]
+             lambda: env.cl.dwithin("parcels", "parcels2", 5.0), lambda: env.cl.join("points", "parcels", False),
+             lambda: env.cl.relate("parcels", "parcels2", "", "all"), lambda: env.cl.join("parcels2", "parcels", True, "all")]
     serial = [rowset(f()[0]) for f in calls]
-    with cf.ThreadPoolExecutor(8) as ex:
-        futs = [ex.submit(calls[i % 4]) for i in range(16)]
+    assert all(len(r) > 0 for r in serial)
+    with cf.ThreadPoolExecutor(12) as ex:
+        futs = [ex.submit(calls[i % len(calls)]) for i in range(4 * len(calls))]
         for i, f in enumerate(futs):
-            got = rowset(f.result()[0])
-            ref = serial[i % 4]
+            got, ref = rowset(f.result()[0]), serial[i % len(calls)]
             assert got.keys() == ref.keys()
+            assert all(same_value(got[k], ref[k]) for k in ref)
 
 
 def test_client_gone_and_drop(env):
