@@ -541,6 +541,10 @@ def run_reference(args, rank, ws):
         gen.write_gset(g, ps)
         with Clocks(0) as clk:
             rs = [RH.run([g, g, "--relate"], reps=2) for _ in range(runs)]
+    except (RuntimeError, OSError, subprocess.TimeoutExpired) as e:   # e.g. no usable CUDA device for the driver
+        why = str(e).strip().splitlines()[-1][:300] if str(e).strip() else type(e).__name__
+        print(json.dumps({"impl": "reference", "unavailable": f"the reference engine's driver did not run: {why}"}), flush=True)
+        return
     finally:
         shutil.rmtree(d, ignore_errors=True)
     gms = [RH.gpu_ms(r) for r in rs]
