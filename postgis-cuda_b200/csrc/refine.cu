@@ -384,11 +384,13 @@ __device__ bool refine_pair_t(const DLayer& P, const DLayer& R, uint32_t a, uint
   G.cy = (double)(G.ov.y0 + 0.414213 * (G.ov.y1 - G.ov.y0));
   int na = 0, nb = 0;
   bool inB_c = false, inA_c = false;
-  for (int side = 0; side < 2; side++) {   // one inlined copy of the gather
-    bool in = false;
-    // MASK: the containment parity of the probe point c is taken in the gather's pass over each polygon's edges
-    const int n = collect<F, MASK>(side ? B : A, G.ov, side ? LB : LA, cap, lane, G.cx, G.cy, &in);
-    if (side) { nb = n; inB_c = in; } else { na = n; inA_c = in; }
+  if constexpr (MASK) {   // both polygons in one pass, with the containment parity of the probe point c
+    collect_both<F>(A, B, G.ov, LA, LB, cap, lane, G.cx, G.cy, na, nb, inA_c, inB_c);
+  } else {
+    for (int side = 0; side < 2; side++) {   // one inlined copy of the gather
+      const int n = collect<F>(side ? B : A, G.ov, side ? LB : LA, cap, lane);
+      if (side) nb = n; else na = n;
+    }
   }
   if (na > cap || nb > cap) return false;
   __syncwarp();
