@@ -71,6 +71,43 @@ __device__ __forceinline__ bool seg_isect(double p0x, double p0y, double p1x, do
   return false;
 }
 
+// ---- FP32 sign filters with certified bounds (the filtered variant's optional first stage) -----------------------
+// Sign of orient(a, b, c) exactly as the FP64 routine above computes it. The FP64 differences are rounded to float
+// (relative error <= u = 2^-24 each) and det = fa*fb - fc*fd is formed in FP32; |det - (ab - cd)| <= 4.0000005 u
+// (|p| + |q|) for the float products p, q (normal floats: |p|, |q| >= 1e-30 with differences below 720 degrees), so
+// |det| > 6 u (|p| + |q|) fixes the sign of ab - cd, far outside the FP64 routine's own error (<= 2^-52 (|ab| + |cd|)),
+// hence the sign the FP64 routine returns. Otherwise (near-degenerate or exact zeros) the FP64 routine decides.
+__device__ __forceinline__ int orient_sign32(double ax, double ay, double bx, double by, double cx, double cy) {
+  const double a = bx - ax, b = cy - ay, c = by - ay, d = cx - ax;
+  const float p = __double2float_rn(a) * __double2float_rn(b), q = __double2float_rn(c) * __double2float_rn(d);
+  const float ap = fabsf(p), aq = fabsf(q);
+  if (ap >= 1e-30f && aq >= 1e-30f) {
+    const float det = p - q, bound = 3.6e-7f * (ap + aq);
+    if (det > bound) return 1;
+    if (det < -bound) return -1;
+  }
+  const double o = orient(ax, ay, bx, by, cx, cy);
+  return o > 0 ? 1 : (o < 0 ? -1 : 0);
+}
+// left_of and seg_isect on the filtered signs: the same booleans as the FP64 forms
+__device__ __forceinline__ bool left_of32(double ax, double ay, double bx, double by, double px, double py) {
+  const int o = orient_sign32(ax, ay, bx, by, px, py);
+  if (o != 0) return o > 0;
+  double dy = by - ay;
+  if (dy != 0) return dy < 0;
+  return bx > ax;
+}
+__device__ __forceinline__ bool seg_isect32(double p0x, double p0y, double p1x, double p1y, double q0x, double q0y, double q1x, double q1y) {
+  const int d1 = orient_sign32(q0x, q0y, q1x, q1y, p0x, p0y), d2 = orient_sign32(q0x, q0y, q1x, q1y, p1x, p1y);
+  const int d3 = orient_sign32(p0x, p0y, p1x, p1y, q0x, q0y), d4 = orient_sign32(p0x, p0y, p1x, p1y, q1x, q1y);
+  if (d1 * d2 < 0 && d3 * d4 < 0) return true;
+  if (d1 == 0 && onseg(q0x, q0y, q1x, q1y, p0x, p0y)) return true;
+  if (d2 == 0 && onseg(q0x, q0y, q1x, q1y, p1x, p1y)) return true;
+  if (d3 == 0 && onseg(p0x, p0y, p1x, p1y, q0x, q0y)) return true;
+  if (d4 == 0 && onseg(p0x, p0y, p1x, p1y, q1x, q1y)) return true;
+  return false;
+}
+
 // A geometry seen in a pair frame: world = shx + stored x.
 struct Frame {
   const DLayer* L; uint32_t r0, r1; double shx, shy;

@@ -24,7 +24,7 @@ __device__ __forceinline__ bool edge_outside(double px, double py, double qx, do
 // all edges of geometry A meeting the overlap box, compacted in ring order with a warp ballot (engine.cuh:358-377).
 // PIP: the same pass also takes the crossing parity of the segment (A's bbox left edge - 1, my) -> (mx, my) over
 // every edge of A, as pip_full_warp does (an XOR over the edges, so the order is free), into *inside.
-template <bool F, bool PIP = false>
+template <bool F, bool PIP = false, bool S32 = false>
 static __device__ int collect(const Frame& A, const Box& ov, EList L, int cap, int lane, double mx = 0, double my = 0, bool* inside = nullptr) {
   const DLayer& S = *A.L;
   const unsigned lt = (1u << lane) - 1;
@@ -44,10 +44,18 @@ static __device__ int collect(const Frame& A, const Box& ov, EList L, int cap, i
         }
         in = F ? !out_cmp(x0, y0, x1, y1, ov.x0, ov.y0, ov.x1, ov.y1) : !edge_outside(x0, y0, x1, y1, ov);
         if (PIP && !((y0 > my) == (y1 > my) && y0 != my && y1 != my)) {
-          const bool so = left_of(x0, y0, x1, y1, ox, oy), sc = left_of(x0, y0, x1, y1, mx, my);
-          if (so != sc) {
-            const bool su = orient(ox, oy, mx, my, x0, y0) > 0, sv = orient(ox, oy, mx, my, x1, y1) > 0;
-            if (su != sv) par = !par;
+          if (S32) {   // the same signs through the certified FP32 filter
+            const bool so = left_of32(x0, y0, x1, y1, ox, oy), sc = left_of32(x0, y0, x1, y1, mx, my);
+            if (so != sc) {
+              const bool su = orient_sign32(ox, oy, mx, my, x0, y0) > 0, sv = orient_sign32(ox, oy, mx, my, x1, y1) > 0;
+              if (su != sv) par = !par;
+            }
+          } else {
+            const bool so = left_of(x0, y0, x1, y1, ox, oy), sc = left_of(x0, y0, x1, y1, mx, my);
+            if (so != sc) {
+              const bool su = orient(ox, oy, mx, my, x0, y0) > 0, sv = orient(ox, oy, mx, my, x1, y1) > 0;
+              if (su != sv) par = !par;
+            }
           }
         }
       }
@@ -61,72 +69,6 @@ static __device__ int collect(const Frame& A, const Box& ov, EList L, int cap, i
   }
   if (PIP) *inside = (__popc(__ballot_sync(0xffffffffu, par)) & 1) != 0;
   return cnt;
-}
-
-// Both geometries of a pair at once: each iteration a lane takes one edge of A and one of B (32 of each per
-// iteration), so the two polygons' load chains are in flight together; each list is compacted in ring order with its
-// own ballot, and each polygon's crossing parity for the probe point (mx, my) is taken in the same pass, as collect
-// does for one geometry. Returns the counts in na / nb (a count above cap: that list was not fully kept).
-struct RingWalk {   // the warp's position in one geometry's rings (the same in every lane)
-  uint32_t r, r1; uint64_t s, e, base; bool done;
-  __device__ __forceinline__ void start(const Frame& G) {
-    const DLayer& S = *G.L;
-    r = G.r0; r1 = G.r1; done = r >= r1; s = e = base = 0;
-    if (!done) { s = S.rvo[r]; e = S.rvo[r + 1]; base = s; }
-    skip(G);
-  }
-  __device__ __forceinline__ void skip(const Frame& G) {   // to the next ring with an edge left
-    const DLayer& S = *G.L;
-    while (!done && base + 1 >= e) {
-      if (++r >= r1) { done = true; break; }
-      s = S.rvo[r]; e = S.rvo[r + 1]; base = s;
-    }
-  }
-};
-template <bool F>
-__device__ __forceinline__ bool take_edge(const Frame& G, const RingWalk& w, const Box& ov, int lane, double mx, double my, bool& par,
-                                          double& x0, double& y0, double& x1, double& y1, uint32_t& fl) {
-  if (w.done) return false;
-  const DLayer& S = *G.L;
-  const uint64_t i = w.base + lane, s = w.s, e = w.e;
-  if (i + 1 >= e) return false;
-  G.v(i, x0, y0); G.v(i + 1, x1, y1);
-  fl = 0;
-  if (S.synb) fl = (uint32_t)S.syn(i) | (S.syn(i > s ? i - 1 : e - 2) ? 2u : 0u) | (S.syn(i + 2 < e ? i + 1 : s) ? 4u : 0u);
-  if (!((y0 > my) == (y1 > my) && y0 != my && y1 != my)) {
-    const double ox = G.shx - (double)1, oy = my;
-    const bool so = left_of(x0, y0, x1, y1, ox, oy), sc = left_of(x0, y0, x1, y1, mx, my);
-    if (so != sc) {
-      const bool su = orient(ox, oy, mx, my, x0, y0) > 0, sv = orient(ox, oy, mx, my, x1, y1) > 0;
-      if (su != sv) par = !par;
-    }
-  }
-  return F ? !out_cmp(x0, y0, x1, y1, ov.x0, ov.y0, ov.x1, ov.y1) : !edge_outside(x0, y0, x1, y1, ov);
-}
-template <bool F>
-static __device__ void collect_both(const Frame& A, const Frame& B, const Box& ov, EList LA, EList LB, int cap, int lane, double mx, double my,
-                                    int& na, int& nb, bool& inA, bool& inB) {
-  const unsigned lt = (1u << lane) - 1;
-  RingWalk wa, wb;
-  wa.start(A); wb.start(B);
-  bool pa = false, pb = false;
-  int ca = 0, cb = 0;
-  while (!wa.done || !wb.done) {
-    double ax0 = 0, ay0 = 0, ax1 = 0, ay1 = 0, bx0 = 0, by0 = 0, bx1 = 0, by1 = 0;
-    uint32_t fa = 0, fb = 0;
-    const bool ka = take_edge<F>(A, wa, ov, lane, mx, my, pa, ax0, ay0, ax1, ay1, fa);
-    const bool kb = take_edge<F>(B, wb, ov, lane, mx, my, pb, bx0, by0, bx1, by1, fb);
-    const unsigned ma = __ballot_sync(0xffffffffu, ka), mb = __ballot_sync(0xffffffffu, kb);
-    const int qa = ca + __popc(ma & lt), qb = cb + __popc(mb & lt);
-    if (ka && qa < cap) { LA.x0[qa] = ax0; LA.y0[qa] = ay0; LA.x1[qa] = ax1; LA.y1[qa] = ay1; LA.fl[qa] = fa; }
-    if (kb && qb < cap) { LB.x0[qb] = bx0; LB.y0[qb] = by0; LB.x1[qb] = bx1; LB.y1[qb] = by1; LB.fl[qb] = fb; }
-    ca += __popc(ma); cb += __popc(mb);
-    if (!wa.done) { wa.base += 32; wa.skip(A); }
-    if (!wb.done) { wb.base += 32; wb.skip(B); }
-  }
-  na = ca; nb = cb;
-  inA = (__popc(__ballot_sync(0xffffffffu, pa)) & 1) != 0;
-  inB = (__popc(__ballot_sync(0xffffffffu, pb)) & 1) != 0;
 }
 
 // crossing parity of segment (B's bbox left edge - 1, my) -> (mx, my) over all of B's edges (engine.cuh:382-397)

@@ -367,7 +367,7 @@ __device__ __forceinline__ double pair_snap(double2 oa, double2 ea) {   // engin
 // MASK (the filtered shared-memory kernel): candidate edge pairs as bit masks (mb).
 // FLAT (the filtered scratch kernel): candidate lists in global scratch; a pair whose list would exceed fb->cap is
 // handed back (false) and runs with the full sweeps.
-template <bool F, bool FLAT = false, bool BUCKETS = false, bool MASK = false>
+template <bool F, bool FLAT = false, bool BUCKETS = false, bool MASK = false, bool S32 = false>
 __device__ bool refine_pair_t(const DLayer& P, const DLayer& R, uint32_t a, uint32_t b, const RefineArgs& rp, EList LA, EList LB, int cap,
                               int lane, uint8_t& o_flag, double& o_area, double4& o_ev, uint32_t& o_evb, const FlatBuf* fb = nullptr,
                               const MaskBuf* mb = nullptr, unsigned long long* ep = nullptr) {
@@ -384,13 +384,11 @@ __device__ bool refine_pair_t(const DLayer& P, const DLayer& R, uint32_t a, uint
   G.cy = (double)(G.ov.y0 + 0.414213 * (G.ov.y1 - G.ov.y0));
   int na = 0, nb = 0;
   bool inB_c = false, inA_c = false;
-  if constexpr (MASK) {   // both polygons in one pass, with the containment parity of the probe point c
-    collect_both<F>(A, B, G.ov, LA, LB, cap, lane, G.cx, G.cy, na, nb, inA_c, inB_c);
-  } else {
-    for (int side = 0; side < 2; side++) {   // one inlined copy of the gather
-      const int n = collect<F>(side ? B : A, G.ov, side ? LB : LA, cap, lane);
-      if (side) nb = n; else na = n;
-    }
+  for (int side = 0; side < 2; side++) {   // one inlined copy of the gather
+    bool in = false;
+    // MASK: the containment parity of the probe point c is taken in the gather's pass over each polygon's edges
+    const int n = collect<F, MASK, S32>(side ? B : A, G.ov, side ? LB : LA, cap, lane, G.cx, G.cy, &in);
+    if (side) { nb = n; inB_c = in; } else { na = n; inA_c = in; }
   }
   if (na > cap || nb > cap) return false;
   __syncwarp();
@@ -439,7 +437,8 @@ __device__ bool refine_pair_t(const DLayer& P, const DLayer& R, uint32_t a, uint
         if (!__any_sync(0xffffffffu, j >= 0)) break;
         if (j >= 0) {
           const double qx0 = LB.x0[j], qy0 = LB.y0[j], qx1 = LB.x1[j], qy1 = LB.y1[j];
-          if (!out_cmp(qx0, qy0, qx1, qy1, ax0, ay0, ax1, ay1) && seg_isect(px0, py0, px1, py1, qx0, qy0, qx1, qy1)) {
+          if (!out_cmp(qx0, qy0, qx1, qy1, ax0, ay0, ax1, ay1) &&
+              (S32 ? seg_isect32(px0, py0, px1, py1, qx0, qy0, qx1, qy1) : seg_isect(px0, py0, px1, py1, qx0, qy0, qx1, qy1))) {
             hit_any = true;
             if (!((fa | LB.fl[j]) & 1u)) hit = true;
           }
@@ -591,7 +590,8 @@ template <> struct Cfg<true> { static constexpr int cap = CAP_F; static constexp
 template <bool F>
 __device__ __forceinline__ EList carve_t(unsigned char* base, int cap) { return F ? carve_f(base, cap) : carve(base, cap); }
 
-template <bool F>
+// S32 (filtered only): the contact test's and the gather's orientation signs through the certified FP32 filter
+template <bool F, bool S32 = false>
 __global__ void __launch_bounds__(RB_WARPS * 32, Cfg<F>::minb) k_refine(DLayer P, DLayer R, const uint2* __restrict__ pairs, uint64_t np,
                                                                         RefineArgs rp, uint8_t* flag, double* area, double4* ev, uint32_t* evb,
                                                                         uint32_t* heavy, unsigned long long* nheavy, unsigned long long* next,
@@ -612,7 +612,7 @@ __global__ void __launch_bounds__(RB_WARPS * 32, Cfg<F>::minb) k_refine(DLayer P
   auto one = [&](uint64_t p) {
     const uint2 pr = pairs[p];
     uint8_t f; double ar; double4 e4; uint32_t b4;
-    const bool ok = refine_pair_t<F, false, false, F>(P, R, pr.x, pr.y, rp, LA, LB, Cfg<F>::cap, lane, f, ar, e4, b4, nullptr, &mbuf, &s_ep[wib]);
+    const bool ok = refine_pair_t<F, false, false, F, S32>(P, R, pr.x, pr.y, rp, LA, LB, Cfg<F>::cap, lane, f, ar, e4, b4, nullptr, &mbuf, &s_ep[wib]);
     if (lane == 0) {
       if (!ok) { heavy[atomicAdd(nheavy, 1ull)] = (uint32_t)p; flag[p] = 0; }
       else {
@@ -653,7 +653,8 @@ __host__ __device__ constexpr size_t scratch_per_warp(int cap, int cph) {
 template <bool F>
 __global__ void __launch_bounds__(128) k_refine_scratch(DLayer P, DLayer R, const uint2* __restrict__ pairs, const uint32_t* __restrict__ heavy,
                                                        uint64_t nh, RefineArgs rp, uint8_t* flag, double* area, double4* ev, uint32_t* evb,
-                                                       unsigned char* scratch, int cap, int cph, int* err, unsigned long long* epairs) {
+                                                       unsigned char* scratch, int cap, int cph, int* err, unsigned long long* epairs,
+                                                       unsigned long long* next) {
   const int lane = threadIdx.x & 31;
   unsigned long long ep = 0;
   const uint64_t w = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
@@ -670,7 +671,12 @@ __global__ void __launch_bounds__(128) k_refine_scratch(DLayer P, DLayer R, cons
     fb.cap = cph;
     fb.blcap = 2 * cap + 64;
   }
-  for (uint64_t h = w; h < nh; h += nw) {
+  (void)nw;
+  for (;;) {   // one listed pair at a time from a counter: their costs vary widely
+    unsigned long long h = 0;
+    if (lane == 0) h = atomicAdd(next, 1ull);
+    h = __shfl_sync(0xffffffffu, h, 0);
+    if (h >= nh) break;
     const uint32_t p = heavy[h];
     const uint2 pr = pairs[p];
     uint8_t f; double ar; double4 e4; uint32_t b4;
@@ -694,17 +700,18 @@ __global__ void __launch_bounds__(128) k_refine_scratch(DLayer P, DLayer R, cons
   if (lane == 0 && ep) atomicAdd(epairs, ep);
 }
 
-template <bool F>
+template <bool F, bool S32 = false>
 static uint64_t refine_t(gsj_ctx* c, const gsj_layer* P, const gsj_layer* R, const uint2* pairs, uint64_t np, const RefineArgs& rp, uint8_t* flag,
                          double* area, double4* ev, uint32_t* evb) {
   cudaStream_t s = c->stream;
-  if (!(c->refine_attr & (F ? 2 : 1))) {
-    GSJ_CK(cudaFuncSetAttribute(k_refine<F>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cfg<F>::smem));
-    c->refine_attr |= F ? 2 : 1;
+  const int bit = S32 ? 4 : (F ? 2 : 1);
+  if (!(c->refine_attr & bit)) {
+    GSJ_CK(cudaFuncSetAttribute(k_refine<F, S32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cfg<F>::smem));
+    c->refine_attr |= bit;
   }
   unsigned long long* ctr = c->counters.as<unsigned long long>(8);
   int* err = reinterpret_cast<int*>(ctr + 1);
-  GSJ_CK(cudaMemsetAsync(ctr, 0, 32, s));   // heavy count, error word, pair counter, local edge pairs
+  GSJ_CK(cudaMemsetAsync(ctr, 0, 40, s));   // heavy count, error word, pair counter, local edge pairs, scratch pair counter
   uint32_t* heavy = c->heavy.as<uint32_t>(np);
   int blocks;
   if constexpr (F) {   // enough warps to cover every pair with REFINE_RUNS fetches each, spread over all SMs
@@ -715,7 +722,7 @@ static uint64_t refine_t(gsj_ctx* c, const gsj_layer* P, const gsj_layer* R, con
   } else {
     blocks = (int)std::min<uint64_t>((np + RB_WARPS - 1) / RB_WARPS, (uint64_t)c->sm_count * 8);
   }
-  k_refine<F><<<blocks, RB_WARPS * 32, Cfg<F>::smem, s>>>(P->d, R->d, pairs, np, rp, flag, area, ev, evb, heavy, ctr, ctr + 2, ctr + 3);
+  k_refine<F, S32><<<blocks, RB_WARPS * 32, Cfg<F>::smem, s>>>(P->d, R->d, pairs, np, rp, flag, area, ev, evb, heavy, ctr, ctr + 2, ctr + 3);
   c->launches++;
   GSJ_CK(cudaGetLastError());
   unsigned long long* h = c->h_counters.as<unsigned long long>(4);
@@ -732,7 +739,7 @@ static uint64_t refine_t(gsj_ctx* c, const gsj_layer* P, const gsj_layer* R, con
     nwarps = (nwarps + 3) / 4 * 4;
     unsigned char* scr = c->scratch.as<unsigned char>(per * nwarps);
     GSJ_CK(cudaMemsetAsync(err, 0, 4, s));
-    k_refine_scratch<F><<<(int)(nwarps / 4), 128, 0, s>>>(P->d, R->d, pairs, heavy, nh, rp, flag, area, ev, evb, scr, cap, cph, err, ctr + 3);
+    k_refine_scratch<F><<<(int)(nwarps / 4), 128, 0, s>>>(P->d, R->d, pairs, heavy, nh, rp, flag, area, ev, evb, scr, cap, cph, err, ctr + 3, ctr + 4);
     c->launches++;
     GSJ_CK(cudaGetLastError());
     GSJ_CK(cudaMemcpyAsync(h, ctr, 32, cudaMemcpyDeviceToHost, s));
@@ -746,6 +753,7 @@ static uint64_t refine_t(gsj_ctx* c, const gsj_layer* P, const gsj_layer* R, con
 uint64_t refine(gsj_ctx* c, const gsj_layer* P, const gsj_layer* R, const uint2* pairs, uint64_t np, const RefineArgs& rp, int mode,
                 uint8_t* flag, double* area, double4* ev, uint32_t* evb) {
   if (!np) return 0;
+  if (mode == GSJ_REFINE_FILTERED_FP32) return refine_t<true, true>(c, P, R, pairs, np, rp, flag, area, ev, evb);
   return mode == GSJ_REFINE_FILTERED ? refine_t<true>(c, P, R, pairs, np, rp, flag, area, ev, evb)
                                      : refine_t<false>(c, P, R, pairs, np, rp, flag, area, ev, evb);
 }

@@ -15,6 +15,7 @@ from ._build import lib_path
 
 GSJ_REFINE_PLAIN = 0
 GSJ_REFINE_FILTERED = 1
+GSJ_REFINE_FILTERED_FP32 = 2   # the filtered variant with certified FP32 sign filters in front of its orientation tests
 
 _u32p = ctypes.POINTER(ctypes.c_uint32)
 _f64p = ctypes.POINTER(ctypes.c_double)
@@ -156,6 +157,13 @@ def de9im_transpose(code: int) -> int:
 
 def de9im_match(code: int, pattern: str) -> bool:
     return bool(lib().gsj_de9im_match(code, pattern.encode()))
+
+
+def _join_chunks(chunks, dtype):
+    """The batches' arrays as one (a single batch is returned as it is, without another copy)."""
+    if not chunks:
+        return np.zeros(0, dtype)
+    return chunks[0] if len(chunks) == 1 else np.concatenate(chunks)
 
 
 def _take(ptr, count, dtype):
@@ -341,9 +349,9 @@ class Engine:
         self._check(lib().gsj_join(self.ctx, P.h, R.h, ctypes.byref(rp), ctypes.byref(o), cb, None, ctypes.byref(st)))
         if not collect:
             return JoinResult(None, None, None, st.as_dict())
-        pairs = np.concatenate(chunks_p).reshape(-1, 2) if chunks_p else np.zeros((0, 2), np.uint32)
-        area = (np.concatenate(chunks_a) if chunks_a else np.zeros(0)) if want_area else None
-        code = (np.concatenate(chunks_c) if chunks_c else np.zeros(0, np.uint32)) if want_relate else None
+        pairs = _join_chunks(chunks_p, np.uint32).reshape(-1, 2)
+        area = _join_chunks(chunks_a, np.float64) if want_area else None
+        code = _join_chunks(chunks_c, np.uint32) if want_relate else None
         return JoinResult(pairs, area, code, st.as_dict())
 
     def join_points(self, pts: Layer, R: Layer, batch_q=0, shard=0, nshards=1, refine_mode=GSJ_REFINE_FILTERED):

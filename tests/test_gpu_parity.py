@@ -8,7 +8,7 @@ import shapes
 from gsj import gen
 
 pytestmark = pytest.mark.gpu
-MODES = [gsj.GSJ_REFINE_PLAIN, gsj.GSJ_REFINE_FILTERED]
+MODES = [gsj.GSJ_REFINE_PLAIN, gsj.GSJ_REFINE_FILTERED, gsj.GSJ_REFINE_FILTERED_FP32]
 SMALL_BOX = (-118.30, 33.95, -118.20, 34.05)
 
 

@@ -61,7 +61,7 @@ def test_relate_self_join_2m(engine, tmp, parcels):
     n_diag = int((want_p[:, 0] == want_p[:, 1]).sum())
     assert len(rows) == 2 * len(want_p) - n_diag == res["count"]["rows"]   # mirrored rows + the diagonal once
     L = engine.upload_polygons(ps)
-    for mode in MODES:
+    for mode in MODES + [gsj.GSJ_REFINE_FILTERED_FP32]:
         r = engine.join(L, L, want_area=False, want_relate=True, upper=True, refine_mode=mode)
         got_p, got_c = RH.sorted_rows(r.pairs, r.code)
         assert np.array_equal(got_p, want_p), f"mode {mode}: pair sets differ from the reference"
