@@ -632,10 +632,15 @@ def main():
         e1.synchronize()
         return r, e0.elapsed_time(e1)
 
+    # untimed: the refinement autotuner picks the filtered variant's launch shape on a sample of this join's
+    # candidate pairs; the plain variant runs with the default shape (the reference's fixed scheme)
+    default_shape = eng.refine_shape
+    tune = eng.tune_refine(L, L, want_area=False, want_relate=True, refine_mode=gsj.GSJ_REFINE_FILTERED, max_pairs=1 << 21)
     for _ in range(args.warmup):
         timed_join(gsj.GSJ_REFINE_FILTERED)
     res = {}
     for mode, name in ((gsj.GSJ_REFINE_FILTERED, "filtered"), (gsj.GSJ_REFINE_PLAIN, "plain")):
+        eng.refine_shape = tune["best"] if name == "filtered" else default_shape
         if name == "plain":
             timed_join(mode)   # warm this variant too
         barrier(ws)
@@ -648,6 +653,7 @@ def main():
         torch.cuda.synchronize()
         barrier(ws)
         res[name] = dict(ms=ms, pairs=pairs, stats=stats, clocks=clk.summary())
+    eng.refine_shape = tune["best"]
     # checks (untimed): the rows of both variants, compared with each other and with the reference engine's
     a = eng.join(L, L, want_area=False, want_relate=True, upper=True, refine_mode=gsj.GSJ_REFINE_FILTERED, **shard)
     b = eng.join(L, L, want_area=False, want_relate=True, upper=True, refine_mode=gsj.GSJ_REFINE_PLAIN, **shard)
@@ -724,6 +730,8 @@ def main():
                    "parallelism": f"probe shards x{ws} (one layer, R replicated)" if shard else f"replicas x{ws} (own layer per rank)",
                    "l2": "inputs > L2 (2.2 GB resident layer)"},
         "gen_s": round(t_gen, 2),
+        "refine_shape": {"filtered": tune["best"], "plain": default_shape, "autotuner": {k: tune[k] for k in ("start_ms", "best_ms", "sample_pairs", "shapes_tried")},
+                         "what": "launch shape of the refinement's two size bins; the filtered one chosen by gsj_tune_refine (untimed)"},
         "latency_ms": ({"p50": serving["filtered"]["p50_ms"], "p99": serving["filtered"]["p99_ms"],
                         "plain_p50": serving["plain"]["p50_ms"], "plain_p99": serving["plain"]["p99_ms"],
                         "what": "gsjd serving the request stream, arrival to end of result stream"} if serving else None),

@@ -196,6 +196,40 @@ int gsj_refine_pairs(gsj_ctx* ctx, const gsj_layer* P, const gsj_layer* R, const
 int gsj_refine_pairs_noalloc(gsj_ctx* ctx, const gsj_layer* P, const gsj_layer* R, const uint32_t* d_pairs, uint64_t np,
                              const gsj_refine_params* rp, uint8_t* d_flag, double* d_area, double* d_ev, uint32_t* d_evb);
 
+/* Launch shape of the refinement's two size bins, per context. No counterpart in the reference (its k_refine takes a
+ * fixed grid, engine.cuh:963-975). Pairs whose local edge lists fit bin_edges per side run in the shared-memory bin
+ * (a warp per pair, warps taking `run` consecutive pairs per fetch, at most `runs` fetches each); the others in the
+ * global-scratch bin with scratch_warps_per_sm warps per SM. Every shape gives the same results, bit for bit; only
+ * the time changes. Defaults: 4, 32, 128, 32. */
+typedef struct gsj_refine_shape {
+  int run;                   /* 1 - 64 */
+  int runs;                  /* 1 - 4096 */
+  int bin_edges;             /* 8 - 128 */
+  int scratch_warps_per_sm;  /* 1 - 64 */
+} gsj_refine_shape;
+int gsj_get_refine_shape(const gsj_ctx* ctx, gsj_refine_shape* out);
+int gsj_set_refine_shape(gsj_ctx* ctx, const gsj_refine_shape* shape);   /* GSJ_ERR_ARG when a field is out of range */
+
+/* Autotuner: times the refinement of P x R's candidate pairs (upper: b >= a only, for self-joins) under launch
+ * shapes searched one field at a time from the context's current shape, on a sample of at most max_pairs candidate
+ * pairs (0: 2^20; 16 evenly spaced runs of consecutive pairs, keeping the traversal order's locality), and sets the
+ * fastest on the context. Fields named in keep (GSJ_TUNE_KEEP_*) stay as they are: e.g. a server whose requests
+ * share the GPU keeps `runs`, which bounds how long a block holds an SM before other streams' kernels get it.
+ * Each shape's outputs are compared with the starting shape's, bit for bit; a difference fails the call
+ * (GSJ_ERR_CUDA) and leaves the shape unchanged. Takes a few seconds at most on large samples. */
+#define GSJ_TUNE_KEEP_RUN 1
+#define GSJ_TUNE_KEEP_RUNS 2
+#define GSJ_TUNE_KEEP_BIN 4
+#define GSJ_TUNE_KEEP_SCRATCH 8
+typedef struct gsj_tune_result {
+  gsj_refine_shape best;
+  double start_ms, best_ms;   /* device time of one refinement of the sample: starting shape, chosen shape */
+  uint64_t sample_pairs;
+  uint32_t shapes_tried;
+} gsj_tune_result;
+int gsj_tune_refine(gsj_ctx* ctx, const gsj_layer* P, const gsj_layer* R, const gsj_refine_params* rp, int refine_mode, int upper,
+                    uint64_t max_pairs, int keep, gsj_tune_result* out);
+
 /* Row encoding on the device (replaces the daemon's host encoder, send_parallel / FrameBuf, gpujoind.cu:178-206).
  * A rowset is a device copy of a layer's row ids (id_blob bytes, id_off[n_rows + 1] offsets) and, for a deduplicated
  * layer, its members (moff[n_geoms + 1], midx: the rows each distinct geometry stands for; NULL: geometry = row).

@@ -87,6 +87,10 @@ void gsj_ctx_destroy(gsj_ctx* c) {
   if (c->stream) {
     c->each_buf([](gsj::DevBuf& b) { b.release(); });   // stream-ordered frees before the stream goes
     cudaStreamSynchronize(c->stream);
+    for (auto& g : c->rgraph) {
+      if (g.exec) cudaGraphExecDestroy(g.exec);
+      if (g.graph) cudaGraphDestroy(g.graph);
+    }
     cudaStreamDestroy(c->stream);
   }
   delete c;
@@ -270,6 +274,26 @@ int gsj_refine_pairs(gsj_ctx* c, const gsj_layer* P, const gsj_layer* R, const u
                      int mode, uint8_t* flag, double* area, double* ev, uint32_t* evb) {
   if (!c || !P || !R || (np && !pairs)) return GSJ_ERR_ARG;
   return guard(c, [&] { gsj::refine_pairs_host(c, P, R, pairs, np, rp, mode, flag, area, ev, evb); });
+}
+
+int gsj_get_refine_shape(const gsj_ctx* c, gsj_refine_shape* out) {
+  if (!c || !out) return GSJ_ERR_ARG;
+  *out = gsj_refine_shape{c->shape.run, c->shape.runs, c->shape.bin_cap, c->shape.scratch_wpsm};
+  return GSJ_OK;
+}
+
+int gsj_set_refine_shape(gsj_ctx* c, const gsj_refine_shape* sh) {
+  if (!c || !sh) return GSJ_ERR_ARG;
+  const gsj::RefineShape v{sh->run, sh->runs, sh->bin_edges, sh->scratch_warps_per_sm};
+  if (!gsj::shape_valid(v)) { c->err = "refine shape field out of range"; return GSJ_ERR_ARG; }
+  c->shape = v;
+  return GSJ_OK;
+}
+
+int gsj_tune_refine(gsj_ctx* c, const gsj_layer* P, const gsj_layer* R, const gsj_refine_params* rp, int mode, int upper, uint64_t max_pairs,
+                    int keep, gsj_tune_result* out) {
+  if (!c || !P || !R) return GSJ_ERR_ARG;
+  return guard(c, [&] { gsj::tune_refine(c, P, R, gsj::to_args(rp), mode, upper, max_pairs, keep, out); });
 }
 
 int gsj_rowset_upload(gsj_ctx* c, uint64_t n_geoms, const uint64_t* moff, const uint32_t* midx, uint64_t n_rows, const char* id_blob,

@@ -70,8 +70,14 @@ struct Config {
   uint32_t stream_batch = 0;   // probe geometries per engine batch when rows are streamed (0: one batch)
   int gpu_encode = 1;           // rows encoded on the device (gsj_encode_rows) when they are sent from the engine's thread
   std::string snapshot_dir;     // prepared layers saved here after LOAD and restored at start-up (empty: off)
+  int tune = 0;                 // run the refinement autotuner on each LOADed polygon layer of >= kTuneGeoms geometries
 };
 Config g_cfg;
+// the refinement launch shape every context takes when it is leased (set by the autotuner at LOAD, --tune)
+std::mutex g_shape_m;
+bool g_shape_set = false;
+gsj_refine_shape g_shape{};
+constexpr uint64_t kTuneGeoms = 100000;
 std::atomic<bool> g_stop{false};
 
 void logf(const char* fmt, ...) {
@@ -148,6 +154,11 @@ class GpuPool {
     busy_++;
     used_ += est;
     cv_.notify_all();
+    lk.unlock();
+    {
+      std::lock_guard<std::mutex> sl(g_shape_m);
+      if (g_shape_set) gsj_set_refine_shape(c, &g_shape);
+    }
     return c;
   }
   void release(gsj_ctx* c, uint64_t est) {
@@ -471,6 +482,22 @@ std::string build_layer(const std::string& name, const std::string& path, int su
     check(lease.get(), gsj_layer_upload_polygons(lease.get(), bn, bnr, bnv, gro, rvo, xy, subdiv > 0 ? spar.p : nullptr,
                                                  subdiv > 0 ? ssyn.p : nullptr, &L->h), "upload");
     L->upload_s = secs_since(t1);
+    if (g_cfg.tune && bn >= kTuneGeoms) {   // launch shape for joins against this layer, from a sample of its self-join
+      gsj_refine_params rp;
+      gsj_refine_params_default(&rp);
+      gsj_tune_result tr;
+      // runs stays: it bounds how long a refinement block holds an SM while other requests' kernels wait for one
+      const int rc = gsj_tune_refine(lease.get(), L->h, L->h, &rp, g_cfg.refine_mode, 1, 1u << 20, GSJ_TUNE_KEEP_RUNS, &tr);
+      if (rc) logf("tune %s: %s", name.c_str(), gsj_last_error(lease.get()));
+      else {
+        std::lock_guard<std::mutex> sl(g_shape_m);
+        g_shape = tr.best;
+        g_shape_set = true;
+        logf("tune %s: shape run=%d runs=%d bin_edges=%d scratch_warps_per_sm=%d, %.2f -> %.2f ms on %llu pairs (%u shapes)", name.c_str(),
+             tr.best.run, tr.best.runs, tr.best.bin_edges, tr.best.scratch_warps_per_sm, tr.start_ms, tr.best_ms, (unsigned long long)tr.sample_pairs,
+             tr.shapes_tried);
+      }
+    }
     if (!g_cfg.snapshot_dir.empty()) {   // the arrays as uploaded (after dedup / subdivision), with the ids and members
       SnapArrays A; A.n = bn; A.nr = bnr; A.nv = bnv; A.gro = gro; A.rvo = rvo; A.xy = xy;
       if (subdiv > 0) { A.parent = spar.p; A.syn = ssyn.p; }
@@ -1289,6 +1316,7 @@ const char* kUsage =
     "usage: gsjd [--socket PATH] [--tcp HOST:PORT] [--token-file FILE] [--data-dir DIR] [--device N] [--workers N]\n"
     "            [--threads N] [--mem-budget-gb G] [--refine plain|filtered] [--stream-batch N] [--gpu-encode 0|1]\n"
     "            [--snapshot-dir DIR (prepared layers saved after LOAD, restored at start-up)]\n"
+    "            [--tune 0|1 (refinement autotuner on each LOADed polygon layer of >= 100k geometries)]\n"
     "            [--conninfo STR (accepted, unused: layers load from files)]\n";
 
 }  // namespace
@@ -1312,6 +1340,7 @@ extern "C" int gsjd_main(int argc, char** argv) {
     else if (a == "--stream-batch" && has) g_cfg.stream_batch = (uint32_t)std::max(0, atoi(argv[++i]));
     else if (a == "--gpu-encode" && has) g_cfg.gpu_encode = atoi(argv[++i]) != 0;
     else if (a == "--snapshot-dir" && has) g_cfg.snapshot_dir = argv[++i];
+    else if (a == "--tune" && has) g_cfg.tune = atoi(argv[++i]) != 0;
     else if (a == "--refine" && has) {
       const std::string m = argv[++i];
       if (m != "plain" && m != "filtered") { fputs("--refine plain|filtered\n", stderr); return 1; }

@@ -8,6 +8,8 @@
 #include <stdexcept>
 #include <string>
 #include <functional>
+#include <tuple>
+#include <utility>
 #include <vector>
 #include "../../include/gsj.h"
 #include "geom.cuh"
@@ -98,6 +100,35 @@ struct gsj_layer {
   int device = 0;
 };
 
+namespace gsj {
+// Kernel arguments held for a graph kernel node: each value converted to the kernel's own parameter type (so the
+// argument list is checked against the kernel's signature at compile time), ptr[] pointing at them.
+template <class... A>
+struct KernelArgs {
+  std::tuple<A...> val;
+  void* ptr[sizeof...(A) ? sizeof...(A) : 1];
+  explicit KernelArgs(A... a) : val(a...) { fill(std::index_sequence_for<A...>{}); }
+  KernelArgs(const KernelArgs&) = delete;
+  KernelArgs& operator=(const KernelArgs&) = delete;
+ private:
+  template <size_t... I> void fill(std::index_sequence<I...>) { ((ptr[I] = &std::get<I>(val)), ...); }
+};
+template <class... A, class... V>
+KernelArgs<A...> kernel_args(void (*)(A...), V&&... v) {
+  static_assert(sizeof...(A) == sizeof...(V), "argument count differs from the kernel's parameters");
+  return KernelArgs<A...>(static_cast<A>(v)...);
+}
+
+// Launch shape of the refinement's two size bins (set by gsj_set_refine_shape or chosen by gsj_tune_refine):
+// run / runs = consecutive pairs a warp of the shared-memory bin takes per fetch / fetches per warp (grid size);
+// bin_cap = local edges per side up to which a pair stays in the shared-memory bin (at most its list capacity);
+// scratch_wpsm = warps per SM of the global-scratch bin.
+struct RefineShape { int run = 4, runs = 32, bin_cap = 128, scratch_wpsm = 32; };
+// The refinement's bins as one CUDA graph per variant (shared-memory bin, then scratch bin), instantiated once per
+// context and re-parameterised per call.
+struct RefineGraph { cudaGraph_t graph = nullptr; cudaGraphExec_t exec = nullptr; cudaGraphNode_t n_main = nullptr, n_scr = nullptr; };
+}  // namespace gsj
+
 struct gsj_ctx {
   int device = 0;
   int sm_count = 148;
@@ -107,6 +138,8 @@ struct gsj_ctx {
   uint64_t launches = 0;      // kernels launched by this context (reported per call in the stats)
   uint64_t node_visits = 0;   // LBVH nodes visited by traversals (roofline accounting)
   uint64_t edge_pairs = 0;    // local edge pairs (na x nb) of the pairs refined (the refinement's work unit)
+  gsj::RefineShape shape;
+  gsj::RefineGraph rgraph[6];   // [variant (plain, filtered, filtered FP32) x with / without the scratch bin]
   // scratch pools
   gsj::DevBuf counters, cand, flag, area, ev, evb, heavy, scratch, keep, opairs, oarea, oev, oevb, ocode, tmp, keys, keys2, idx,
       idx2, agg_area, agg_ev, agg_evb, agg_flag, qbb, uf, misc1, misc2, misc3,
@@ -149,6 +182,11 @@ gsj_join_opts opts_or_default(const gsj_join_opts* o);
 // per-pair refinement (flag, area, ev, evb); returns the number of pairs that took the oversized path
 uint64_t refine(gsj_ctx* c, const gsj_layer* P, const gsj_layer* R, const uint2* pairs, uint64_t np, const RefineArgs& rp, int mode,
                 uint8_t* flag, double* area, double4* ev, uint32_t* evb);
+
+// refinement launch shapes (tune.cu)
+bool shape_valid(const RefineShape& s);
+void tune_refine(gsj_ctx* c, const gsj_layer* P, const gsj_layer* R, const RefineArgs& rp, int mode, int upper, uint64_t max_pairs, int keep,
+                 gsj_tune_result* out);
 
 // device row encoding (encode.cu)
 uint64_t encode_rows(gsj_ctx* c, const gsj_rowset* P, const gsj_rowset* Q, const gsj_encode_spec* spec, const uint32_t* pairs, const double* area,

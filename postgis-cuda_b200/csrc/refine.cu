@@ -35,7 +35,6 @@ struct PairGeo { Box ov; double tol, eps_par, snap, cx, cy; };
 // 2 tol of each other - a superset of the pairs any box test of the pair routine keeps (those use tol or no pad).
 // Built by one lane-balanced sweep over the na x nb grid (ballot compaction keeps (i, j) order); per-edge
 // ranges: A edge i owns cp[sa[i] .. sa[i+1]), B edge j owns pj[(j ? sb[j-1] : 0) .. sb[j]) (entries in i order).
-constexpr int REFINE_RUN = 4, REFINE_RUNS = 32;   // filtered kernel: pairs per fetch, fetches per warp
 // Large grids are searched by buckets instead: NBK slabs along the overlap box's longer side, B's edges listed per
 // slab (bl, boff), each lane scanning only its A edge's slabs and reporting a pair once, in the first slab both
 // edges reach; the lane sorts its few candidates (at most LCAP) so the list keeps (i, j) order.
@@ -595,7 +594,7 @@ template <bool F, bool S32 = false>
 __global__ void __launch_bounds__(RB_WARPS * 32, Cfg<F>::minb) k_refine(DLayer P, DLayer R, const uint2* __restrict__ pairs, uint64_t np,
                                                                         RefineArgs rp, uint8_t* flag, double* area, double4* ev, uint32_t* evb,
                                                                         uint32_t* heavy, unsigned long long* nheavy, unsigned long long* next,
-                                                                        unsigned long long* epairs) {
+                                                                        unsigned long long* epairs, int run, int runs, int bin_cap) {
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ unsigned long long s_ep[RB_WARPS];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
@@ -612,7 +611,7 @@ __global__ void __launch_bounds__(RB_WARPS * 32, Cfg<F>::minb) k_refine(DLayer P
   auto one = [&](uint64_t p) {
     const uint2 pr = pairs[p];
     uint8_t f; double ar; double4 e4; uint32_t b4;
-    const bool ok = refine_pair_t<F, false, false, F, S32>(P, R, pr.x, pr.y, rp, LA, LB, Cfg<F>::cap, lane, f, ar, e4, b4, nullptr, &mbuf, &s_ep[wib]);
+    const bool ok = refine_pair_t<F, false, false, F, S32>(P, R, pr.x, pr.y, rp, LA, LB, bin_cap, lane, f, ar, e4, b4, nullptr, &mbuf, &s_ep[wib]);
     if (lane == 0) {
       if (!ok) { heavy[atomicAdd(nheavy, 1ull)] = (uint32_t)p; flag[p] = 0; }
       else {
@@ -624,15 +623,15 @@ __global__ void __launch_bounds__(RB_WARPS * 32, Cfg<F>::minb) k_refine(DLayer P
     __syncwarp();
   };
   if constexpr (F) {
-    // warps take runs of consecutive pairs (shared probe geometry) from a counter, at most REFINE_RUNS runs each:
+    // warps take runs of `run` consecutive pairs (shared probe geometry) from a counter, at most `runs` runs each:
     // the grid is sized to cover every pair that way, and bounded block lifetimes let the kernels of other
     // streams (higher-priority requests) take SMs as blocks retire
-    for (int k = 0; k < REFINE_RUNS; k++) {
+    for (int k = 0; k < runs; k++) {
       unsigned long long p0 = 0;
-      if (lane == 0) p0 = atomicAdd(next, (unsigned long long)REFINE_RUN);
+      if (lane == 0) p0 = atomicAdd(next, (unsigned long long)run);
       p0 = __shfl_sync(0xffffffffu, p0, 0);
       if (p0 >= np) break;
-      const uint64_t p1 = p0 + REFINE_RUN < np ? p0 + REFINE_RUN : np;
+      const uint64_t p1 = p0 + run < np ? p0 + run : np;
       for (uint64_t p = p0; p < p1; p++) one(p);
     }
   } else {
@@ -652,10 +651,12 @@ __host__ __device__ constexpr size_t scratch_per_warp(int cap, int cph) {
 }
 template <bool F>
 __global__ void __launch_bounds__(128) k_refine_scratch(DLayer P, DLayer R, const uint2* __restrict__ pairs, const uint32_t* __restrict__ heavy,
-                                                       uint64_t nh, RefineArgs rp, uint8_t* flag, double* area, double4* ev, uint32_t* evb,
+                                                       const unsigned long long* nheavy, RefineArgs rp, uint8_t* flag, double* area, double4* ev, uint32_t* evb,
                                                        unsigned char* scratch, int cap, int cph, int* err, unsigned long long* epairs,
                                                        unsigned long long* next) {
   const int lane = threadIdx.x & 31;
+  const uint64_t nh = *nheavy;   // written by the shared-memory bin launched before this kernel on the same stream
+  if (nh == 0) return;
   unsigned long long ep = 0;
   const uint64_t w = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
   unsigned char* base = scratch + w * scratch_per_warp<F>(cap, cph);
@@ -700,6 +701,22 @@ __global__ void __launch_bounds__(128) k_refine_scratch(DLayer P, DLayer R, cons
   if (lane == 0 && ep) atomicAdd(epairs, ep);
 }
 
+// Scratch-bin layout for a layer pair: list capacity (rounded to 8 edges, which keeps every double array of the slab
+// 8-byte aligned), candidate entries (indices stay below 2^16) and bytes per warp.
+struct ScratchGeom { int cap, cph; size_t per; };
+template <bool F>
+static ScratchGeom scratch_geom(const gsj_layer* P, const gsj_layer* R) {
+  ScratchGeom g;
+  g.cap = (int)((std::max<uint32_t>(std::max(P->max_geom_edges, R->max_geom_edges), 1u) + 7u) & ~7u);
+  g.cph = std::min(8 * g.cap, 1 << 16);
+  g.per = scratch_per_warp<F>(g.cap, g.cph);
+  return g;
+}
+
+// One refinement = one graph launch between the counters' reset and their copy to pinned host memory: the
+// shared-memory bin (pairs whose local lists fit bin_cap), then the scratch bin (the pairs the first bin listed as
+// oversized; it reads their count on the device, so no host round trip separates the bins); then one stream sync.
+// The executable graph is built once per context and variant and re-parameterised per call.
 template <bool F, bool S32 = false>
 static uint64_t refine_t(gsj_ctx* c, const gsj_layer* P, const gsj_layer* R, const uint2* pairs, uint64_t np, const RefineArgs& rp, uint8_t* flag,
                          double* area, double4* ev, uint32_t* evb) {
@@ -709,45 +726,69 @@ static uint64_t refine_t(gsj_ctx* c, const gsj_layer* P, const gsj_layer* R, con
     GSJ_CK(cudaFuncSetAttribute(k_refine<F, S32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cfg<F>::smem));
     c->refine_attr |= bit;
   }
+  const RefineShape& sh = c->shape;
   unsigned long long* ctr = c->counters.as<unsigned long long>(8);
   int* err = reinterpret_cast<int*>(ctr + 1);
-  GSJ_CK(cudaMemsetAsync(ctr, 0, 40, s));   // heavy count, error word, pair counter, local edge pairs, scratch pair counter
   uint32_t* heavy = c->heavy.as<uint32_t>(np);
+  const int bin_cap = std::min(sh.bin_cap, Cfg<F>::cap), run = sh.run, runs = sh.runs;
   int blocks;
-  if constexpr (F) {   // enough warps to cover every pair with REFINE_RUNS fetches each, spread over all SMs
-    const uint64_t per_block = (uint64_t)RB_WARPS * REFINE_RUNS * REFINE_RUN;
-    const uint64_t cover = (np + per_block - 1) / per_block;
-    const uint64_t spread = std::min<uint64_t>((np + RB_WARPS * REFINE_RUN - 1) / (RB_WARPS * REFINE_RUN), (uint64_t)c->sm_count * Cfg<F>::minb);
-    blocks = (int)std::max<uint64_t>(cover, spread);
+  if constexpr (F) {
+    // enough warps to cover every pair with `runs` fetches each, spread over all SMs; more than one wave of blocks
+    // is rounded up to whole waves, so the last wave's blocks share the remaining pairs (the counter hands them out)
+    // instead of leaving part of the GPU idle while a partial wave runs
+    const uint64_t per_block = (uint64_t)RB_WARPS * runs * run, wave = (uint64_t)c->sm_count * Cfg<F>::minb;
+    uint64_t cover = (np + per_block - 1) / per_block;
+    if (cover > wave) cover = (cover + wave - 1) / wave * wave;
+    const uint64_t spread = std::min<uint64_t>((np + (uint64_t)RB_WARPS * run - 1) / ((uint64_t)RB_WARPS * run), wave);
+    blocks = (int)std::min<uint64_t>(std::max<uint64_t>(cover, spread), 1u << 30);
   } else {
     blocks = (int)std::min<uint64_t>((np + RB_WARPS - 1) / RB_WARPS, (uint64_t)c->sm_count * 8);
   }
-  k_refine<F, S32><<<blocks, RB_WARPS * 32, Cfg<F>::smem, s>>>(P->d, R->d, pairs, np, rp, flag, area, ev, evb, heavy, ctr, ctr + 2, ctr + 3);
-  c->launches++;
-  GSJ_CK(cudaGetLastError());
+  // a pair can only be oversized when one of its polygons has more edges than the bin holds
+  const bool scr = std::max(P->max_geom_edges, R->max_geom_edges) > (uint32_t)bin_cap;
+  const ScratchGeom sg = scratch_geom<F>(P, R);
+  int sblocks = 0;
+  unsigned char* sbuf = nullptr;
+  if (scr) {   // warps: the shape's share of every SM, at most one per pair and at most 1 GiB of lists
+    uint64_t nwarps = std::min<uint64_t>((uint64_t)c->sm_count * sh.scratch_wpsm, std::max<uint64_t>(1, (1ull << 30) / sg.per));
+    nwarps = std::min<uint64_t>(nwarps, np);
+    nwarps = (nwarps + 3) / 4 * 4;
+    sblocks = (int)(nwarps / 4);
+    sbuf = c->scratch.as<unsigned char>(sg.per * nwarps);
+  }
   unsigned long long* h = c->h_counters.as<unsigned long long>(4);
+  auto a_main = kernel_args(k_refine<F, S32>, P->d, R->d, pairs, np, rp, flag, area, ev, evb, heavy, ctr, ctr + 2, ctr + 3, run, runs, bin_cap);
+  auto a_scr = kernel_args(k_refine_scratch<F>, P->d, R->d, pairs, heavy, ctr, rp, flag, area, ev, evb, sbuf, sg.cap, sg.cph, err, ctr + 3,
+                           ctr + 4);
+  cudaKernelNodeParams km{}, ks{};
+  km.func = (void*)k_refine<F, S32>;
+  km.gridDim = dim3(blocks);
+  km.blockDim = dim3(RB_WARPS * 32);
+  km.sharedMemBytes = (unsigned)Cfg<F>::smem;
+  km.kernelParams = a_main.ptr;
+  ks.func = (void*)k_refine_scratch<F>;
+  ks.gridDim = dim3(std::max(sblocks, 1));
+  ks.blockDim = dim3(128);
+  ks.kernelParams = a_scr.ptr;
+  RefineGraph& g = c->rgraph[(S32 ? 2 : (F ? 1 : 0)) * 2 + (scr ? 1 : 0)];
+  if (!g.exec) {   // the graph is kept with its executable: the node handles used for the updates belong to it
+    if (!g.graph) GSJ_CK(cudaGraphCreate(&g.graph, 0));
+    if (!g.n_main) GSJ_CK(cudaGraphAddKernelNode(&g.n_main, g.graph, nullptr, 0, &km));
+    if (scr && !g.n_scr) GSJ_CK(cudaGraphAddKernelNode(&g.n_scr, g.graph, &g.n_main, 1, &ks));
+    GSJ_CK(cudaGraphInstantiate(&g.exec, g.graph, 0));
+  } else {
+    GSJ_CK(cudaGraphExecKernelNodeSetParams(g.exec, g.n_main, &km));
+    if (scr) GSJ_CK(cudaGraphExecKernelNodeSetParams(g.exec, g.n_scr, &ks));
+  }
+  // heavy count, error word, pair counter, local edge pairs, scratch pair counter
+  GSJ_CK(cudaMemsetAsync(ctr, 0, 40, s));
+  GSJ_CK(cudaGraphLaunch(g.exec, s));
+  c->launches += scr ? 2 : 1;
   GSJ_CK(cudaMemcpyAsync(h, ctr, 32, cudaMemcpyDeviceToHost, s));
   GSJ_CK(cudaStreamSynchronize(s));
-  const uint64_t nh = h[0];
-  if (nh) {
-    // list capacity rounded to 8 edges keeps every double array of the slab 8-byte aligned
-    const int cap = (int)((std::max<uint32_t>(std::max(P->max_geom_edges, R->max_geom_edges), 1u) + 7u) & ~7u);
-    const int cph = std::min(8 * cap, 1 << 16);   // candidate entries (indices stay below 2^16)
-    const size_t per = scratch_per_warp<F>(cap, cph);
-    uint64_t nwarps = std::min<uint64_t>(nh, std::max<uint64_t>(1, (1ull << 30) / per));
-    nwarps = std::min<uint64_t>(nwarps, (uint64_t)c->sm_count * 32);
-    nwarps = (nwarps + 3) / 4 * 4;
-    unsigned char* scr = c->scratch.as<unsigned char>(per * nwarps);
-    GSJ_CK(cudaMemsetAsync(err, 0, 4, s));
-    k_refine_scratch<F><<<(int)(nwarps / 4), 128, 0, s>>>(P->d, R->d, pairs, heavy, nh, rp, flag, area, ev, evb, scr, cap, cph, err, ctr + 3, ctr + 4);
-    c->launches++;
-    GSJ_CK(cudaGetLastError());
-    GSJ_CK(cudaMemcpyAsync(h, ctr, 32, cudaMemcpyDeviceToHost, s));
-    GSJ_CK(cudaStreamSynchronize(s));
-    if (reinterpret_cast<int*>(h + 1)[0]) throw Error(GSJ_ERR_CUDA, "oversized pair exceeded the scratch edge capacity");
-  }
+  if (reinterpret_cast<int*>(h + 1)[0]) throw Error(GSJ_ERR_CUDA, "oversized pair exceeded the scratch edge capacity");
   c->edge_pairs += h[3];
-  return nh;
+  return h[0];
 }
 
 uint64_t refine(gsj_ctx* c, const gsj_layer* P, const gsj_layer* R, const uint2* pairs, uint64_t np, const RefineArgs& rp, int mode,

@@ -54,6 +54,18 @@ class JoinStats(ctypes.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class RefineShape(ctypes.Structure):
+    _fields_ = [("run", ctypes.c_int), ("runs", ctypes.c_int), ("bin_edges", ctypes.c_int), ("scratch_warps_per_sm", ctypes.c_int)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class TuneResult(ctypes.Structure):
+    _fields_ = [("best", RefineShape), ("start_ms", ctypes.c_double), ("best_ms", ctypes.c_double), ("sample_pairs", ctypes.c_uint64),
+                ("shapes_tried", ctypes.c_uint32)]
+
+
 class LayerInfo(ctypes.Structure):
     _fields_ = [("n", ctypes.c_uint64), ("nr", ctypes.c_uint64), ("nv", ctypes.c_uint64), ("nparent", ctypes.c_uint32),
                 ("is_points", ctypes.c_int), ("max_geom_edges", ctypes.c_uint32), ("device_bytes", ctypes.c_uint64)]
@@ -103,6 +115,10 @@ SIGNATURES = {
     "gsj_candidates": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_int, PAIRS_SINK, _vp]),
     "gsj_refine_pairs": (ctypes.c_int, [_vp, _vp, _vp, _vp, ctypes.c_uint64, ctypes.POINTER(RefineParams), ctypes.c_int, _vp, _vp, _vp, _vp]),
     "gsj_refine_pairs_noalloc": (ctypes.c_int, [_vp, _vp, _vp, _vp, ctypes.c_uint64, ctypes.POINTER(RefineParams), _vp, _vp, _vp, _vp]),
+    "gsj_get_refine_shape": (ctypes.c_int, [_vp, ctypes.POINTER(RefineShape)]),
+    "gsj_set_refine_shape": (ctypes.c_int, [_vp, ctypes.POINTER(RefineShape)]),
+    "gsj_tune_refine": (ctypes.c_int, [_vp, _vp, _vp, ctypes.POINTER(RefineParams), ctypes.c_int, ctypes.c_int, ctypes.c_uint64, ctypes.c_int,
+                                       ctypes.POINTER(TuneResult)]),
     "gsj_subdivide": (ctypes.c_int, [ctypes.c_uint64] * 3 + [_vp] * 3 + [ctypes.c_int] + [ctypes.POINTER(ctypes.c_uint64)] * 3 +
                       [ctypes.POINTER(_vp)] * 5),
     "gsj_dedup": (ctypes.c_int, [ctypes.c_uint64] * 3 + [_vp] * 3 + [ctypes.c_int] + [ctypes.POINTER(ctypes.c_uint64)] * 3 +
@@ -461,6 +477,31 @@ class Engine:
         cb = PAIRS_SINK(sink)
         self._check(lib().gsj_candidates(self.ctx, P.h, R.h, int(upper), cb, None))
         return np.concatenate(chunks).reshape(-1, 2) if chunks else np.zeros((0, 2), np.uint32)
+
+    @property
+    def refine_shape(self) -> dict:
+        """The context's refinement launch shape (gsj_get_refine_shape): run, runs, bin_edges, scratch_warps_per_sm."""
+        sh = RefineShape()
+        self._check(lib().gsj_get_refine_shape(self.ctx, ctypes.byref(sh)))
+        return sh.as_dict()
+
+    @refine_shape.setter
+    def refine_shape(self, shape: dict):
+        sh = RefineShape(**{**self.refine_shape, **shape})
+        self._check(lib().gsj_set_refine_shape(self.ctx, ctypes.byref(sh)))
+
+    def tune_refine(self, P: Layer, R: Layer, want_area=True, want_relate=False, refine_mode=GSJ_REFINE_FILTERED, upper=None, max_pairs=0,
+                    keep=()) -> dict:
+        """Runs the refinement autotuner (gsj_tune_refine) on P x R's candidate pairs and sets the chosen shape on this
+        context; keep names shape fields left as they are. Returns {'best': shape, 'start_ms', 'best_ms', 'sample_pairs',
+        'shapes_tried'}."""
+        rp = refine_params(want_area, want_relate)
+        r = TuneResult()
+        up = (P is R) if upper is None else bool(upper)
+        bits = {"run": 1, "runs": 2, "bin_edges": 4, "scratch_warps_per_sm": 8}
+        mask = sum(bits[k] for k in keep)
+        self._check(lib().gsj_tune_refine(self.ctx, P.h, R.h, ctypes.byref(rp), refine_mode, int(up), int(max_pairs), mask, ctypes.byref(r)))
+        return {"best": r.best.as_dict(), "start_ms": r.start_ms, "best_ms": r.best_ms, "sample_pairs": r.sample_pairs, "shapes_tried": r.shapes_tried}
 
     def refine_pairs(self, P: Layer, R: Layer, pairs, want_area=True, want_relate=False, refine_mode=GSJ_REFINE_FILTERED, snap_half_ulp=False):
         pairs = np.ascontiguousarray(pairs, dtype=np.uint32)

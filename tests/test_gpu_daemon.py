@@ -321,3 +321,31 @@ def test_snapshots_restore_layers(env, tmp_path):
     finally:
         D.stop(p)
         log.close()
+
+
+def test_tune_at_load_same_rows(env):
+    """--tune 1: loading a polygon layer of >= 100k geometries runs the refinement autotuner (logged) and every
+    context takes the chosen launch shape; the rows are the same as without it."""
+    big = gen.layer_parcels(120_000, (-118.6, 33.7, -118.0, 34.3), seed=21)
+    gen.write_gset(str(env.dir / "big.gset"), big)
+    logp = env.dir / "gsjd_tune.log"
+    log = open(logp, "w")
+    sock = str(env.dir / "gsjd_tune.sock")
+    p = D.start(sock, str(env.dir), workers=2, log=log, extra=["--tune", "1"])
+    try:
+        cl = C.Client(sock)
+        cl.load("big", "big.gset", dedup=False)
+        got = sorted(cl.join("big", "big", True, "distinct")[0])
+        got_rel = sorted(cl.relate("big", "big", "", "distinct")[0])
+    finally:
+        D.stop(p)
+        log.close()
+    env.cl.load("big", "big.gset", dedup=False)
+    try:
+        want = sorted(env.cl.join("big", "big", True, "distinct")[0])
+        want_rel = sorted(env.cl.relate("big", "big", "", "distinct")[0])
+    finally:
+        env.cl.drop("big")
+    text = logp.read_text()
+    assert "tune big: shape run=" in text, text[-2000:]
+    assert got == want and got_rel == want_rel and len(want) > 100_000
