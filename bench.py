@@ -228,9 +228,10 @@ def serving_schedule(rng, qpoly, n, rate):
     return "\n".join(lines) + "\n"
 
 
-SERVE_ARMS = (   # name -> gsjd flags; the same daemon, schedule and priming, only the refinement differs
-    ("filtered", ["--refine", "filtered"]),
-    ("plain", ["--refine", "plain"]),
+SERVE_ARMS = (   # name -> gsjd flags; the same daemon, schedule and priming, only the refinement differs; each arm's
+    # refinement launch shape is chosen by the autotuner when the resident layer is loaded
+    ("filtered", ["--refine", "filtered", "--tune", "1"]),
+    ("plain", ["--refine", "plain", "--tune", "1"]),
 )
 
 

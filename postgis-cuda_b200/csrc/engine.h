@@ -126,7 +126,10 @@ KernelArgs<A...> kernel_args(void (*)(A...), V&&... v) {
 struct RefineShape { int run = 4, runs = 32, bin_cap = 128, scratch_wpsm = 32; };
 // The refinement's bins as one CUDA graph per variant (shared-memory bin, then scratch bin), instantiated once per
 // context and re-parameterised per call.
-struct RefineGraph { cudaGraph_t graph = nullptr; cudaGraphExec_t exec = nullptr; cudaGraphNode_t n_main = nullptr, n_scr = nullptr; };
+struct RefineGraph {
+  cudaGraph_t graph = nullptr; cudaGraphExec_t exec = nullptr;
+  cudaGraphNode_t n_main = nullptr, n_scr = nullptr, n_idx = nullptr, n_self = nullptr;
+};
 }  // namespace gsj
 
 struct gsj_ctx {
@@ -139,15 +142,15 @@ struct gsj_ctx {
   uint64_t node_visits = 0;   // LBVH nodes visited by traversals (roofline accounting)
   uint64_t edge_pairs = 0;    // local edge pairs (na x nb) of the pairs refined (the refinement's work unit)
   gsj::RefineShape shape;
-  gsj::RefineGraph rgraph[6];   // [variant (plain, filtered, filtered FP32) x with / without the scratch bin]
+  gsj::RefineGraph rgraph[12];   // [variant (plain, filtered, filtered FP32) x scratch bin or not x self bin or not]
   // scratch pools
-  gsj::DevBuf counters, cand, flag, area, ev, evb, heavy, scratch, keep, opairs, oarea, oev, oevb, ocode, tmp, keys, keys2, idx,
+  gsj::DevBuf counters, cand, flag, area, ev, evb, heavy, selfidx, scratch, keep, opairs, oarea, oev, oevb, ocode, tmp, keys, keys2, idx,
       idx2, agg_area, agg_ev, agg_evb, agg_flag, qbb, uf, misc1, misc2, misc3,
       er_pf, er_keep, er_off, er_pairs, er_flag, er_heavy, er_tiles, er_tiles2, er_slab, er_again, er_scr, er_ctr, er_tmp,
       enc_in, enc_cnt, enc_pre, enc_blk, enc_out;
   // every scratch pool, e.g. to bind them to the stream or release them before the stream goes
   template <class Fn> void each_buf(Fn&& fn) {
-    for (gsj::DevBuf* b : {&counters, &cand, &flag, &area, &ev, &evb, &heavy, &scratch, &keep, &opairs, &oarea, &oev, &oevb, &ocode, &tmp, &keys, &keys2, &idx, &idx2, &agg_area, &agg_ev, &agg_evb, &agg_flag, &qbb, &uf, &misc1, &misc2, &misc3, &er_pf, &er_keep, &er_off, &er_pairs, &er_flag, &er_heavy, &er_tiles, &er_tiles2, &er_slab, &er_again, &er_scr, &er_ctr, &er_tmp, &enc_in, &enc_cnt, &enc_pre, &enc_blk, &enc_out}) fn(*b);
+    for (gsj::DevBuf* b : {&counters, &cand, &flag, &area, &ev, &evb, &heavy, &selfidx, &scratch, &keep, &opairs, &oarea, &oev, &oevb, &ocode, &tmp, &keys, &keys2, &idx, &idx2, &agg_area, &agg_ev, &agg_evb, &agg_flag, &qbb, &uf, &misc1, &misc2, &misc3, &er_pf, &er_keep, &er_off, &er_pairs, &er_flag, &er_heavy, &er_tiles, &er_tiles2, &er_slab, &er_again, &er_scr, &er_ctr, &er_tmp, &enc_in, &enc_cnt, &enc_pre, &enc_blk, &enc_out}) fn(*b);
   }
   gsj::PinnedBuf h_counters, h_pairs, h_area, h_code, h_where, h_enc;
 };

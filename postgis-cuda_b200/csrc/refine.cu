@@ -224,7 +224,9 @@ __device__ __forceinline__ uint32_t warp_transpose32(uint32_t x, int lane) {
 }
 
 // lane i (per 32 A edges) keeps its padded box in registers and tests every B edge j, read once for the whole warp
-// (a shared-memory broadcast); each 32 x 32 block of rows is transposed into columns by shuffles
+// (a shared-memory broadcast); each 32 x 32 block of rows is transposed into columns by shuffles (COLS; the self
+// bin reads rows only). STRIDE: rows per mask word plane (the bin's list capacity).
+template <int STRIDE = CAP_F, bool COLS = true>
 __device__ void mask_candidates(const EList& LA, int na, const EList& LB, int nb, double pad, const MaskBuf& mb, int lane) {
   const int nbw = (nb + 31) >> 5;
   const double inf = __longlong_as_double(0x7ff0000000000000LL);
@@ -241,9 +243,11 @@ __device__ void mask_candidates(const EList& LA, int na, const EList& LB, int nb
       uint32_t bits = 0;
       for (int j = j0; j < j1; j++)
         bits |= (out_cmp(LB.x0[j], LB.y0[j], LB.x1[j], LB.y1[j], ax0, ay0, ax1, ay1) ? 0u : 1u) << (j - j0);
-      if (i < na) mb.rm[w * CAP_F + i] = bits;
-      const uint32_t col = warp_transpose32(bits, lane);
-      if (j0 + lane < nb) mb.cm[(ic >> 5) * CAP_F + j0 + lane] = col;
+      if (i < na) mb.rm[w * STRIDE + i] = bits;
+      if constexpr (COLS) {
+        const uint32_t col = warp_transpose32(bits, lane);
+        if (j0 + lane < nb) mb.cm[(ic >> 5) * STRIDE + j0 + lane] = col;
+      }
     }
   }
   __syncwarp();
@@ -366,7 +370,11 @@ __device__ __forceinline__ double pair_snap(double2 oa, double2 ea) {   // engin
 // MASK (the filtered shared-memory kernel): candidate edge pairs as bit masks (mb).
 // FLAT (the filtered scratch kernel): candidate lists in global scratch; a pair whose list would exceed fb->cap is
 // handed back (false) and runs with the full sweeps.
-template <bool F, bool FLAT = false, bool BUCKETS = false, bool MASK = false, bool S32 = false>
+// SELF (> 0, filtered shared-memory bin only): the pair is a geometry with itself in one layer; the caller passes
+// one list of SELF edges as both LA and LB. B's gather and B's contribution pass would repeat A's exactly (the same
+// edges in the same frame, the same candidates in the same order, so the same values): A's pass runs once and each
+// lane adds its recorded values a second time, in the same order, which is the sum the two passes make.
+template <bool F, bool FLAT = false, bool BUCKETS = false, bool MASK = false, bool S32 = false, int SELF = 0>
 __device__ bool refine_pair_t(const DLayer& P, const DLayer& R, uint32_t a, uint32_t b, const RefineArgs& rp, EList LA, EList LB, int cap,
                               int lane, uint8_t& o_flag, double& o_area, double4& o_ev, uint32_t& o_evb, const FlatBuf* fb = nullptr,
                               const MaskBuf* mb = nullptr, unsigned long long* ep = nullptr) {
@@ -383,17 +391,19 @@ __device__ bool refine_pair_t(const DLayer& P, const DLayer& R, uint32_t a, uint
   G.cy = (double)(G.ov.y0 + 0.414213 * (G.ov.y1 - G.ov.y0));
   int na = 0, nb = 0;
   bool inB_c = false, inA_c = false;
-  for (int side = 0; side < 2; side++) {   // one inlined copy of the gather
+  for (int side = 0; side < (SELF ? 1 : 2); side++) {   // one inlined copy of the gather
     bool in = false;
     // MASK: the containment parity of the probe point c is taken in the gather's pass over each polygon's edges
     const int n = collect<F, MASK, S32>(side ? B : A, G.ov, side ? LB : LA, cap, lane, G.cx, G.cy, &in);
     if (side) { nb = n; inB_c = in; } else { na = n; inA_c = in; }
   }
+  if constexpr (SELF > 0) { nb = na; inB_c = inA_c; }
   if (na > cap || nb > cap) return false;
   __syncwarp();
+  constexpr int MW = SELF ? SELF / 32 : MASK_WORDS, MS = SELF ? SELF : CAP_F;   // mask words per row, row stride
   int ncp = -1;   // candidate edge pairs (FLAT); -1: sweep every edge pair
   if constexpr (MASK) {
-    mask_candidates(LA, na, LB, nb, 2.0 * G.tol, *mb, lane);
+    mask_candidates<MS, SELF == 0>(LA, na, LB, nb, 2.0 * G.tol, *mb, lane);
   } else if constexpr (FLAT) {
     ncp = flat_candidates<BUCKETS>(LA, na, LB, nb, 2.0 * G.tol, G.ov, *fb, lane);
     if (ncp > fb->cap) return false;
@@ -421,9 +431,9 @@ __device__ bool refine_pair_t(const DLayer& P, const DLayer& R, uint32_t a, uint
     const int nbw = (nb + 31) >> 5;
     for (int ic = 0; ic < na && !hit; ic += 32) {
       const int i = ic + lane;
-      uint32_t w[MASK_WORDS];
+      uint32_t w[MW];
       #pragma unroll
-      for (int q = 0; q < MASK_WORDS; q++) w[q] = (i < na && q < nbw) ? mb->rm[q * CAP_F + i] : 0u;
+      for (int q = 0; q < MW; q++) w[q] = (i < na && q < nbw) ? mb->rm[q * MS + i] : 0u;
       double px0 = 0, py0 = 0, px1 = 0, py1 = 0;
       uint32_t fa = 0;
       if (i < na) { px0 = LA.x0[i]; py0 = LA.y0[i]; px1 = LA.x1[i]; py1 = LA.y1[i]; fa = LA.fl[i]; }
@@ -431,7 +441,7 @@ __device__ bool refine_pair_t(const DLayer& P, const DLayer& R, uint32_t a, uint
       for (;;) {
         int j = -1;
         #pragma unroll
-        for (int q = 0; q < MASK_WORDS; q++)
+        for (int q = 0; q < MW; q++)
           if (j < 0 && w[q]) { j = (q << 5) + __ffs(w[q]) - 1; w[q] &= w[q] - 1; }
         if (!__any_sync(0xffffffffu, j >= 0)) break;
         if (j >= 0) {
@@ -515,7 +525,23 @@ __device__ bool refine_pair_t(const DLayer& P, const DLayer& R, uint32_t a, uint
     double s2 = 0.0, ai = 0, ao = 0, bi = 0, bo = 0;
     uint32_t bits = rtouch ? REL_TOUCH : 0;
     const bool rel = rp.want_relate != 0;
-    if constexpr (MASK) {   // visit only each edge's candidates, in increasing order, by walking the set bits
+    if constexpr (MASK && SELF > 0) {   // A's pass once, then each lane's recorded values added again in order
+      const int nbw = (nb + 31) >> 5;
+      double rec[MW];
+      double lin = 0.0, lon = 0.0;
+      int k = 0;
+      for (int i = lane; i < na; i += 32, k++) {
+        const uint32_t f = LA.fl[i];
+        rec[k] = edge_contrib_k<F>(LA.x0[i], LA.y0[i], LA.x1[i], LA.y1[i], LB, nb, inB_c, G, !(f & 1u), rel ? &lin : nullptr, &lon, &bits, f,
+                                   [&](auto&& visit) {
+                                     for (int q = 0; q < nbw; q++)
+                                       for (uint32_t m = mb->rm[q * MS + i]; m; m &= m - 1) visit((q << 5) + __ffs(m) - 1);
+                                   });
+        s2 += rec[k];
+      }
+      for (int q = 0; q < k; q++) s2 += rec[q];
+      ai = bi = lin; ao = bo = lon;
+    } else if constexpr (MASK) {   // visit only each edge's candidates, in increasing order, by walking the set bits
       const int nbw = (nb + 31) >> 5, naw = (na + 31) >> 5;
       for (int pass = 0; pass < 2; pass++) {
         const EList& LS = pass ? LB : LA;
@@ -594,7 +620,8 @@ template <bool F, bool S32 = false>
 __global__ void __launch_bounds__(RB_WARPS * 32, Cfg<F>::minb) k_refine(DLayer P, DLayer R, const uint2* __restrict__ pairs, uint64_t np,
                                                                         RefineArgs rp, uint8_t* flag, double* area, double4* ev, uint32_t* evb,
                                                                         uint32_t* heavy, unsigned long long* nheavy, unsigned long long* next,
-                                                                        unsigned long long* epairs, int run, int runs, int bin_cap) {
+                                                                        unsigned long long* epairs, int run, int runs, int bin_cap,
+                                                                        int skip_self) {
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ unsigned long long s_ep[RB_WARPS];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
@@ -610,6 +637,7 @@ __global__ void __launch_bounds__(RB_WARPS * 32, Cfg<F>::minb) k_refine(DLayer P
   }
   auto one = [&](uint64_t p) {
     const uint2 pr = pairs[p];
+    if (skip_self && pr.x == pr.y) return;   // a geometry with itself: the self bin's
     uint8_t f; double ar; double4 e4; uint32_t b4;
     const bool ok = refine_pair_t<F, false, false, F, S32>(P, R, pr.x, pr.y, rp, LA, LB, bin_cap, lane, f, ar, e4, b4, nullptr, &mbuf, &s_ep[wib]);
     if (lane == 0) {
@@ -637,6 +665,74 @@ __global__ void __launch_bounds__(RB_WARPS * 32, Cfg<F>::minb) k_refine(DLayer P
   } else {
     const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
     for (uint64_t p = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; p < np; p += nw) one(p);
+  }
+  __syncwarp();
+  if (lane == 0 && s_ep[wib]) atomicAdd(epairs, s_ep[wib]);
+}
+
+// Self bin (filtered variants, a layer joined with itself): the pairs of a geometry with itself, 24 % of a parcel
+// self-join's pairs and the costliest (every edge is local). One list of up to 2 x bin_cap edges per warp in the
+// shared memory two lists would take, row masks only, A's gather and contribution pass only (refine_pair_t SELF).
+constexpr int CAP_SELF = 2 * CAP_F;
+constexpr size_t SELF_LIST = (size_t)CAP_SELF * EDGE_BYTES_F;
+constexpr size_t SELF_MASK = (size_t)(CAP_SELF / 32) * CAP_SELF * sizeof(uint32_t);
+constexpr size_t SELF_SMEM = (size_t)RB_WARPS * (SELF_LIST + SELF_MASK);
+constexpr int SELF_MINB = 3;   // blocks per SM: 3 x 68 KB of shared memory
+
+// positions of the self pairs (a == b) among the candidate pairs, warp-aggregated (order free: outputs go by position)
+__global__ void k_self_index(const uint2* __restrict__ pairs, uint64_t np, uint32_t* sidx, unsigned long long* nself) {
+  const int lane = threadIdx.x & 31;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t base = (uint64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < np; base += stride) {   // warp-uniform
+    const uint64_t p = base + lane;
+    bool is = false;
+    if (p < np) { const uint2 pr = pairs[p]; is = pr.x == pr.y; }
+    const unsigned m = __ballot_sync(0xffffffffu, is);
+    unsigned long long at = 0;
+    if (lane == 0 && m) at = atomicAdd(nself, (unsigned long long)__popc(m));
+    at = __shfl_sync(0xffffffffu, at, 0);
+    if (is) sidx[at + __popc(m & ((1u << lane) - 1))] = (uint32_t)p;
+  }
+}
+
+template <bool S32>
+__global__ void __launch_bounds__(RB_WARPS * 32, SELF_MINB) k_refine_self(DLayer P, const uint2* __restrict__ pairs, const uint32_t* __restrict__ sidx,
+                                                                          const unsigned long long* nself, RefineArgs rp, uint8_t* flag, double* area,
+                                                                          double4* ev, uint32_t* evb, uint32_t* heavy, unsigned long long* nheavy,
+                                                                          unsigned long long* next, unsigned long long* epairs, int run, int runs,
+                                                                          int self_cap) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ unsigned long long s_ep[RB_WARPS];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  if (lane == 0) s_ep[wib] = 0;
+  __syncwarp();
+  const EList L = carve_f(smem + (size_t)wib * SELF_LIST, CAP_SELF);
+  MaskBuf mbuf;
+  mbuf.rm = reinterpret_cast<uint32_t*>(smem + (size_t)RB_WARPS * SELF_LIST + (size_t)wib * SELF_MASK);
+  mbuf.cm = nullptr;
+  const uint64_t n = *nself;   // written by k_self_index, launched before this kernel
+  for (int k = 0; k < runs; k++) {
+    unsigned long long h0 = 0;
+    if (lane == 0) h0 = atomicAdd(next, (unsigned long long)run);
+    h0 = __shfl_sync(0xffffffffu, h0, 0);
+    if (h0 >= n) break;
+    const uint64_t h1 = h0 + run < n ? h0 + run : n;
+    for (uint64_t h = h0; h < h1; h++) {
+      const uint32_t p = sidx[h];
+      const uint2 pr = pairs[p];
+      uint8_t f; double ar; double4 e4; uint32_t b4;
+      const bool ok = refine_pair_t<true, false, false, true, S32, CAP_SELF>(P, P, pr.x, pr.y, rp, L, L, self_cap, lane, f, ar, e4, b4, nullptr, &mbuf,
+                                                                            &s_ep[wib]);
+      if (lane == 0) {
+        if (!ok) { heavy[atomicAdd(nheavy, 1ull)] = p; flag[p] = 0; }
+        else {
+          flag[p] = f;
+          if (area) area[p] = ar;
+          if (ev) { ev[p] = e4; evb[p] = b4; }
+        }
+      }
+      __syncwarp();
+    }
   }
   __syncwarp();
   if (lane == 0 && s_ep[wib]) atomicAdd(epairs, s_ep[wib]);
@@ -756,11 +852,37 @@ static uint64_t refine_t(gsj_ctx* c, const gsj_layer* P, const gsj_layer* R, con
     sblocks = (int)(nwarps / 4);
     sbuf = c->scratch.as<unsigned char>(sg.per * nwarps);
   }
+  // self bin: a layer joined with itself (filtered variants); its pairs of a geometry with itself go to
+  // k_refine_self, the others stay in the shared-memory bin, and the two run side by side
+  const bool self = F && P == R;
+  int iblocks = 1, fblocks = 1;
+  uint32_t* sidx = nullptr;
+  const int self_cap = std::min(2 * bin_cap, CAP_SELF);
+  if (self) {
+    const int sbit = S32 ? 16 : 8;
+    if (!(c->refine_attr & sbit)) {
+      GSJ_CK(cudaFuncSetAttribute(k_refine_self<S32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SELF_SMEM));
+      c->refine_attr |= sbit;
+    }
+    sidx = c->selfidx.as<uint32_t>(np);
+    iblocks = (int)std::min<uint64_t>((np + 255) / 256, (uint64_t)c->sm_count * 8);
+    // at most one self pair per probe geometry: cover that many with `runs` fetches per warp, whole waves
+    const uint64_t ub = std::min<uint64_t>(np, P->d.n), per_block = (uint64_t)RB_WARPS * runs * run, wave = (uint64_t)c->sm_count * SELF_MINB;
+    uint64_t cover = (ub + per_block - 1) / per_block;
+    if (cover > wave) cover = (cover + wave - 1) / wave * wave;
+    const uint64_t spread = std::min<uint64_t>((ub + (uint64_t)RB_WARPS * run - 1) / ((uint64_t)RB_WARPS * run), wave);
+    fblocks = (int)std::min<uint64_t>(std::max<uint64_t>(cover, spread), 1u << 30);
+  }
   unsigned long long* h = c->h_counters.as<unsigned long long>(4);
-  auto a_main = kernel_args(k_refine<F, S32>, P->d, R->d, pairs, np, rp, flag, area, ev, evb, heavy, ctr, ctr + 2, ctr + 3, run, runs, bin_cap);
+  // counters: [0] oversized pairs, [1] error word, [2] pair counter, [3] local edge pairs, [4] scratch pair counter,
+  // [5] self pairs, [6] self pair counter
+  auto a_main = kernel_args(k_refine<F, S32>, P->d, R->d, pairs, np, rp, flag, area, ev, evb, heavy, ctr, ctr + 2, ctr + 3, run, runs, bin_cap,
+                            self ? 1 : 0);
   auto a_scr = kernel_args(k_refine_scratch<F>, P->d, R->d, pairs, heavy, ctr, rp, flag, area, ev, evb, sbuf, sg.cap, sg.cph, err, ctr + 3,
                            ctr + 4);
-  cudaKernelNodeParams km{}, ks{};
+  auto a_idx = kernel_args(k_self_index, pairs, np, sidx, ctr + 5);
+  auto a_self = kernel_args(k_refine_self<S32>, P->d, pairs, sidx, ctr + 5, rp, flag, area, ev, evb, heavy, ctr, ctr + 6, ctr + 3, run, runs, self_cap);
+  cudaKernelNodeParams km{}, ks{}, ki{}, kf{};
   km.func = (void*)k_refine<F, S32>;
   km.gridDim = dim3(blocks);
   km.blockDim = dim3(RB_WARPS * 32);
@@ -770,20 +892,41 @@ static uint64_t refine_t(gsj_ctx* c, const gsj_layer* P, const gsj_layer* R, con
   ks.gridDim = dim3(std::max(sblocks, 1));
   ks.blockDim = dim3(128);
   ks.kernelParams = a_scr.ptr;
-  RefineGraph& g = c->rgraph[(S32 ? 2 : (F ? 1 : 0)) * 2 + (scr ? 1 : 0)];
+  ki.func = (void*)k_self_index;
+  ki.gridDim = dim3(iblocks);
+  ki.blockDim = dim3(256);
+  ki.kernelParams = a_idx.ptr;
+  kf.func = (void*)k_refine_self<S32>;
+  kf.gridDim = dim3(fblocks);
+  kf.blockDim = dim3(RB_WARPS * 32);
+  kf.sharedMemBytes = (unsigned)SELF_SMEM;
+  kf.kernelParams = a_self.ptr;
+  RefineGraph& g = c->rgraph[((S32 ? 2 : (F ? 1 : 0)) * 2 + (scr ? 1 : 0)) * 2 + (self ? 1 : 0)];
   if (!g.exec) {   // the graph is kept with its executable: the node handles used for the updates belong to it
-    if (!g.graph) GSJ_CK(cudaGraphCreate(&g.graph, 0));
-    if (!g.n_main) GSJ_CK(cudaGraphAddKernelNode(&g.n_main, g.graph, nullptr, 0, &km));
-    if (scr && !g.n_scr) GSJ_CK(cudaGraphAddKernelNode(&g.n_scr, g.graph, &g.n_main, 1, &ks));
+    if (!g.graph) {
+      GSJ_CK(cudaGraphCreate(&g.graph, 0));
+      // shared-memory bin || (self index -> self bin), then the scratch bin after both
+      GSJ_CK(cudaGraphAddKernelNode(&g.n_main, g.graph, nullptr, 0, &km));
+      std::vector<cudaGraphNode_t> before{g.n_main};
+      if (self) {
+        GSJ_CK(cudaGraphAddKernelNode(&g.n_idx, g.graph, nullptr, 0, &ki));
+        GSJ_CK(cudaGraphAddKernelNode(&g.n_self, g.graph, &g.n_idx, 1, &kf));
+        before.push_back(g.n_self);
+      }
+      if (scr) GSJ_CK(cudaGraphAddKernelNode(&g.n_scr, g.graph, before.data(), before.size(), &ks));
+    }
     GSJ_CK(cudaGraphInstantiate(&g.exec, g.graph, 0));
   } else {
     GSJ_CK(cudaGraphExecKernelNodeSetParams(g.exec, g.n_main, &km));
+    if (self) {
+      GSJ_CK(cudaGraphExecKernelNodeSetParams(g.exec, g.n_idx, &ki));
+      GSJ_CK(cudaGraphExecKernelNodeSetParams(g.exec, g.n_self, &kf));
+    }
     if (scr) GSJ_CK(cudaGraphExecKernelNodeSetParams(g.exec, g.n_scr, &ks));
   }
-  // heavy count, error word, pair counter, local edge pairs, scratch pair counter
-  GSJ_CK(cudaMemsetAsync(ctr, 0, 40, s));
+  GSJ_CK(cudaMemsetAsync(ctr, 0, 7 * sizeof(unsigned long long), s));
   GSJ_CK(cudaGraphLaunch(g.exec, s));
-  c->launches += scr ? 2 : 1;
+  c->launches += 1 + (scr ? 1 : 0) + (self ? 2 : 0);
   GSJ_CK(cudaMemcpyAsync(h, ctr, 32, cudaMemcpyDeviceToHost, s));
   GSJ_CK(cudaStreamSynchronize(s));
   if (reinterpret_cast<int*>(h + 1)[0]) throw Error(GSJ_ERR_CUDA, "oversized pair exceeded the scratch edge capacity");
