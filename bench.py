@@ -588,6 +588,7 @@ def main():
     ap.add_argument("--no-serve", action="store_true", help="skip the serving-latency leg (gsjd under a Poisson request stream)")
     ap.add_argument("--no-reference-check", action="store_true", help="skip the row-by-row comparison with the reference engine's driver")
     ap.add_argument("--serve-small", action="store_true", help="the serving leg on a scaled-down copy of its workload (quick runs)")
+    ap.add_argument("--no-tune", action="store_true", help="skip the refinement autotuner: the default launch shape (profiling)")
     ap.add_argument("--op", default="relate", choices=["relate", "area", "dwithin", "erode", "cluster"])
     ap.add_argument("--arms", default="filtered,plain", help="refinement variants an --op run times (filtered first; for profiling one)")
     ap.add_argument("--shard", action="store_true",
@@ -636,7 +637,8 @@ def main():
     # untimed: the refinement autotuner picks the filtered variant's launch shape on a sample of this join's
     # candidate pairs; the plain variant runs with the default shape (the reference's fixed scheme)
     default_shape = eng.refine_shape
-    tune = eng.tune_refine(L, L, want_area=False, want_relate=True, refine_mode=gsj.GSJ_REFINE_FILTERED, max_pairs=1 << 21)
+    tune = ({"best": default_shape, "start_ms": None, "best_ms": None, "sample_pairs": 0, "shapes_tried": 0} if args.no_tune else
+            eng.tune_refine(L, L, want_area=False, want_relate=True, refine_mode=gsj.GSJ_REFINE_FILTERED, max_pairs=1 << 21))
     for _ in range(args.warmup):
         timed_join(gsj.GSJ_REFINE_FILTERED)
     res = {}
