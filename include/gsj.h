@@ -189,9 +189,10 @@ int gsj_refine_pairs(gsj_ctx* ctx, const gsj_layer* P, const gsj_layer* R, const
  * d_ev[4np] with d_evb[np]. Its scratch is one static device array of GSJ_NOALLOC_SCRATCH_BYTES per GPU (held by
  * every GPU that loads the library, until exit); layers whose largest geometry needs a larger per-warp slab
  * (more than ~466k edges) are rejected with GSJ_ERR_ARG. All calls share that array: calls that overlap on the GPU
- * race and must be serialised. The first call on a device looks up the array's address; make it before any
- * stream capture. The address is kept until the process exits: do not call this on a device after resetting it
- * (cudaDeviceReset). Runs on the context's stream and returns after it finished. */
+ * race and must be serialised. The address of the array is looked up on the first call on a device and kept until
+ * the process exits: do not call this on a device after resetting it (cudaDeviceReset). Runs on the context's
+ * stream and synchronises it before returning (it reads a status word back), so a call cannot be captured into a
+ * CUDA graph. */
 #define GSJ_NOALLOC_SCRATCH_BYTES (32u << 20)
 int gsj_refine_pairs_noalloc(gsj_ctx* ctx, const gsj_layer* P, const gsj_layer* R, const uint32_t* d_pairs, uint64_t np,
                              const gsj_refine_params* rp, uint8_t* d_flag, double* d_area, double* d_ev, uint32_t* d_evb);

@@ -11,9 +11,10 @@
 // geometry edge count rounded up to 8; calls whose one-warp slab does not fit are rejected with GSJ_ERR_ARG.
 // Every call on a device uses the same array: calls that overlap on the GPU (other streams, other contexts on
 // the device, other host threads) race on it and must be serialised by the caller. The first call on a device
-// looks the array's device address up (cudaGetSymbolAddress); make that first call before any stream capture. The
-// address is kept for the life of the process: a host application that resets a device (cudaDeviceReset) must not
-// call this entry point on that device afterwards.
+// looks the array's device address up (cudaGetSymbolAddress). The address is kept for the life of the process: a
+// host application that resets a device (cudaDeviceReset) must not call this entry point on that device afterwards.
+// Every call synchronises the context's stream (the status word comes back to the host), so no call can be captured
+// into a CUDA graph.
 #include <mutex>
 #include "engine.h"
 
