@@ -676,15 +676,18 @@ def main():
     del b
 
     # end-to-end through the C ABI from pinned host buffers: upload + LBVH + join + D2H of the rows
-    e2e_ms, e2e_pairs = [], 0
+    e2e_ms, e2e_pairs, e2e_parts = [], 0, []
     for i in range(1 + args.steps):
         t = time.perf_counter()
-        Lx = eng.upload_polygons(hps)
+        Lx = eng.upload_polygons(hps)   # returns after the layer and its LBVH are on the device
+        t1 = time.perf_counter()
         r = eng.join(Lx, Lx, want_area=False, want_relate=True, upper=True, **shard)
+        t2 = time.perf_counter()
         Lx.free()
         dt = (time.perf_counter() - t) * 1000.0
         if i:
             e2e_ms.append(dt); e2e_pairs += len(r.pairs)
+            e2e_parts.append(((t1 - t) * 1000.0, (t2 - t1) * 1000.0))
     h2d = int(ps.gro.nbytes + ps.rvo.nbytes + ps.xy.nbytes)
     d2h = int(len(r.pairs) * 12)
 
@@ -710,7 +713,7 @@ def main():
     try:
         for ln in open(os.path.join(ROOT, "profiles", "traffic_per_launch.txt")):
             k, v = ln.split()[:2]
-            if k == "k_refine":   # measured on a smaller case, scaled by the candidate pairs of one launch
+            if k == "k_refine":   # DRAM bytes per candidate pair from one ncu pass over this join, times its candidate pairs
                 traffic = float(v) * float(st[0]["candidates"])
     except OSError:
         pass
@@ -748,8 +751,12 @@ def main():
         "reference_check": refcheck,
         "phases_ms": {k: float(np.mean([s[k] for s in st])) for k in ("traverse_ms", "refine_ms", "compact_ms", "copy_ms")},
         "e2e": {"value": e2e_value, "unit": "pairs/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                "ms_per_step": e2e_tot / args.steps},
-        "roofline": {"kernel": "k_refine<1> (+k_refine_scratch<1>)", "bound": "fp64", "achieved": flops / (refine_ms / 1000.0) / 1e12,
+                "ms_per_step": e2e_tot / args.steps,
+                "parts_ms": {"upload_and_lbvh": float(np.mean([a for a, _ in e2e_parts])),
+                             "join_and_rows_to_host": float(np.mean([b for _, b in e2e_parts])),
+                             "what": "host clock: gsj_layer_upload_polygons (H2D of the arrays, device prep, LBVH), then gsj_join with the "
+                                     "rows copied out of the library's pinned buffers"}},
+        "roofline": {"kernel": "k_refine<1> + k_refine_self + k_refine_scratch<1> (the refinement graph)", "bound": "fp64", "achieved": flops / (refine_ms / 1000.0) / 1e12,
                      "peak": FP64_PEAK_TFLOPS, "unit": "TFLOP/s", "frac": flops / (refine_ms / 1000.0) / 1e12 / FP64_PEAK_TFLOPS,
                      "traffic": traffic, "peak_source": "B200 FP64 specification (HGX B200: 296 TFLOPS / 8 GPUs); not measured here",
                      "work": {"edge_pairs_per_launch": edge_pairs, "flops_per_edge_pair": FLOPS_PER_EDGE_PAIR,
