@@ -36,14 +36,9 @@ static __device__ int collect(const Frame& A, const Box& ov, EList L, int cap, i
     for (uint64_t base = s; base + 1 < e; base += 32) {
       const uint64_t i = base + lane;
       bool in = false;
-      // each lane loads vertex i once; its edge's end vertex i + 1 is the next lane's (lane 31 loads its own)
-      double vx = 0, vy = 0;
-      if (i < e) A.v(i, vx, vy);
-      double nx = __shfl_down_sync(0xffffffffu, vx, 1), ny = __shfl_down_sync(0xffffffffu, vy, 1);
-      if (lane == 31 && i + 1 < e) A.v(i + 1, nx, ny);
       double x0 = 0, y0 = 0, x1 = 0, y1 = 0; uint32_t fl = 0;
       if (i + 1 < e) {
-        x0 = vx; y0 = vy; x1 = nx; y1 = ny;
+        A.v(i, x0, y0); A.v(i + 1, x1, y1);
         if (S.synb) {
           fl = (uint32_t)S.syn(i) | (S.syn(i > s ? i - 1 : e - 2) ? 2u : 0u) | (S.syn(i + 2 < e ? i + 1 : s) ? 4u : 0u);
         }
