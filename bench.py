@@ -336,7 +336,7 @@ def run_op(args, rank, local, ws):
     if op == "area":
         A, B = gen.layer_cfg_parcels_small(20000, seed=rank), gen.layer_cfg_zones(50, seed=1)
         workload = "intersects + area, 20k Voronoi zones (6-40 vertices, LA box) x 50 zones"
-        metric, unit = "join pairs/s (intersects + area, filtered+batched FP64)", "pairs/s"
+        metric, unit = "join pairs/s (intersects + area, filtered FP64 refinement)", "pairs/s"
     elif op == "dwithin":
         box = (-119.0, 33.0, -118.0, 34.0)
         A, B = None, gen.layer_parcels(1_000_000, box, seed=rank)

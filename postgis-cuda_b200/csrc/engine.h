@@ -83,6 +83,9 @@ struct Timer {
   ~Timer() { if (a) cudaEventDestroy(a); if (b) cudaEventDestroy(b); }
   void start() { GSJ_CK(cudaEventRecord(a, s)); }
   float stop() { GSJ_CK(cudaEventRecord(b, s)); GSJ_CK(cudaEventSynchronize(b)); float ms = 0; GSJ_CK(cudaEventElapsedTime(&ms, a, b)); return ms; }
+  // without a host wait: record the end now, read the time after a later stream sync
+  void mark_end() { GSJ_CK(cudaEventRecord(b, s)); }
+  float elapsed() { float ms = 0; GSJ_CK(cudaEventElapsedTime(&ms, a, b)); return ms; }
 };
 
 }  // namespace gsj
@@ -152,7 +155,8 @@ struct gsj_ctx {
   template <class Fn> void each_buf(Fn&& fn) {
     for (gsj::DevBuf* b : {&counters, &cand, &flag, &area, &ev, &evb, &heavy, &selfidx, &scratch, &keep, &opairs, &oarea, &oev, &oevb, &ocode, &tmp, &keys, &keys2, &idx, &idx2, &agg_area, &agg_ev, &agg_evb, &agg_flag, &qbb, &uf, &misc1, &misc2, &misc3, &er_pf, &er_keep, &er_off, &er_pairs, &er_flag, &er_heavy, &er_tiles, &er_tiles2, &er_slab, &er_again, &er_scr, &er_ctr, &er_tmp, &enc_in, &enc_cnt, &enc_pre, &enc_blk, &enc_out}) fn(*b);
   }
-  gsj::PinnedBuf h_counters, h_pairs, h_area, h_code, h_where, h_enc;
+  gsj::PinnedBuf h_counters, h_refine, h_pairs, h_area, h_code, h_where, h_enc;
+  bool refine_pending = false;   // a refinement's counters are on their way to h_refine (refine_enqueue)
 };
 
 namespace gsj {
@@ -185,6 +189,12 @@ gsj_join_opts opts_or_default(const gsj_join_opts* o);
 // per-pair refinement (flag, area, ev, evb); returns the number of pairs that took the oversized path
 uint64_t refine(gsj_ctx* c, const gsj_layer* P, const gsj_layer* R, const uint2* pairs, uint64_t np, const RefineArgs& rp, int mode,
                 uint8_t* flag, double* area, double4* ev, uint32_t* evb);
+// the same in two halves, for callers with a stream sync of their own after it: refine_enqueue puts the bins and the
+// copy of their counters on the stream; refine_result, after the caller's next sync, checks the error word and
+// returns the oversized-pair count (the outputs must not be used before it returned without throwing)
+void refine_enqueue(gsj_ctx* c, const gsj_layer* P, const gsj_layer* R, const uint2* pairs, uint64_t np, const RefineArgs& rp, int mode,
+                    uint8_t* flag, double* area, double4* ev, uint32_t* evb);
+uint64_t refine_result(gsj_ctx* c);
 
 // refinement launch shapes (tune.cu)
 bool shape_valid(const RefineShape& s);

@@ -160,7 +160,7 @@ void run_join(gsj_ctx* c, const gsj_layer* P, const gsj_layer* R, const RefineAr
   cudaStream_t s = c->stream;
   const bool agg = (P->d.parent || R->d.parent) && !o.no_agg;
   const bool rel = rp.want_relate != 0;
-  Timer tm(s);
+  Timer tm(s), tr(s);
   // Morton-ordered probes for coherent traversal; batches by index ranges keep a parent's pieces together
   bool whole = false;
   const std::vector<Batch> batches = make_batches(P, o, whole);
@@ -174,20 +174,23 @@ void run_join(gsj_ctx* c, const gsj_layer* P, const gsj_layer* R, const RefineAr
     st.batches++;
     if (pre && *pre && np) np = (*pre)(pairs, np);
     if (!np) continue;
-    tm.start();
+    tr.start();
     uint8_t* flag = c->flag.as<uint8_t>(np);
     double* area = (rp.want_area) ? c->area.as<double>(np) : nullptr;
     double4* ev = rel ? c->ev.as<double4>(np) : nullptr;
     uint32_t* evb = rel ? c->evb.as<uint32_t>(np) : nullptr;
-    // area is needed for the piece fold or the output; relate-only joins still fold (zero) areas
-    st.heavy += refine(c, P, R, pairs, np, rp, o.refine_mode, flag, area, ev, evb);
-    st.refine_ms += tm.stop();
+    // area is needed for the piece fold or the output; relate-only joins still fold (zero) areas.
+    // The refinement's counters come back with the compaction's count: one host round trip for both.
+    refine_enqueue(c, P, R, pairs, np, rp, o.refine_mode, flag, area, ev, evb);
+    tr.mark_end();
     tm.start();
     uint32_t* keep = c->keep.as<uint32_t>(np);
     uint32_t* off = c->idx.as<uint32_t>(np);
     k_keep<<<grid_for(np, 256), 256, 0, s>>>(flag, np, agg ? 1 : 0, keep); c->launches++;
     exclusive_scan(c, keep, off, np);
     uint64_t nk = read_last(c, off, keep, np);
+    st.heavy += refine_result(c);
+    st.refine_ms += tr.elapsed();
     JoinOut out{nullptr, nullptr, nullptr, 0};
     if (!agg) {
       out.pairs = c->opairs.as<uint2>(nk);

@@ -814,8 +814,8 @@ static ScratchGeom scratch_geom(const gsj_layer* P, const gsj_layer* R) {
 // oversized; it reads their count on the device, so no host round trip separates the bins); then one stream sync.
 // The executable graph is built once per context and variant and re-parameterised per call.
 template <bool F, bool S32 = false>
-static uint64_t refine_t(gsj_ctx* c, const gsj_layer* P, const gsj_layer* R, const uint2* pairs, uint64_t np, const RefineArgs& rp, uint8_t* flag,
-                         double* area, double4* ev, uint32_t* evb) {
+static void refine_t(gsj_ctx* c, const gsj_layer* P, const gsj_layer* R, const uint2* pairs, uint64_t np, const RefineArgs& rp, uint8_t* flag,
+                     double* area, double4* ev, uint32_t* evb) {
   cudaStream_t s = c->stream;
   const int bit = S32 ? 4 : (F ? 2 : 1);
   if (!(c->refine_attr & bit)) {
@@ -873,7 +873,7 @@ static uint64_t refine_t(gsj_ctx* c, const gsj_layer* P, const gsj_layer* R, con
     const uint64_t spread = std::min<uint64_t>((ub + (uint64_t)RB_WARPS * run - 1) / ((uint64_t)RB_WARPS * run), wave);
     fblocks = (int)std::min<uint64_t>(std::max<uint64_t>(cover, spread), 1u << 30);
   }
-  unsigned long long* h = c->h_counters.as<unsigned long long>(4);
+  unsigned long long* h = c->h_refine.as<unsigned long long>(4);
   // counters: [0] oversized pairs, [1] error word, [2] pair counter, [3] local edge pairs, [4] scratch pair counter,
   // [5] self pairs, [6] self pair counter
   auto a_main = kernel_args(k_refine<F, S32>, P->d, R->d, pairs, np, rp, flag, area, ev, evb, heavy, ctr, ctr + 2, ctr + 3, run, runs, bin_cap,
@@ -928,18 +928,31 @@ static uint64_t refine_t(gsj_ctx* c, const gsj_layer* P, const gsj_layer* R, con
   GSJ_CK(cudaGraphLaunch(g.exec, s));
   c->launches += 1 + (scr ? 1 : 0) + (self ? 2 : 0);
   GSJ_CK(cudaMemcpyAsync(h, ctr, 32, cudaMemcpyDeviceToHost, s));
-  GSJ_CK(cudaStreamSynchronize(s));
-  if (reinterpret_cast<int*>(h + 1)[0]) throw Error(GSJ_ERR_CUDA, "oversized pair exceeded the scratch edge capacity");
+  c->refine_pending = true;
+}
+
+void refine_enqueue(gsj_ctx* c, const gsj_layer* P, const gsj_layer* R, const uint2* pairs, uint64_t np, const RefineArgs& rp, int mode,
+                    uint8_t* flag, double* area, double4* ev, uint32_t* evb) {
+  if (!np) return;
+  if (mode == GSJ_REFINE_FILTERED_FP32) refine_t<true, true>(c, P, R, pairs, np, rp, flag, area, ev, evb);
+  else if (mode == GSJ_REFINE_FILTERED) refine_t<true>(c, P, R, pairs, np, rp, flag, area, ev, evb);
+  else refine_t<false>(c, P, R, pairs, np, rp, flag, area, ev, evb);
+}
+
+uint64_t refine_result(gsj_ctx* c) {
+  if (!c->refine_pending) return 0;
+  c->refine_pending = false;
+  const unsigned long long* h = c->h_refine.as<unsigned long long>(4);
+  if (reinterpret_cast<const int*>(h + 1)[0]) throw Error(GSJ_ERR_CUDA, "oversized pair exceeded the scratch edge capacity");
   c->edge_pairs += h[3];
   return h[0];
 }
 
 uint64_t refine(gsj_ctx* c, const gsj_layer* P, const gsj_layer* R, const uint2* pairs, uint64_t np, const RefineArgs& rp, int mode,
                 uint8_t* flag, double* area, double4* ev, uint32_t* evb) {
-  if (!np) return 0;
-  if (mode == GSJ_REFINE_FILTERED_FP32) return refine_t<true, true>(c, P, R, pairs, np, rp, flag, area, ev, evb);
-  return mode == GSJ_REFINE_FILTERED ? refine_t<true>(c, P, R, pairs, np, rp, flag, area, ev, evb)
-                                     : refine_t<false>(c, P, R, pairs, np, rp, flag, area, ev, evb);
+  refine_enqueue(c, P, R, pairs, np, rp, mode, flag, area, ev, evb);
+  GSJ_CK(cudaStreamSynchronize(c->stream));
+  return refine_result(c);
 }
 
 }  // namespace gsj
