@@ -41,7 +41,8 @@ struct PairGeo { Box ov; double tol, eps_par, snap, cx, cy; };
 // Only the oversized pairs of the scratch kernel use the buckets: for the shared-memory bins the grid is faster.
 constexpr int NBK = 16, LCAP = 32;
 constexpr int GRID_MAX = 2048;   // scratch kernel: na x nb up to this: the grid sweep
-struct FlatBuf { uint32_t* cp; uint16_t* pj; uint32_t* sa; uint32_t* sb; uint32_t* bl; uint32_t* boff; int cap, blcap; };   // cap: entries of cp / pj
+// cap: entries of cp / pj; rec: a self pair's recorded contributions, one per A edge (the scratch kernel's B list)
+struct FlatBuf { uint32_t* cp; uint16_t* pj; uint32_t* sa; uint32_t* sb; uint32_t* bl; uint32_t* boff; int cap, blcap; double* rec; };
 
 __device__ __forceinline__ void warp_exscan(uint32_t* a, int n, int lane) {   // in place over a[0 .. n)
   uint32_t run = 0;
@@ -560,6 +561,21 @@ __device__ bool refine_pair_t(const DLayer& P, const DLayer& R, uint32_t a, uint
         }
         if (pass) { bi = lin; bo = lon; } else { ai = lin; ao = lon; }
       }
+    } else if constexpr (FLAT && SELF > 0) {   // the self pair's A pass, recorded per edge, then added again in order
+      const uint32_t* cp = fb->cp;
+      double lin = 0.0, lon = 0.0;
+      for (int i = lane; i < na; i += 32) {
+        const uint32_t f = LA.fl[i];
+        const int r0 = (int)fb->sa[i], r1 = (int)fb->sa[i + 1];
+        const double v = edge_contrib_k<F>(LA.x0[i], LA.y0[i], LA.x1[i], LA.y1[i], LB, nb, inB_c, G, !(f & 1u), rel ? &lin : nullptr, &lon, &bits, f,
+                                           [&](auto&& visit) {
+                                             for (int e = r0; e < r1; e++) visit((int)(cp[e] >> 16));
+                                           });
+        fb->rec[i] = v;
+        s2 += v;
+      }
+      for (int i = lane; i < na; i += 32) s2 += fb->rec[i];
+      ai = bi = lin; ao = bo = lon;
     } else if constexpr (FLAT) {   // visit only each edge's candidates, in the same increasing order; one call site for both passes
       const uint32_t* cp = fb->cp;
       const uint16_t* pj = fb->pj;
@@ -749,7 +765,7 @@ template <bool F>
 __global__ void __launch_bounds__(128) k_refine_scratch(DLayer P, DLayer R, const uint2* __restrict__ pairs, const uint32_t* __restrict__ heavy,
                                                        const unsigned long long* nheavy, RefineArgs rp, uint8_t* flag, double* area, double4* ev, uint32_t* evb,
                                                        unsigned char* scratch, int cap, int cph, int* err, unsigned long long* epairs,
-                                                       unsigned long long* next) {
+                                                       unsigned long long* next, int same_layer) {
   const int lane = threadIdx.x & 31;
   const uint64_t nh = *nheavy;   // written by the shared-memory bin launched before this kernel on the same stream
   if (nh == 0) return;
@@ -767,6 +783,7 @@ __global__ void __launch_bounds__(128) k_refine_scratch(DLayer P, DLayer R, cons
     fb.pj = reinterpret_cast<uint16_t*>(fb.boff + (NBK + 1));
     fb.cap = cph;
     fb.blcap = 2 * cap + 64;
+    fb.rec = LB.x0;   // cap doubles, unused by a self pair's single list
   }
   (void)nw;
   for (;;) {   // one listed pair at a time from a counter: their costs vary widely
@@ -779,7 +796,10 @@ __global__ void __launch_bounds__(128) k_refine_scratch(DLayer P, DLayer R, cons
     uint8_t f; double ar; double4 e4; uint32_t b4;
     bool ok;
     if constexpr (F) {   // candidate entries pack both edge indices in 16 bits each
-      ok = cap <= 0xFFFF && refine_pair_t<F, true, true>(P, R, pr.x, pr.y, rp, LA, LB, cap, lane, f, ar, e4, b4, &fb, nullptr, &ep);
+      if (same_layer && pr.x == pr.y)   // a geometry with itself: one list, one contribution pass (B's list records it)
+        ok = cap <= 0xFFFF && refine_pair_t<F, true, true, false, false, 1>(P, P, pr.x, pr.y, rp, LA, LA, cap, lane, f, ar, e4, b4, &fb, nullptr, &ep);
+      else
+        ok = cap <= 0xFFFF && refine_pair_t<F, true, true>(P, R, pr.x, pr.y, rp, LA, LB, cap, lane, f, ar, e4, b4, &fb, nullptr, &ep);
       if (!ok) ok = refine_pair_t<F, false>(P, R, pr.x, pr.y, rp, LA, LB, cap, lane, f, ar, e4, b4, nullptr, nullptr, &ep);
     } else {
       ok = refine_pair_t<F, false>(P, R, pr.x, pr.y, rp, LA, LB, cap, lane, f, ar, e4, b4, nullptr, nullptr, &ep);
@@ -879,7 +899,7 @@ static void refine_t(gsj_ctx* c, const gsj_layer* P, const gsj_layer* R, const u
   auto a_main = kernel_args(k_refine<F, S32>, P->d, R->d, pairs, np, rp, flag, area, ev, evb, heavy, ctr, ctr + 2, ctr + 3, run, runs, bin_cap,
                             self ? 1 : 0);
   auto a_scr = kernel_args(k_refine_scratch<F>, P->d, R->d, pairs, heavy, ctr, rp, flag, area, ev, evb, sbuf, sg.cap, sg.cph, err, ctr + 3,
-                           ctr + 4);
+                           ctr + 4, P == R ? 1 : 0);
   auto a_idx = kernel_args(k_self_index, pairs, np, sidx, ctr + 5);
   auto a_self = kernel_args(k_refine_self<S32>, P->d, pairs, sidx, ctr + 5, rp, flag, area, ev, evb, heavy, ctr, ctr + 6, ctr + 3, run, runs, self_cap);
   cudaKernelNodeParams km{}, ks{}, ki{}, kf{};
