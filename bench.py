@@ -301,6 +301,9 @@ def serving_leg(cfg, workers=4):
             finally:
                 D.stop(p)
                 log.close()
+            if mode in out:   # the launch shape the daemon's autotuner chose when the resident layer was loaded
+                tl = [ln.strip() for ln in open(os.path.join(d, f"gsjd_{mode}.log")) if "tune resident:" in ln]
+                out[mode]["autotuner"] = tl[-1].split("tune resident: ", 1)[1] if tl else None
         out["pairs_per_s_saturated"] = {m: out[m]["saturated"]["rows_per_s"] for m, _ in SERVE_ARMS}
         out["p99_ratio_plain_over_filtered"] = out["plain"]["p99_ms"] / out["filtered"]["p99_ms"] if out["filtered"]["p99_ms"] else None
         out["saturated_ratio_filtered_over_plain"] = (out["pairs_per_s_saturated"]["filtered"] / out["pairs_per_s_saturated"]["plain"]

@@ -486,8 +486,9 @@ std::string build_layer(const std::string& name, const std::string& path, int su
       gsj_refine_params rp;
       gsj_refine_params_default(&rp);
       gsj_tune_result tr;
-      // runs stays: it bounds how long a refinement block holds an SM while other requests' kernels wait for one
-      const int rc = gsj_tune_refine(lease.get(), L->h, L->h, &rp, g_cfg.refine_mode, 1, 1u << 20, GSJ_TUNE_KEEP_RUNS, &tr);
+      // run and runs stay: their product bounds how long a refinement block holds an SM while other requests'
+      // kernels (high-priority streams) wait for one
+      const int rc = gsj_tune_refine(lease.get(), L->h, L->h, &rp, g_cfg.refine_mode, 1, 1u << 20, GSJ_TUNE_KEEP_RUN | GSJ_TUNE_KEEP_RUNS, &tr);
       if (rc) logf("tune %s: %s", name.c_str(), gsj_last_error(lease.get()));
       else {
         std::lock_guard<std::mutex> sl(g_shape_m);

@@ -175,6 +175,32 @@ def de9im_match(code: int, pattern: str) -> bool:
     return bool(lib().gsj_de9im_match(code, pattern.encode()))
 
 
+_COPY_POOL = None
+
+
+def _copy_out(ptr, count, dtype):
+    """count elements from a host pointer the library owns only during a sink call, into a new numpy array. Large
+    arrays are copied in 8 slices on a small thread pool (ctypes.memmove releases the GIL), so a sink's copy of a
+    few hundred MB of rows is not one thread's memcpy."""
+    global _COPY_POOL
+    out = np.empty(count, dtype)
+    nbytes = out.nbytes
+    src = ctypes.cast(ptr, ctypes.c_void_p).value
+    if nbytes < (8 << 20):
+        if nbytes:
+            ctypes.memmove(out.ctypes.data, src, nbytes)
+        return out
+    if _COPY_POOL is None:
+        import concurrent.futures
+        _COPY_POOL = concurrent.futures.ThreadPoolExecutor(max_workers=8, thread_name_prefix="gsj-copy")
+    step = ((nbytes + 7) // 8 + 63) & ~63
+    dst = out.ctypes.data
+    futs = [_COPY_POOL.submit(ctypes.memmove, dst + o, src + o, min(step, nbytes - o)) for o in range(0, nbytes, step)]
+    for f in futs:
+        f.result()
+    return out
+
+
 def _join_chunks(chunks, dtype):
     """The batches' arrays as one (a single batch is returned as it is, without another copy)."""
     if not chunks:
@@ -353,11 +379,11 @@ class Engine:
         def sink(user, pairs, area, code, n):
             if not collect:
                 return 0
-            chunks_p.append(np.ctypeslib.as_array(pairs, (n * 2,)).copy())
+            chunks_p.append(_copy_out(pairs, n * 2, np.uint32))
             if area:
-                chunks_a.append(np.ctypeslib.as_array(area, (n,)).copy())
+                chunks_a.append(_copy_out(area, n, np.float64))
             if code:
-                chunks_c.append(np.ctypeslib.as_array(code, (n,)).copy())
+                chunks_c.append(_copy_out(code, n, np.uint32))
             return 0
 
         cb = JOIN_SINK(sink)

@@ -52,3 +52,18 @@ def test_errors_are_status_codes_not_exits():
 def test_result_types_construct_without_gpu():
     r = gsj.JoinResult(np.zeros((0, 2), np.uint32), None, None, {"candidates": 0})
     assert len(r.pairs) == 0 and r.stats["candidates"] == 0
+
+
+def test_sink_copy_out_matches_source():
+    """The binding's copy of a sink's rows out of library-owned host memory (sliced across threads above 8 MiB)."""
+    import ctypes
+
+    import numpy as np
+
+    import gsj
+    rng = np.random.default_rng(3)
+    for n, dt in ((0, np.uint32), (7, np.float64), (3_000_001, np.uint32), (1_500_007, np.float64)):
+        src = rng.integers(0, 2**31, n).astype(dt)
+        ptr = src.ctypes.data_as(ctypes.POINTER(np.ctypeslib.as_ctypes_type(dt)))
+        out = gsj._copy_out(ptr, n, dt)
+        assert out.dtype == dt and np.array_equal(out, src) and out.ctypes.data != src.ctypes.data

@@ -347,5 +347,5 @@ def test_tune_at_load_same_rows(env):
     finally:
         env.cl.drop("big")
     text = logp.read_text()
-    assert "tune big: shape run=" in text, text[-2000:]
+    assert "tune big: shape run=4 runs=32 " in text, text[-2000:]   # the block-lifetime fields stay at their defaults
     assert got == want and got_rel == want_rel and len(want) > 100_000
