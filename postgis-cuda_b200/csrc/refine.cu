@@ -687,13 +687,14 @@ __global__ void __launch_bounds__(RB_WARPS * 32, Cfg<F>::minb) k_refine(DLayer P
 }
 
 // Self bin (filtered variants, a layer joined with itself): the pairs of a geometry with itself, 24 % of a parcel
-// self-join's pairs and the costliest (every edge is local). One list of up to 2 x bin_cap edges per warp in the
-// shared memory two lists would take, row masks only, A's gather and contribution pass only (refine_pair_t SELF).
-constexpr int CAP_SELF = 2 * CAP_F;
+// self-join's pairs and the costliest (every edge is local). One list of up to 192 edges per warp (a multiple of 32
+// for the row masks; the largest that keeps 4 blocks of 4 warps per SM: 256 with 3 blocks measured 5 % slower),
+// row masks only, A's gather and contribution pass only (refine_pair_t SELF).
+constexpr int CAP_SELF = 192;
 constexpr size_t SELF_LIST = (size_t)CAP_SELF * EDGE_BYTES_F;
 constexpr size_t SELF_MASK = (size_t)(CAP_SELF / 32) * CAP_SELF * sizeof(uint32_t);
 constexpr size_t SELF_SMEM = (size_t)RB_WARPS * (SELF_LIST + SELF_MASK);
-constexpr int SELF_MINB = 3;   // blocks per SM: 3 x 68 KB of shared memory
+constexpr int SELF_MINB = 4;   // blocks per SM: 4 x 46 KB of shared memory
 
 // positions of the self pairs (a == b) among the candidate pairs, warp-aggregated (order free: outputs go by position)
 __global__ void k_self_index(const uint2* __restrict__ pairs, uint64_t np, uint32_t* sidx, unsigned long long* nself) {
@@ -877,7 +878,7 @@ static void refine_t(gsj_ctx* c, const gsj_layer* P, const gsj_layer* R, const u
   const bool self = F && P == R;
   int iblocks = 1, fblocks = 1;
   uint32_t* sidx = nullptr;
-  const int self_cap = std::min(2 * bin_cap, CAP_SELF);
+  const int self_cap = std::min(bin_cap + bin_cap / 2, CAP_SELF);   // the self bin holds 1.5 x the shared-memory bin
   if (self) {
     const int sbit = S32 ? 16 : 8;
     if (!(c->refine_attr & sbit)) {
