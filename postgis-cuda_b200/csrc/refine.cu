@@ -878,7 +878,7 @@ static void refine_t(gsj_ctx* c, const gsj_layer* P, const gsj_layer* R, const u
   const bool self = F && P == R;
   int iblocks = 1, fblocks = 1;
   uint32_t* sidx = nullptr;
-  const int self_cap = std::min(bin_cap + bin_cap / 2, CAP_SELF);   // the self bin holds 1.5 x the shared-memory bin
+  const int self_cap = std::min(sh.bin_cap + sh.bin_cap / 2, CAP_SELF);   // 1.5 x the shape's shared-memory bin threshold
   if (self) {
     const int sbit = S32 ? 16 : 8;
     if (!(c->refine_attr & sbit)) {
