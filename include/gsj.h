@@ -76,10 +76,10 @@ void gsj_refine_params_default(gsj_refine_params* p);
  * reorganised around per-pair candidate edge-pair lists (only edge pairs whose boxes come within 2 tol are visited). */
 #define GSJ_REFINE_PLAIN 0
 #define GSJ_REFINE_FILTERED 1
-/* GSJ_REFINE_FILTERED with its pure-sign orientation tests (the contact test, the probe point's crossing parity) first
- * decided in FP32 under a certified error bound, FP64 only where the bound cannot decide: the same results, bit for
- * bit (kept beside GSJ_REFINE_FILTERED for measured comparison). Ops other than joins and clustering run it as
- * GSJ_REFINE_FILTERED. */
+/* GSJ_REFINE_FILTERED with its pure-sign orientation tests (the contact test, the probe point's crossing parity, the
+ * point-in-ring tests of the area / relate sweeps) first decided in FP32 under a certified error bound, FP64 only
+ * where the bound cannot decide: the same results, bit for bit (kept beside GSJ_REFINE_FILTERED for measured
+ * comparison). Ops other than joins and clustering, and oversized pairs, run it as GSJ_REFINE_FILTERED. */
 #define GSJ_REFINE_FILTERED_FP32 2
 
 /* JoinOpts (engine.cuh:799-813). */

@@ -91,7 +91,8 @@ static __device__ bool pip_full_warp(const Frame& B, double mx, double my, int l
 }
 
 // inside(x) = inside(c) xor crossings of c -> x with the local edges (engine.cuh:400-412)
-template <bool F>
+// S32: the four orientation signs through the certified FP32 filter (the same booleans)
+template <bool F, bool S32 = false>
 __device__ __forceinline__ bool inside_from_c(const EList& L, int cnt, double cx, double cy, bool in_c, double x, double y) {
   bool in = in_c;
   const double sx0 = fmin(cx, x), sx1 = fmax(cx, x), sy0 = fmin(cy, y), sy1 = fmax(cy, y);
@@ -99,10 +100,17 @@ __device__ __forceinline__ bool inside_from_c(const EList& L, int cnt, double cx
     const double ex0 = L.x0[k], ey0 = L.y0[k], ex1 = L.x1[k], ey1 = L.y1[k];
     if (F ? out_cmp(ex0, ey0, ex1, ey1, sx0, sy0, sx1, sy1)
           : (fmax(ex0, ex1) < sx0 || fmin(ex0, ex1) > sx1 || fmax(ey0, ey1) < sy0 || fmin(ey0, ey1) > sy1)) return false;
-    bool sc = left_of(ex0, ey0, ex1, ey1, cx, cy), sx = left_of(ex0, ey0, ex1, ey1, x, y);
-    if (sc == sx) return false;
-    bool su = orient(cx, cy, x, y, ex0, ey0) > 0, sv = orient(cx, cy, x, y, ex1, ey1) > 0;
-    if (su != sv) in = !in;
+    if constexpr (S32) {
+      const bool sc = left_of32(ex0, ey0, ex1, ey1, cx, cy), sx = left_of32(ex0, ey0, ex1, ey1, x, y);
+      if (sc == sx) return false;
+      const bool su = orient_sign32(cx, cy, x, y, ex0, ey0) > 0, sv = orient_sign32(cx, cy, x, y, ex1, ey1) > 0;
+      if (su != sv) in = !in;
+    } else {
+      bool sc = left_of(ex0, ey0, ex1, ey1, cx, cy), sx = left_of(ex0, ey0, ex1, ey1, x, y);
+      if (sc == sx) return false;
+      bool su = orient(cx, cy, x, y, ex0, ey0) > 0, sv = orient(cx, cy, x, y, ex1, ey1) > 0;
+      if (su != sv) in = !in;
+    }
     return false;
   };
   for (int k = 0; k < cnt; k++) step(k);
@@ -111,15 +119,18 @@ __device__ __forceinline__ bool inside_from_c(const EList& L, int cnt, double cx
 
 // The same parity for one query point shared by the whole warp: lanes split the edges, a ballot counts crossings
 // (the parity does not depend on the order of the edges).
+template <bool S32 = false>
 static __device__ bool inside_from_c_warp(const EList& L, int cnt, double cx, double cy, bool in_c, double x, double y, int lane) {
   const double sx0 = fmin(cx, x), sx1 = fmax(cx, x), sy0 = fmin(cy, y), sy1 = fmax(cy, y);
   bool par = false;
   for (int k = lane; k < cnt; k += 32) {
     const double ex0 = L.x0[k], ey0 = L.y0[k], ex1 = L.x1[k], ey1 = L.y1[k];
     if (out_cmp(ex0, ey0, ex1, ey1, sx0, sy0, sx1, sy1)) continue;
-    bool sc = left_of(ex0, ey0, ex1, ey1, cx, cy), sx = left_of(ex0, ey0, ex1, ey1, x, y);
+    const bool sc = S32 ? left_of32(ex0, ey0, ex1, ey1, cx, cy) : left_of(ex0, ey0, ex1, ey1, cx, cy);
+    const bool sx = S32 ? left_of32(ex0, ey0, ex1, ey1, x, y) : left_of(ex0, ey0, ex1, ey1, x, y);
     if (sc == sx) continue;
-    bool su = orient(cx, cy, x, y, ex0, ey0) > 0, sv = orient(cx, cy, x, y, ex1, ey1) > 0;
+    const bool su = (S32 ? orient_sign32(cx, cy, x, y, ex0, ey0) : orient(cx, cy, x, y, ex0, ey0)) > 0;
+    const bool sv = (S32 ? orient_sign32(cx, cy, x, y, ex1, ey1) : orient(cx, cy, x, y, ex1, ey1)) > 0;
     if (su != sv) par = !par;
   }
   const bool odd = (__popc(__ballot_sync(0xffffffffu, par)) & 1) != 0;

@@ -257,7 +257,7 @@ __device__ void mask_candidates(const EList& LA, int na, const EList& LB, int nb
 // Green's-theorem contribution of edge p->q within the other polygon + relate lengths (engine.cuh:416-515).
 // each_k(visit) calls visit(k) for the other polygon's local edges k in increasing order: all of them, or only
 // those of a candidate list that holds every k passing the box test below (the same visits, the same results).
-template <bool F, class EachK>
+template <bool F, bool S32, class EachK>
 __device__ double edge_contrib_k(double px, double py, double qx, double qy, const EList& L, int cnt, bool in_c, const PairGeo& G, bool real,
                                  double* l_in, double* l_on, uint32_t* bits, uint32_t cut, EachK&& each_k) {
   const double dx = qx - px, dy = qy - py;
@@ -327,7 +327,7 @@ __device__ double edge_contrib_k(double px, double py, double qx, double qy, con
     // the inside test of the midpoint, evaluated once and only where a branch below reads it
     const bool lens = l_in && real;
     const bool need = first < 0 || (net != 1 && net != -1) || (lens && net_real == 0 && !(n_real == 0 && (net == 1 || net == -1)));
-    const int vin = (need && in_ov && inside_from_c<F>(L, cnt, G.cx, G.cy, in_c, mx, my)) ? 1 : 0;
+    const int vin = (need && in_ov && inside_from_c<F, S32>(L, cnt, G.cx, G.cy, in_c, mx, my)) ? 1 : 0;
     if (lens) {
       const double seg = sqrt(len2) * (t1 - t0);
       if (net_real != 0) { *l_on += seg; *bits |= (net_real > 0 ? REL_COIN_SAME : REL_COIN_OPP) | REL_TOUCH; }
@@ -357,7 +357,7 @@ __device__ double edge_contrib_k(double px, double py, double qx, double qy, con
 template <bool F>
 __device__ __forceinline__ double edge_contrib(double px, double py, double qx, double qy, const EList& L, int cnt, bool in_c, const PairGeo& G,
                                                bool real, double* l_in, double* l_on, uint32_t* bits, uint32_t cut) {
-  return edge_contrib_k<F>(px, py, qx, qy, L, cnt, in_c, G, real, l_in, l_on, bits, cut, [&](auto&& visit) {
+  return edge_contrib_k<F, false>(px, py, qx, qy, L, cnt, in_c, G, real, l_in, l_on, bits, cut, [&](auto&& visit) {
     for (int k = 0; k < cnt; k++) visit(k);
   });
 }
@@ -499,7 +499,7 @@ __device__ bool refine_pair_t(const DLayer& P, const DLayer& R, uint32_t a, uint
         for (uint32_t r = S.r0; r < S.r1 && !h; r++) {
           double x, y; const bool real = probe_vertex(S, r, x, y);
           if (!real) S.v(SL.rvo[r], x, y);
-          if (x >= G.ov.x0 && x <= G.ov.x1 && y >= G.ov.y0 && y <= G.ov.y1 && inside_from_c_warp(LO, no_, G.cx, G.cy, inc, x, y, lane)) {
+          if (x >= G.ov.x0 && x <= G.ov.x1 && y >= G.ov.y0 && y <= G.ov.y1 && inside_from_c_warp<S32>(LO, no_, G.cx, G.cy, inc, x, y, lane)) {
             ha = true; h = real;
           }
         }
@@ -533,7 +533,7 @@ __device__ bool refine_pair_t(const DLayer& P, const DLayer& R, uint32_t a, uint
       int k = 0;
       for (int i = lane; i < na; i += 32, k++) {
         const uint32_t f = LA.fl[i];
-        rec[k] = edge_contrib_k<F>(LA.x0[i], LA.y0[i], LA.x1[i], LA.y1[i], LB, nb, inB_c, G, !(f & 1u), rel ? &lin : nullptr, &lon, &bits, f,
+        rec[k] = edge_contrib_k<F, S32>(LA.x0[i], LA.y0[i], LA.x1[i], LA.y1[i], LB, nb, inB_c, G, !(f & 1u), rel ? &lin : nullptr, &lon, &bits, f,
                                    [&](auto&& visit) {
                                      for (int q = 0; q < nbw; q++)
                                        for (uint32_t m = mb->rm[q * MS + i]; m; m &= m - 1) visit((q << 5) + __ffs(m) - 1);
@@ -553,7 +553,7 @@ __device__ bool refine_pair_t(const DLayer& P, const DLayer& R, uint32_t a, uint
         double lin = 0.0, lon = 0.0;   // this pass's lengths (each starts from 0, so the sums are the same)
         for (int i = lane; i < nself; i += 32) {
           const uint32_t f = LS.fl[i];
-          s2 += edge_contrib_k<F>(LS.x0[i], LS.y0[i], LS.x1[i], LS.y1[i], LO, nother, inc, G, !(f & 1u), rel ? &lin : nullptr, &lon, &bits, f,
+          s2 += edge_contrib_k<F, S32>(LS.x0[i], LS.y0[i], LS.x1[i], LS.y1[i], LO, nother, inc, G, !(f & 1u), rel ? &lin : nullptr, &lon, &bits, f,
                                   [&](auto&& visit) {
                                     for (int q = 0; q < nw; q++)
                                       for (uint32_t m = mrow[q * CAP_F + i]; m; m &= m - 1) visit((q << 5) + __ffs(m) - 1);
@@ -567,7 +567,7 @@ __device__ bool refine_pair_t(const DLayer& P, const DLayer& R, uint32_t a, uint
       for (int i = lane; i < na; i += 32) {
         const uint32_t f = LA.fl[i];
         const int r0 = (int)fb->sa[i], r1 = (int)fb->sa[i + 1];
-        const double v = edge_contrib_k<F>(LA.x0[i], LA.y0[i], LA.x1[i], LA.y1[i], LB, nb, inB_c, G, !(f & 1u), rel ? &lin : nullptr, &lon, &bits, f,
+        const double v = edge_contrib_k<F, S32>(LA.x0[i], LA.y0[i], LA.x1[i], LA.y1[i], LB, nb, inB_c, G, !(f & 1u), rel ? &lin : nullptr, &lon, &bits, f,
                                            [&](auto&& visit) {
                                              for (int e = r0; e < r1; e++) visit((int)(cp[e] >> 16));
                                            });
@@ -589,7 +589,7 @@ __device__ bool refine_pair_t(const DLayer& P, const DLayer& R, uint32_t a, uint
           const uint32_t f = LS.fl[i];
           const int r0 = pass ? (i ? (int)fb->sb[i - 1] : 0) : (int)fb->sa[i];
           const int r1 = pass ? (int)fb->sb[i] : (int)fb->sa[i + 1];
-          s2 += edge_contrib_k<F>(LS.x0[i], LS.y0[i], LS.x1[i], LS.y1[i], LO, nother, inc, G, !(f & 1u), rel ? &lin : nullptr, &lon, &bits, f,
+          s2 += edge_contrib_k<F, S32>(LS.x0[i], LS.y0[i], LS.x1[i], LS.y1[i], LO, nother, inc, G, !(f & 1u), rel ? &lin : nullptr, &lon, &bits, f,
                                   [&](auto&& visit) {
                                     for (int e = r0; e < r1; e++) visit(pass ? (int)(cp[pj[e]] & 0xFFFFu) : (int)(cp[e] >> 16));
                                   });
