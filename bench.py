@@ -492,8 +492,50 @@ def run_op(args, rank, local, ws):
         pv, pms = aggregate(float(np.sum(res["plain"]["ms"])), float(res["plain"]["units"]), ws)
         line["plain_fp64"] = {"value": pv, "ms_per_step": pms / args.steps, "speedup_filtered": (pms / tot_ms) if tot_ms > 0 else None,
                               "same_units": res["plain"]["units"] == f["units"]}
+    if op in ("erode", "cluster") and ws == 1 and not cl_shard:
+        line["non_degenerate"] = non_degenerate_leg(eng, ext, op, n, box, LA, args)
     if rank == 0:
         print(json.dumps(line), flush=True)
+
+
+def non_degenerate_leg(eng, ext, op, n, box, LA, args):
+    """Beside the cfg5 numbers, the same op on inputs whose answer is not trivial on a tiling (where neighbours only
+    touch): erosion of the layer against an independently seeded layer of the same size (interiors overlap, so
+    eroded pairs survive), and clustering of a layer whose parcels are 55 % shrunk (components of every size).
+    Filtered variant, the same warm-up and step counts."""
+    import torch
+    from gsj import gen
+    if op == "erode":
+        other = gen.layer_cfg5(n, box, seed=1)
+        L2 = eng.upload_polygons(other)
+        work = f"erosion (1 m) of the layer against an independently seeded {n / 1e6:g}M-parcel layer"
+        run = lambda: eng.erode(LA, L2, 1.0, 1.0, same=False)[0]
+        count = len
+        unit = "pairs"
+    else:
+        shr = gen.shrunk(gen.layer_cfg5(n, box, seed=3), seed=3)
+        L2 = eng.upload_polygons(shr)
+        work = f"ST_ClusterIntersecting of {n / 1e6:g}M parcels, 55 % of them shrunk (components of every size)"
+        run = lambda: eng.cluster(L2)[0]
+        count = lambda root: int(len(np.unique(root)))
+        unit = "components"
+    ms, last = [], None
+    for i in range(args.warmup + args.steps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(ext):
+            e0.record()
+        r = run()
+        with torch.cuda.stream(ext):
+            e1.record()
+        e1.synchronize()
+        if i >= args.warmup:
+            ms.append(e0.elapsed_time(e1)); last = r
+    units = count(last)   # outside the timed region
+    L2.free()
+    out = {"workload": work, "ms_per_step": float(np.mean(ms)), unit: units}
+    out["value"] = (units if op == "erode" else n) / (float(np.mean(ms)) / 1000.0)
+    out["unit"] = "pairs/s" if op == "erode" else "parcels/s"
+    return out
 
 
 def reference_check(ps, filt, tmpdir):
