@@ -67,3 +67,20 @@ def test_sink_copy_out_matches_source():
         ptr = src.ctypes.data_as(ctypes.POINTER(np.ctypeslib.as_ctypes_type(dt)))
         out = gsj._copy_out(ptr, n, dt)
         assert out.dtype == dt and np.array_equal(out, src) and out.ctypes.data != src.ctypes.data
+
+
+def test_headers_are_plain_c(tmp_path):
+    """include/gsj.h and include/gsjd.h compile as C99 (what a cgo / FFI binding or the reference's C callers see)."""
+    import shutil
+    import subprocess
+    gcc = shutil.which("gcc")
+    if gcc is None:
+        import pytest
+        pytest.skip("no C compiler")
+    inc = os.path.join(ROOT, "include")
+    src = tmp_path / "h.c"
+    src.write_text('#include "gsj.h"\n#include "gsjd.h"\nint main(void) { gsj_refine_shape s = {4, 32, 128, 32}; gsj_tune_result t;\n'
+                   '  (void)t; return s.run + GSJ_TUNE_KEEP_RUNS + GSJ_REFINE_FILTERED_FP32; }\n')
+    r = subprocess.run([gcc, "-std=c99", "-Wall", "-Wextra", "-Werror", "-pedantic", "-I", inc, "-c", str(src), "-o", str(tmp_path / "h.o")],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
