@@ -576,6 +576,9 @@ def run_reference(args, rank, ws):
     if not RH.available():
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/harness (the reference engine's driver) is not built"}), flush=True)
         return
+    if args.op != "relate":
+        run_reference_op(args, RH)
+        return
     ps = gen.layer_parcels(args.seeds, BOX, seed=0)
     d = tempfile.mkdtemp(prefix="gsj_ref_")
     # The driver reports its phase times for its last repetition only, and its repetitions slow down after the first
@@ -617,6 +620,69 @@ def run_reference(args, rank, ws):
             "cpu_baseline": {"value": value, "unit": "pairs/s", "cores": os.cpu_count(), "kind": "reference",
                              "sample": f"the reference engine's driver on this box's GPU (host threads for its prep: {os.cpu_count()}); "
                                        f"relate self-join of {ps.n} parcels, the warm repetition, median of {runs} processes"},
+            "clocks": clk.summary()}
+    print(json.dumps(line), flush=True)
+
+
+def run_reference_op(args, RH):
+    """--impl reference --op X: the reference engine's driver on the layers `--op X` uses (rank 0's seeds). area: cfg1's
+    20k zones x 50 zones; dwithin: 1M points x 1M parcels at 5 m; cluster: the cfg5 layer; erode: the cfg5 layer against
+    an independently seeded one (the driver's self-join drops a geometry's pair with itself, so the two-layer form is
+    the one both engines define alike: the `non_degenerate` leg of `--op erode`). value = units / its GPU phase time
+    (traverse + refine + compact) of the warm repetition, median over up to 5 (cfg5: 3) driver processes."""
+    import shutil
+    import tempfile
+    from gsj import gen
+    op = args.op
+    d = tempfile.mkdtemp(prefix="gsj_refop_")
+    try:
+        if op == "area":
+            A, B = gen.layer_cfg_parcels_small(20000, seed=0), gen.layer_cfg_zones(50, seed=1)
+            fa, fb = os.path.join(d, "a.gset"), os.path.join(d, "b.gset")
+            gen.write_gset(fa, A); gen.write_gset(fb, B)
+            cmd, unit, key, work = [fa, fb, "--area"], "pairs/s", "gpu_hits", "intersects + area, 20k Voronoi zones x 50 zones"
+        elif op == "dwithin":
+            box = (-119.0, 33.0, -118.0, 34.0)
+            fp, fb = os.path.join(d, "p.pset"), os.path.join(d, "b.gset")
+            gen.write_pset(fp, gen.points(1_000_000, box, 7)); gen.write_gset(fb, gen.layer_parcels(1_000_000, box, seed=0))
+            cmd, unit, key, work = [fp, fb, "--dwithin", "5"], "pairs/s", "rows", "ST_DWithin 5 m, 1M points x 1M parcels"
+        else:
+            n = args.seeds or 20_000_000
+            side = 2.0 * (n / 2e6) ** 0.5
+            box = (-119.0, 33.0, -119.0 + side, 33.0 + side)
+            fa = os.path.join(d, "a.gset")
+            la = gen.layer_cfg5(n, box, seed=0)
+            gen.write_gset(fa, la)
+            n = int(la.n)   # parcels of the layer (the seeds' cells)
+            del la
+            if op == "erode":
+                fb = os.path.join(d, "b.gset")
+                gen.write_gset(fb, gen.layer_cfg5(n, box, seed=1))
+                cmd, unit, key = [fa, fb, "--erode", "1"], "pairs/s", "rows"
+                work = f"erosion (1 m) of a {n / 1e6:g}M-parcel layer against an independently seeded one"
+            else:
+                cmd, unit, key = [fa, fa, "--cluster"], "parcels/s", None
+                work = f"ST_ClusterIntersecting, {n / 1e6:g}M parcels"
+        runs = max(1, min(args.steps, 5 if op in ("area", "dwithin") else 3))
+        with Clocks(0) as clk:
+            rs = [RH.run(cmd, reps=2, timeout=3600) for _ in range(runs)]
+    except (RuntimeError, OSError, subprocess.TimeoutExpired) as e:
+        why = str(e).strip().splitlines()[-1][:300] if str(e).strip() else type(e).__name__
+        print(json.dumps({"impl": "reference", "unavailable": f"the reference engine's driver did not run: {why}"}), flush=True)
+        return
+    finally:
+        shutil.rmtree(d, ignore_errors=True)
+    # GPU phases as the driver reports them; clustering adds its union-find (gsj's cluster time includes its own)
+    gms = [RH.gpu_ms(r) + (r["ms"].get("union-find", 0.0) if op == "cluster" else 0.0) for r in rs]
+    k = int(np.argsort(gms)[len(gms) // 2])
+    r, ms = rs[k], gms[k]
+    units = r["count"][key] if key else n
+    line = {"impl": "reference", "metric": f"{unit} ({op})", "value": units / (ms / 1000.0), "unit": unit, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic (seeded Voronoi parcels / uniform points)", "config": {"workload": work, "units_per_step": int(units)},
+            "reference_engine": {"driver": "landstats-us/postgis-cuda engine/harness.cu, unmodified, nvcc -arch=sm_100a",
+                                 "command": "harness " + " ".join(os.path.basename(x) if x.endswith("set") else x for x in cmd) + " --reps 2",
+                                 "processes": runs, "phases_ms": r["ms"], "counts": r["count"], "gpu_ms_per_process": gms},
             "clocks": clk.summary()}
     print(json.dumps(line), flush=True)
 
