@@ -579,6 +579,7 @@ struct BEl { double x0, y0, x1, y1; };                                  // eleme
 constexpr double FILLET_QUANTUM = 3.14159265358979323846 / 16.0;       // 8 segments per quarter circle (GEOS default)
 constexpr int ER_WARPS = 2, ER_CAPE = 64, ER_CAPL = 128, ER_MAX_DEPTH = 12;
 constexpr int ER_QCAP = 64;                                                // crossing candidates queued per warp
+constexpr int ER_RUN = 4, ER_RUNS = 64, ER_MINB = 4;   // k_erode_main: pairs per fetch, fetches per warp, blocks per SM
 constexpr size_t ER_SMEM_WARP = 2 * ER_CAPE * sizeof(BEd) + 2 * ER_CAPL * sizeof(BEl) + ER_QCAP * sizeof(uint2);
 constexpr size_t ER_SMEM = (size_t)ER_WARPS * ER_SMEM_WARP;
 struct ErScratch { BEd* EA; BEd* EB; BEl* LA; BEl* LB; uint2* Q; int capE, capL; };
@@ -586,7 +587,7 @@ __host__ __device__ constexpr size_t er_scratch_bytes(size_t capE, size_t capL) 
   return 2 * capE * sizeof(BEd) + 2 * capL * sizeof(BEl) + ER_QCAP * sizeof(uint2);
 }
 struct ETile { uint32_t pair, depth; double4 box; };
-struct ErCtr { unsigned int ntile, nslab; int needE, needL; };
+struct ErCtr { unsigned int ntile, nslab; int needE, needL; unsigned long long next; };   // next: k_erode_main's pair counter
 struct EFrame { double ox, oy, kx, ky; };
 
 __device__ bool in_excl(const BEd* E, int n, double r, double x, double y, double eps) {   // buffer.cuh:285-319
@@ -963,17 +964,25 @@ __global__ void k_er_filter(const uint2* __restrict__ pr, const double* __restri
 }
 __global__ void __launch_bounds__(ER_WARPS * 32) k_erode_main(DLayer P, DLayer R, const uint32_t* pfP, const uint32_t* pfR, const uint2* __restrict__ pairs,
                                                               uint64_t np, double ra, double rb, bool self_layer, uint8_t* flag, uint32_t* heavy,
-                                                              unsigned int* nheavy) {
+                                                              unsigned int* nheavy, unsigned long long* next) {
   extern __shared__ __align__(16) unsigned char smem[];
   const int lane = threadIdx.x & 31;
   const ErScratch sc = er_smem(smem, threadIdx.x >> 5);
-  const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
-  for (uint64_t p = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; p < np; p += nw) {
-    const uint2 pr = pairs[p];
-    const int r = er_pair(P, R, piece_range(pfP, pr.x), piece_range(pfR, pr.y), ra, rb, sc, lane, nullptr, nullptr, nullptr, nullptr,
-                          self_layer && pr.x == pr.y);
-    if (lane == 0) { flag[p] = r > 0 ? 1 : 0; if (r < 0) heavy[atomicAdd(nheavy, 1u)] = (uint32_t)p; }
-    __syncwarp();
+  // warps take runs of ER_RUN consecutive pairs from a counter (pair costs vary widely: a fixed stride left most of
+  // the GPU idle behind the slowest warps), at most ER_RUNS runs each so that blocks retire
+  for (int k = 0; k < ER_RUNS; k++) {
+    unsigned long long p0 = 0;
+    if (lane == 0) p0 = atomicAdd(next, (unsigned long long)ER_RUN);
+    p0 = __shfl_sync(0xffffffffu, p0, 0);
+    if (p0 >= np) break;
+    const uint64_t p1 = p0 + ER_RUN < np ? p0 + ER_RUN : np;
+    for (uint64_t p = p0; p < p1; p++) {
+      const uint2 pr = pairs[p];
+      const int r = er_pair(P, R, piece_range(pfP, pr.x), piece_range(pfR, pr.y), ra, rb, sc, lane, nullptr, nullptr, nullptr, nullptr,
+                            self_layer && pr.x == pr.y);
+      if (lane == 0) { flag[p] = r > 0 ? 1 : 0; if (r < 0) heavy[atomicAdd(nheavy, 1u)] = (uint32_t)p; }
+      __syncwarp();
+    }
   }
 }
 __global__ void k_tiles_init(const uint32_t* __restrict__ heavy, uint64_t n, ETile* items) {
@@ -1102,8 +1111,14 @@ void erode_host(gsj_ctx* c, const gsj_layer* P, const gsj_layer* R, double ra, d
     uint32_t* heavy = c->er_heavy.as<uint32_t>(ne);
     ErCtr* ctr = c->er_ctr.as<ErCtr>(2);
     GSJ_CK(cudaMemsetAsync(ctr, 0, sizeof(ErCtr), s));
-    const int G = (int)std::min<uint64_t>((ne * 32 + 63) / 64, (uint64_t)c->sm_count * 32);
-    k_erode_main<<<G, ER_WARPS * 32, ER_SMEM, s>>>(P->d, R->d, pfP, pfR, ep, ne, ra, rb, self_layer, flag, heavy, &ctr->ntile); c->launches++;
+    // enough warps to cover every pair with ER_RUNS fetches each, spread over all SMs, whole waves beyond one
+    const uint64_t per_block = (uint64_t)ER_WARPS * ER_RUNS * ER_RUN, wave = (uint64_t)c->sm_count * ER_MINB;
+    uint64_t cover = (ne + per_block - 1) / per_block;
+    if (cover > wave) cover = (cover + wave - 1) / wave * wave;
+    const uint64_t spread = std::min<uint64_t>((ne + ER_WARPS * ER_RUN - 1) / (ER_WARPS * ER_RUN), wave);
+    const int G = (int)std::min<uint64_t>(std::max(cover, spread), 1u << 30);
+    k_erode_main<<<G, ER_WARPS * 32, ER_SMEM, s>>>(P->d, R->d, pfP, pfR, ep, ne, ra, rb, self_layer, flag, heavy, &ctr->ntile, &ctr->next);
+    c->launches++;
     GSJ_CK(cudaGetLastError());
     ErCtr h{};
     GSJ_CK(cudaMemcpyAsync(&h, ctr, sizeof(ErCtr), cudaMemcpyDeviceToHost, s));
