@@ -480,7 +480,13 @@ def run_op(args, rank, local, ws):
                      "peak": hbm, "unit": "GB/s", "frac": ref_bytes / (ref_ms / 1000.0) / 1e9 / hbm if ref_ms > 0 else None, "traffic": None,
                      "peak_source": "MEASURED_PEAKS.json hbm_gbs" if "hbm_gbs" in pk else "fallback",
                      "note": "bytes = candidates x both geometries' mean vertex bytes; the kernels are FP64/latency-bound, not HBM-bound"
-                             + ("; the cluster rounds refine a subset of the candidates" if op == "cluster" else "")},
+                             + ("; the cluster rounds refine a subset of the candidates" if op == "cluster" else ""),
+                     # the polygon refinement's FP64 work, as on the headline line: 70 flops per local edge pair, counted in the kernels
+                     "fp64": ({"achieved_tflops": ep * FLOPS_PER_EDGE_PAIR / (ref_ms / 1000.0) / 1e12,
+                               "frac": ep * FLOPS_PER_EDGE_PAIR / (ref_ms / 1000.0) / 1e12 / FP64_PEAK_TFLOPS, "peak_tflops": FP64_PEAK_TFLOPS,
+                               "edge_pairs_per_step": ep,
+                               "what": "the refine phase's time includes the erosion tests" if op == "erode" else "the refine phase"}
+                              if (ep := float(np.mean([s_.get("edge_pairs", 0) for s_ in st]))) > 0 and ref_ms > 0 else None)},
         "roofline_traversal": {"kernel": "k_traverse", "bound": "hbm",
                                "achieved": trav_bytes / (trav_ms / 1000.0) / 1e9 if trav_ms > 0 else None, "peak": hbm, "unit": "GB/s",
                                "frac": trav_bytes / (trav_ms / 1000.0) / 1e9 / hbm if trav_ms > 0 else None},
